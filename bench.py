@@ -1,0 +1,320 @@
+"""Benchmark: MLUPS of the LBM_Mutiwing time step on B200.
+
+Default workload: the 4000x2000 two-wing case (4001 x 2001 nodes, dx = 0.01,
+Re 1000, two NACA0012 wings with 200 cosine-spaced markers each, analytic
+pitch/heave motion), FP32 deviation storage, FP64 immersed boundary and force
+reductions.  A "step" is one lattice time step (evolution, solution.f90:272)
+of one episode; with N GPUs every rank advances its own episode (episodes are
+independent: weak scaling, no collective on the data path).
+
+value  = whole-job MLUPS = sum over ranks of nx*ny*steps / max-over-ranks time,
+         timed with CUDA events on the library's stream, state resident in HBM.
+e2e    = the same metric through the online STEP path of the C ABI: per
+         segment of 50 steps, the segment's two motion rows go host -> device
+         and every step's force row comes back device -> host, both inside the
+         timed region.
+roofline: the fused collide-stream kernel's algorithmic traffic (9 reads +
+         9 writes of 4 bytes per interior node) over its mean CUDA-event time,
+         against the measured HBM copy bandwidth.
+The distribution planes (2 x 288 MB) exceed the 126 MB L2, so no separate L2
+flush is needed between steps.
+
+--impl reference times the CPU oracle (the C++ FP64 restatement of the
+reference's Fortran, which cannot be compiled here) on the same workload with
+all host threads, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS (lattice node updates per second / 1e6)"
+UNIT = "MLUPS"
+SEG = 50
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(name, steps):
+    from lbm_mutiwing_b200 import workloads as wl
+    return wl.config1(steps=steps) if name == "cfg1" else wl.config2(steps=steps)
+
+
+def dist_init(n):
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+            sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+            mx = max(float(r[2]) for r in rows)
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                    "reasons": sorted(reasons), "samples": len(rows)}
+        except Exception as e:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload_name):
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "fused_bulk_traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(workload_name)
+    except Exception:
+        return None
+
+
+def cpu_sample(ep, steps, threads):
+    """Time the oracle on the full workload for a bounded number of steps."""
+    from oracle import oracle
+    oracle.build()
+    o = oracle.Oracle(ep, nthreads=threads)
+    o.step(1)                      # first step: allocation and page-in
+    t0 = time.perf_counter()
+    for n in range(2, 2 + steps):
+        o.step(n)
+    dt = time.perf_counter() - t0
+    o.close()
+    return ep.nx * ep.ny * steps / dt / 1e6, dt
+
+
+def run_reference(args):
+    rank, world, _ = dist_init(args.gpus)
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    ep = workload(args.workload, steps + args.warmup + 2)
+    threads = os.cpu_count() or 1
+    from oracle import oracle
+    oracle.build()
+    o = oracle.Oracle(ep, nthreads=threads)
+    for n in range(1, 1 + args.warmup):
+        o.step(n)
+    t0 = time.perf_counter()
+    for n in range(1 + args.warmup, 1 + args.warmup + steps):
+        o.step(n)
+    dt = time.perf_counter() - t0
+    mlups = ep.nx * ep.ny * steps / dt / 1e6
+    line = {"metric": METRIC, "value": mlups, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded NACA0012 geometry, analytic motion)",
+            "config": {"workload": ep.name, "nodes": ep.nx * ep.ny, "wings": ep.wing_count,
+                       "markers_per_wing": int(ep.markers[0].shape[0] - 1)},
+            "cpu_baseline": {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} full steps of {ep.name} after {args.warmup} warm-up"},
+            "e2e": {"value": mlups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    rank, world, local = dist_init(args.gpus)
+    import torch
+    from lbm_mutiwing_b200 import api, build
+    if rank == 0:
+        build.build()
+    barrier(world)
+    torch.cuda.set_device(local)
+    prec = api.PRECISION_FP32 if args.precision == "fp32" else api.PRECISION_FP64
+    K, Wm = args.steps, max(3, args.warmup)
+    ep = workload(args.workload, Wm + 2 * K + 4)
+    nodes = ep.nx * ep.ny
+    sim = api.Simulation(ep, prec, device=local)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    # warm-up
+    sim.step(Wm, first_cycle=1, rows=False)
+    torch.cuda.synchronize()
+    # timed region: K steps, device time by CUDA events on the library stream
+    barrier(world)
+    torch.cuda.synchronize()
+    sim.set_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        sim.step(K, first_cycle=Wm + 1, rows=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    phases = sim.phase_times()
+    sim.set_timing(False)
+    ms_max = allmax(ms, world)
+    barrier(world)
+    value = nodes * K * world / (ms_max / 1e3) / 1e6
+
+    sim.close()
+
+    # e2e: online STEP segments (driver.f90:174-195) through the C ABI with
+    # host buffers -- per segment the start and target motion rows go to the
+    # device, and every step's force row comes back.
+    sim_e = api.Simulation(ep, prec, motion_source=api.MOTION_STREAM, device=local)
+    ncol = 1 + 9 * ep.wing_count
+    # online rows carry displacements relative to the wing bases (mode.f90:207-214)
+    motion_rows = ep.motion.copy()
+    for w in range(ep.wing_count):
+        motion_rows[:, 4 + 9 * w] -= ep.wing_x_origin + w * ep.wing_x_spacing
+        motion_rows[:, 7 + 9 * w] -= ep.wing_y_origin
+    sim_e.set_stream_rows(motion_rows[0], motion_rows[SEG])
+    sim_e.step(Wm, first_cycle=1, rows=False)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done, cyc = 0, Wm + 1
+    while done < K:
+        n = min(SEG, K - done)
+        a = motion_rows[cyc - 1]
+        b = motion_rows[min(cyc - 1 + n, motion_rows.shape[0] - 1)]
+        sim_e.set_stream_rows(a, b)
+        out = sim_e.step(n, first_cycle=cyc, rows=True)
+        assert out.shape == (n, sim_e.row_len)
+        done += n
+        cyc += n
+    torch.cuda.synchronize()
+    e2e_s = allmax(time.perf_counter() - t0, world)
+    e2e = nodes * K * world / e2e_s / 1e6
+    h2d = 2 * ncol * 8 / SEG
+    d2h = sim_e.row_len * 8
+    sim_e.close()
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    bytes_per_node = 72 if prec == api.PRECISION_FP32 else 144
+    interior = (ep.nx - 2) * (ep.ny - 2)
+    alg_bytes = bytes_per_node * interior
+    bulk_ms = phases["collide_stream_ms"] / max(1, phases["steps"])
+    achieved = alg_bytes / (bulk_ms / 1e3) / 1e9
+    roof = {"kernel": "fused_bulk_kernel" if prec == api.PRECISION_FP32 else "plain stream+moments+collide",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": ncu_traffic(ep.name) if prec == api.PRECISION_FP32 else None,
+            "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": bulk_ms}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == api.PRECISION_FP32 else "f64",
+            "data": "synthetic (seeded NACA0012 geometry, analytic pitch/heave motion)",
+            "config": {"workload": ep.name, "nodes": nodes, "wings": ep.wing_count,
+                       "markers_per_wing": int(ep.markers[0].shape[0] - 1),
+                       "storage": "fp32 deviation" if prec == api.PRECISION_FP32 else "fp64 plain",
+                       "l2": "planes 2 x %.0f MB exceed the 126 MB L2; no flush" % (9 * ep.nx * ep.ny * (4 if prec else 8) / 1e6),
+                       "parallelism": f"{world} independent episodes"},
+            "phases_ms_per_step": {k: v / max(1, phases["steps"]) for k, v in phases.items() if k != "steps"},
+            "roofline": roof,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "segment_steps": SEG},
+            "clocks": clk.summary(),
+            "gpu_launches": K * (5 if prec == api.PRECISION_FP32 else 7)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cpu_steps = 8
+        mlups, dt = cpu_sample(workload(args.workload, cpu_steps + 4), cpu_steps, threads)
+        line["cpu_baseline"] = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{cpu_steps} full steps of {ep.name} ({dt:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/*
+ * lbm_mutiwing.h -- C ABI of the B200 implementation of the LBM_Mutiwing time
+ * step: D2Q9 MRT collide-and-stream plus the implicit immersed-boundary
+ * (bc_num = 4) interpolate / velocity-correct / spread cycle for moving
+ * multi-airfoils, on one GPU.
+ *
+ * The reference (R-IFFERY/LBM_Mutiwing, Fortran 90 + OpenACC) keeps all state
+ * in module globals and calls `evolution` once per lattice step.  Each entry
+ * point below replaces one reference routine; the citation names it
+ * (file:line in the reference project).  A Fortran host binds these with an
+ * ISO_C_BINDING interface block.
+ *
+ * Conventions
+ *  - Status: 0 on success, negative on error; lbm_last_error() gives the text
+ *    (the text an online driver sends back as "ERROR <msg>").  Nothing in the
+ *    library exits or stops the process.
+ *  - Ownership: the library owns all device memory; callers own host buffers.
+ *  - Threading: calls on one handle are serialised by the caller; handles are
+ *    independent.  Work is stream-ordered; calls that return host data
+ *    synchronise before returning.
+ *  - Arrays are row-major with x fastest: index (j-1)*nx + (i-1) holds the
+ *    reference's mesh%f(i,j) etc.; distribution planes are 9 consecutive
+ *    nx*ny planes in the reference's velocity order.
+ */
+#ifndef LBM_MUTIWING_H
+#define LBM_MUTIWING_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* Storage / compute path. */
+#define LBM_PRECISION_FP64 0   /* plain FP64, reference kernel order (the drop-in) */
+#define LBM_PRECISION_FP32 1   /* fused pull kernel, FP32 deviation storage */
+
+/* Motion source (driver.f90:10-31, LBM_MOTION_SOURCE). */
+#define LBM_MOTION_FILE 1      /* per-step table built from motion_params.dat rows */
+#define LBM_MOTION_STREAM 2    /* online smooth ramp between two rows (ZeroMQ STEP) */
+
+/* lbm_step flags */
+#define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */
+#define LBM_STEP_ERR 2         /* last two steps keep u, u0 so lbm_err is available */
+
+typedef struct LbmHandle LbmHandle;
+
+/* Runtime form of the reference's compile-time parameters
+ * (main.f90:7-152, ini_mesh.f90:15-67). */
+typedef struct LbmConfig {
+    int32_t nx, ny;              /* lattice nodes: nint(W/scale)+1, nint(H/scale)+1 (ini_mesh.f90:22-23) */
+    double scale;                /* lattice spacing in chords (mesh_max_scale, main.f90:32) */
+    double uu;                   /* inflow lattice velocity UU (main.f90:12) */
+    double re;                   /* Reynolds number on the chord (main.f90:106) */
+    double ox, oy;               /* physical position of node (1,1) (ini_mesh.f90:36-37) */
+    double s[9];                 /* MRT rates (ini_mesh.f90:59-67); s[7], s[8] <= 0 select 1/tau */
+    int32_t wing_count;          /* wings (main.f90:18); 0 allowed (no immersed body) */
+    double wing_x_origin;        /* main.f90:34 */
+    double wing_x_spacing;       /* main.f90:35 */
+    double wing_y_origin;        /* main.f90:36 */
+    double xc, yc;               /* flow-centre offset (main.f90:114) */
+    int32_t motion_source;       /* LBM_MOTION_FILE or LBM_MOTION_STREAM */
+    int32_t precision;           /* LBM_PRECISION_* */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t reserved[7];
+} LbmConfig;
+
+/* Fill cfg with the reference defaults: 4001x2001 lattice, scale 0.01,
+ * UU 0.01, Re 500, two wings at x 0.0 / 1.5, y 0.5, file motion, FP64. */
+void lbm_config_default(LbmConfig* cfg);
+
+/* Allocate and initialise one simulation: ini_mesh (ini_mesh.f90:1-80),
+ * init (solution.f90:1-75) and read_boundary (airfoil.f90:207-242).
+ * markers_xy: body-frame points (x, y) of all wings back to back, each wing a
+ * closed loop with its first point repeated last; points_per_wing[w] >= 2. */
+int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* points_per_wing,
+               LbmHandle** out);
+
+/* Episode reset: reset_zmq_episode (driver.f90:205-258) -- fresh initial
+ * state, empty band, cycle 1, force sums cleared. */
+int lbm_reset(LbmHandle* h);
+
+/* load_motion_table + build_motion_step_table (mode.f90:104-178, 388-412):
+ * rows of 1 + 9*wing_count columns, non-decreasing time, absolute x and y. */
+int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_t ncols);
+
+/* Online segment (driver.f90:174-186): motion between start_row and
+ * target_row, each 1 + 9*wing_count values, interpolated per step as
+ * lookup_stream_motion_row (mode.f90:414-449). */
+int lbm_set_stream_rows(LbmHandle* h, const double* start_row, const double* target_row);
+
+/* build_stream_target_row (mode.f90:287-325), host-side helper:
+ * delta_row = (t, domega, dxv, dyv per wing). */
+int lbm_build_stream_target_row(const LbmHandle* h, const double* start_row, double target_time,
+                                const double* delta_row, double* target_row);
+
+/* n_steps passes of evolution (solution.f90:272-422) for cycles
+ * first_cycle .. first_cycle+n_steps-1, each followed by the move_mesh check
+ * (main.f90:393-411).  force_rows (may be NULL) receives n_steps rows of
+ * 4 + 12*wing_count doubles in the force_row layout of solution.f90:352-378.
+ * Each row is also added to the running sums (latest_force_sum_row). */
+int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_rows, int32_t flags);
+
+/* Running force sums since the last reset (solution.f90:379-385). */
+int lbm_get_sums(LbmHandle* h, double* sum_row, int32_t* sample_count, int32_t* row_len);
+int lbm_reset_sums(LbmHandle* h);
+
+/* rho, u, v, pre after the last step (any pointer may be NULL) -- the fields
+ * output (solution.f90:132-241) reads.  The FP32 path needs LBM_STEP_FIELDS
+ * on that step. */
+int lbm_get_fields(LbmHandle* h, double* rho, double* u, double* v, double* pre);
+
+/* erranalysis (solution.f90:77-130) on the fields of the last two steps. */
+int lbm_err(LbmHandle* h, double* err);
+
+/* Distributions f (9 planes, FP64) of the current state; set replaces them. */
+int lbm_get_f(LbmHandle* h, double* f);
+int lbm_set_f(LbmHandle* h, const double* f);
+
+/* Band of the last step (adjoint_p, adjoint_wing_id; airfoil.f90:322-333):
+ * 3 ints per node (i, j, wing), 1-based, in the reference's order. */
+int lbm_get_band(LbmHandle* h, int32_t* n, int32_t* ij_wing, int32_t cap);
+
+/* Marker points xb1, yb1 and segment midpoints xb2, yb2 of the last step. */
+int lbm_get_markers(LbmHandle* h, double* xb1, double* yb1, double* xb2, double* yb2);
+
+/* move_mesh (move_mesh.f90:1-336): shift the lattice one column (dr = +1/-1). */
+int lbm_move_mesh(LbmHandle* h, int32_t dr);
+
+/* Relative no-slip residual |X du - (ub - X u*)| / |ub - X u*| of the last step. */
+int lbm_ibm_residual(LbmHandle* h, double* res);
+
+/* Bit set of numerical warnings since the last call (band capacity, pivot
+ * clamps, coupled wings); cleared on read. */
+int lbm_status(LbmHandle* h, int32_t* bits);
+
+/* Phase timers, the device-side counterpart of the reference's cpu_time
+ * phase totals (main.f90:384-392, 443-456).  When enabled, every step records
+ * CUDA events around its kernels; lbm_get_phase_times returns, in ms summed
+ * over the timed steps: [0] marker/band/IBM, [1] collide-stream (bulk or
+ * stream+moments+collide), [2] band re-collision, [3] far-field boundary,
+ * [4] number of steps timed.  Enabling (or disabling) clears the totals. */
+int lbm_set_timing(LbmHandle* h, int32_t enable);
+int lbm_get_phase_times(LbmHandle* h, double* out5);
+
+/* The CUDA stream (cudaStream_t) the handle's step kernels are ordered on,
+ * for callers that record their own events around lbm_step. */
+void* lbm_stream(LbmHandle* h);
+
+/* Device memory the handle holds, in bytes. */
+int64_t lbm_device_bytes(const LbmHandle* h);
+
+const char* lbm_last_error(const LbmHandle* h);
+void lbm_destroy(LbmHandle* h);
+int lbm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,262 @@
+// Fused FP32 path: one pull-scheme kernel does streaming, moments and the MRT
+// collision for every interior node (solution.f90:440-669 in one pass), on
+// distributions stored in FP32 as deviations from the rest equilibrium,
+// g_k = f_k - w_k (rho0 = 1, w_k the FP32-rounded weights of D2Q9model.f90).
+//
+// Layout in HBM: nine planes g[k][y][x] with a padded row pitch (multiple of
+// 32 floats), two copies (ping-pong A -> B).  A thread owns one x column and
+// walks ROWS consecutive rows; the nine loads of a row are warp-coalesced
+// (shifted by the lattice velocity) and each stored value is read exactly once
+// by the next step, so HBM traffic is 9 reads + 9 writes of 4 bytes per node.
+//
+// Deviation form of the collision: with c = M w (only c0, c1, c2 are
+// non-zero), m_dev = M g and rho = 1 + (m_dev,0 + W - 1), the post-collision
+// deviation is m'_dev = m_dev + S (m_eq(rho, j) - c - m_dev), g' = M^-1 m'_dev.
+// Bulk nodes carry no body force (the immersed-boundary force is non-zero
+// only on band nodes), so j = (m_dev,3, m_dev,5) and m_eq needs no division.
+// Band nodes are re-collided afterwards in FP64 by fused_band_kernel with the
+// corrected velocity and the Guo forcing term.
+#include "lbm_kernels.h"
+
+namespace lbm {
+
+constexpr int BULK_TX = 128;
+constexpr int BULK_ROWS = 4;
+
+FusedConsts fused_consts(const DevState& d) {
+    double w0 = weight(0), w1 = weight(1), w5 = weight(5);
+    double W = w0 + 4.0 * w1 + 4.0 * w5;
+    double c1 = -4.0 * w0 - 4.0 * w1 + 8.0 * w5;
+    double c2 = 4.0 * w0 - 8.0 * w1 + 4.0 * w5;
+    FusedConsts c;
+    c.s1 = (float)d.s[1]; c.s2 = (float)d.s[2]; c.s4 = (float)d.s[4];
+    c.s6 = (float)d.s[6]; c.s7 = (float)d.s[7]; c.s8 = (float)d.s[8];
+    c.k1 = (float)(2.0 + c1);
+    c.k2 = (float)(1.0 - c2);
+    c.wm1 = (float)(W - 1.0);
+    return c;
+}
+
+template <bool FIELDS>
+__global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __restrict__ gA, float* __restrict__ gB,
+                                                             int nx, int ny, int pitch, long long plane,
+                                                             FusedConsts c, double* __restrict__ fo_rho,
+                                                             double* __restrict__ fo_u, double* __restrict__ fo_v) {
+    const int i = blockIdx.x * BULK_TX + threadIdx.x + 1;
+    if (i > nx - 2) return;
+    const int j0 = blockIdx.y * BULK_ROWS + 1;
+#pragma unroll
+    for (int r = 0; r < BULK_ROWS; ++r) {
+        const int j = j0 + r;
+        if (j > ny - 2) break;
+        const long long p = (long long)j * pitch + i;
+        float g[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g[k] = __ldg(gA + k * plane + p - ex(k) - (long long)ey(k) * pitch);
+        // moments of the deviation
+        const float s14 = (g[1] + g[3]) + (g[2] + g[4]);
+        const float s58 = (g[5] + g[7]) + (g[6] + g[8]);
+        const float m0 = (g[0] + s14) + s58;
+        const float m1 = -4.0f * g[0] - s14 + 2.0f * s58;
+        const float m2 = 4.0f * g[0] - 2.0f * s14 + s58;
+        const float d13 = g[1] - g[3], d24 = g[2] - g[4];
+        const float a5 = g[5] - g[7], a6 = g[6] - g[8];
+        const float jx = d13 + a5 - a6;
+        const float m4 = -2.0f * d13 + a5 - a6;
+        const float jy = d24 + a5 + a6;
+        const float m6 = -2.0f * d24 + a5 + a6;
+        const float m7 = (g[1] + g[3]) - (g[2] + g[4]);
+        const float m8 = (g[5] + g[7]) - (g[6] + g[8]);
+        // relaxation toward the equilibrium moments (solution.f90:616-646)
+        const float drho = m0 + c.wm1;
+        const float jxx = jx * jx, jyy = jy * jy;
+        const float e1 = m1 + c.s1 * ((-2.0f * drho + 3.0f * (jxx + jyy) - c.k1) - m1);
+        const float e2 = m2 + c.s2 * ((drho - 3.0f * (jxx + jyy) + c.k2) - m2);
+        const float e4 = m4 + c.s4 * (-jx - m4);
+        const float e6 = m6 + c.s6 * (-jy - m6);
+        const float e7 = m7 + c.s7 * ((jxx - jyy) - m7);
+        const float e8 = m8 + c.s8 * (jx * jy - m8);
+        // back to populations: M^-1 = M^T diag(1/9, 1/36, 1/36, 1/6, 1/12, 1/6, 1/12, 1/4, 1/4)
+        const float b0 = m0 * (1.0f / 9.0f);
+        const float b1 = e1 * (1.0f / 36.0f), b2 = e2 * (1.0f / 36.0f);
+        const float b3 = jx * (1.0f / 6.0f), b4 = e4 * (1.0f / 12.0f);
+        const float b5 = jy * (1.0f / 6.0f), b6 = e6 * (1.0f / 12.0f);
+        const float b7 = e7 * 0.25f, b8 = e8 * 0.25f;
+        const float rA = b0 - b1 - 2.0f * b2;       // axis populations, common part
+        const float rD = b0 + 2.0f * b1 + b2;       // diagonal populations, common part
+        const float x34 = b3 - 2.0f * b4, y56 = b5 - 2.0f * b6;
+        const float xd = b3 + b4, yd = b5 + b6;
+        float o[9];
+        o[0] = b0 - 4.0f * b1 + 4.0f * b2;
+        o[1] = rA + x34 + b7;
+        o[2] = rA + y56 - b7;
+        o[3] = rA - x34 + b7;
+        o[4] = rA - y56 - b7;
+        o[5] = rD + xd + yd + b8;
+        o[6] = rD - xd + yd - b8;
+        o[7] = rD - xd - yd + b8;
+        o[8] = rD + xd - yd - b8;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gB[k * plane + p] = o[k];
+        if (FIELDS) {
+            const double rho = 1.0 + (double)drho;
+            fo_rho[p] = rho;
+            fo_u[p] = (double)jx / rho;
+            fo_v[p] = (double)jy / rho;
+        }
+    }
+}
+
+// Band nodes: FP64 re-collision with the corrected velocity u* + du and the
+// body force 2 rho du (solution.f90:599-655 with boundary_condition.f90:1645-1659).
+template <bool FIELDS>
+__global__ void fused_band_kernel(DevState d) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.band_n[0]) return;
+    const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
+    if (i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1) return;
+    const long long p = pidx(d, i, j);
+    double f[9], temp[9], temp1[9], fp[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sum = sum + (double)mrt_m(r, q) * f[q];
+        temp1[r] = sum;
+    }
+    const double rt = d.band_rho[b];
+    const double ut = d.band_us[b] + d.band_du[b], vt = d.band_vs[b] + d.band_dv[b];
+    const double gx = 2.0 * rt * d.band_du[b], gy = 2.0 * rt * d.band_dv[b];
+    const double* s = d.s;
+    temp[0] = 0.0;
+    temp[1] = -(2.0 * rt) + 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[2] = rt - 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[3] = 0.0;
+    temp[4] = -(rt * ut);
+    temp[5] = 0.0;
+    temp[6] = -(rt * vt);
+    temp[7] = (rt * ut * rt * ut - rt * vt * rt * vt);
+    temp[8] = (rt * ut * rt * vt);
+    fp[0] = 0.0;
+    fp[1] = 6.0 * (1.0 - 0.5 * s[1]) * (ut * gx + vt * gy);
+    fp[2] = -(6.0 * (1.0 - 0.5 * s[2]) * (ut * gx + vt * gy));
+    fp[3] = gx;
+    fp[4] = -((1.0 - 0.5 * s[4]) * gx);
+    fp[5] = gy;
+    fp[6] = -((1.0 - 0.5 * s[6]) * gy);
+    fp[7] = 2.0 * (1.0 - 0.5 * s[7]) * (ut * gx - vt * gy);
+    fp[8] = (1.0 - 0.5 * s[8]) * (ut * gy + vt * gx);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) temp[k] = temp1[k] + (temp[k] - temp1[k]) * s[k] + fp[k];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sum = sum + d.minv[r * 9 + q] * temp[q];
+        d.gB[r * d.plane + p] = (float)(sum - weight(r));
+    }
+    if (FIELDS && d.fo_rho) {
+        d.fo_rho[p] = rt;
+        d.fo_u[p] = ut;
+        d.fo_v[p] = vt;
+    }
+}
+
+// Initial state (solution.f90:44-61): f = f0 = feq(1, UU, 0) on every node,
+// both copies of the planes and the border f0 store.
+__global__ void fused_init_kernel(DevState d) {
+    const long long n = d.plane;
+    const long long per = 2LL * d.ny + 2LL * d.nx;
+    double fe[9];
+    const double u1 = d.uu, v1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        double eu = (double)ex(k) * u1 + (double)ey(k) * v1;
+        double utwo = u1 * u1 + v1 * v1;
+        fe[k] = weight(k) * 1.0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * utwo);
+    }
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            float g = (float)(fe[k] - weight(k));
+            d.gA[k * n + t] = g;
+            d.gB[k * n + t] = g;
+        }
+        if (t < per) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) d.edge_f0[k * per + t] = fe[k];
+        }
+    }
+}
+
+// move_mesh for the fused path: gB = gA shifted by one column (dr = +1 takes
+// the right neighbour), and the border f0 store takes the shifted values as
+// the reference's f0 does (move_mesh.f90:36-55).
+__global__ void fused_shift_kernel(DevState d, int dr) {
+    const long long per = 2LL * d.ny + 2LL * d.nx;
+    const long long total = (long long)d.nx * d.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx), j = (int)(t / d.nx);
+        const bool moved = dr == 1 ? (i <= d.nx - 2) : (i >= 1);
+        const int src = moved ? i + dr : i;
+        const long long p = pidx(d, i, j), q = pidx(d, src, j);
+        for (int k = 0; k < 9; ++k) d.gB[k * d.plane + p] = d.gA[k * d.plane + q];
+        if (moved) {
+            long long e = -1;
+            if (i == 0) e = j;
+            else if (i == d.nx - 1) e = d.ny + j;
+            if (e >= 0)
+                for (int k = 0; k < 9; ++k) d.edge_f0[k * per + e] = (double)d.gA[k * d.plane + q] + weight(k);
+            e = -1;
+            if (j == 0) e = 2LL * d.ny + i;
+            else if (j == d.ny - 1) e = 2LL * d.ny + d.nx + i;
+            if (e >= 0)
+                for (int k = 0; k < 9; ++k) d.edge_f0[k * per + e] = (double)d.gA[k * d.plane + q] + weight(k);
+        }
+    }
+}
+
+__global__ void fused_export_kernel(DevState d, const float* g, double* f) {
+    const long long total = (long long)d.nx * d.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx), j = (int)(t / d.nx);
+        const long long p = pidx(d, i, j);
+        for (int k = 0; k < 9; ++k) f[k * total + t] = (double)g[k * d.plane + p] + weight(k);
+    }
+}
+
+__global__ void fused_import_kernel(DevState d, const double* f, float* g) {
+    const long long total = (long long)d.nx * d.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx), j = (int)(t / d.nx);
+        const long long p = pidx(d, i, j);
+        for (int k = 0; k < 9; ++k) g[k * d.plane + p] = (float)(f[k * total + t] - weight(k));
+    }
+}
+
+void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st) {
+    dim3 b(BULK_TX), g((d.nx - 2 + BULK_TX - 1) / BULK_TX, (d.ny - 2 + BULK_ROWS - 1) / BULK_ROWS);
+    if (fields)
+        fused_bulk_kernel<true><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, d.fo_rho, d.fo_u, d.fo_v);
+    else
+        fused_bulk_kernel<false><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr);
+}
+void launch_fused_band(const DevState& d, bool fields, cudaStream_t st) {
+    const int n = d.band_cap;
+    if (fields)
+        fused_band_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(d);
+    else
+        fused_band_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(d);
+}
+void launch_fused_init(const DevState& d, cudaStream_t st) { fused_init_kernel<<<1184, 256, 0, st>>>(d); }
+void launch_fused_shift(const DevState& d, int dr, cudaStream_t st) { fused_shift_kernel<<<1184, 256, 0, st>>>(d, dr); }
+void launch_fused_export(const DevState& d, const float* g, double* f, cudaStream_t st) {
+    fused_export_kernel<<<1184, 256, 0, st>>>(d, g, f);
+}
+void launch_fused_import(const DevState& d, const double* f, float* g, cudaStream_t st) {
+    fused_import_kernel<<<1184, 256, 0, st>>>(d, f, g);
+}
+
+}  // namespace lbm

@@ -1,0 +1,918 @@
+// C ABI and host-side orchestration: set-up (ini_mesh, init, read_boundary),
+// motion tables (mode.f90), the step sequence of evolution and its
+// force-row bookkeeping, field export and the lattice shift.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_mutiwing.h"
+#include "lbm_kernels.h"
+
+namespace lbm {
+cudaError_t ibm_set_smem_limit(size_t bytes);
+
+// nizhen (solution.f90:1474-1529): Gauss-Jordan inverse of M as the reference
+// computes it, so the plain path multiplies by the same M^-1 entries.
+static void gauss_jordan_inverse(double out[81]) {
+    double a[10][10], b1[10][10];
+    for (int i = 1; i <= 9; ++i)
+        for (int j = 1; j <= 9; ++j) { a[i][j] = mrt_m(i - 1, j - 1); b1[i][j] = (i == j) ? 1.0 : 0.0; }
+    const int Nm = 9;
+    double temp, mik;
+    for (int k = 1; k <= Nm - 1; ++k) {
+        int ik = k;
+        temp = std::fabs(a[ik][k]);
+        for (int i = k; i <= Nm; ++i)
+            if (std::fabs(a[i][k]) > std::fabs(temp)) { temp = std::fabs(a[i][k]); ik = i; }
+        for (int j = 1; j <= Nm; ++j) {
+            std::swap(a[ik][j], a[k][j]);
+            std::swap(b1[ik][j], b1[k][j]);
+        }
+        for (int i = 1; i <= Nm; ++i) {
+            mik = a[i][k] / a[k][k];
+            temp = a[k][k];
+            for (int j = k; j <= Nm; ++j)
+                if (i != k) a[i][j] = a[i][j] - mik * a[k][j];
+            for (int j = k; j <= Nm; ++j) a[k][j] = a[k][j] / temp;
+            for (int j = 1; j <= Nm; ++j)
+                if (i != k) b1[i][j] = b1[i][j] - mik * b1[k][j];
+            for (int j = 1; j <= Nm; ++j) b1[k][j] = b1[k][j] / temp;
+        }
+    }
+    temp = a[Nm][Nm];
+    for (int i = 1; i <= Nm - 1; ++i) {
+        mik = a[i][Nm] / a[Nm][Nm];
+        a[i][Nm] = 0.0;
+        for (int j = 1; j <= Nm; ++j) b1[i][j] = b1[i][j] - mik * b1[Nm][j];
+    }
+    for (int j = 1; j <= Nm; ++j) b1[Nm][j] = b1[Nm][j] / temp;
+    for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) out[i * 9 + j] = b1[i + 1][j + 1];
+}
+
+// Reverse Cuthill-McKee order of one wing's segments on the graph "midpoints
+// within 7.1 lattice spacings" -- a superset of the pairs whose 6 x 6 support
+// boxes can overlap (|dx|, |dy| <= 5 spacings), invariant under the wing's
+// rigid motion.  Returns the order and the half bandwidth.
+static int rcm_order(const std::vector<double>& mx, const std::vector<double>& my, double spacing,
+                     std::vector<int>& order) {
+    const int n = (int)mx.size();
+    const double r2 = (7.1 * spacing) * (7.1 * spacing);
+    std::vector<std::vector<int>> adj(n);
+    for (int a = 0; a < n; ++a)
+        for (int b = a + 1; b < n; ++b) {
+            double dx = mx[a] - mx[b], dy = my[a] - my[b];
+            if (dx * dx + dy * dy <= r2) { adj[a].push_back(b); adj[b].push_back(a); }
+        }
+    std::vector<int> deg(n);
+    for (int a = 0; a < n; ++a) deg[a] = (int)adj[a].size();
+    std::vector<char> seen(n, 0);
+    std::vector<int> cm;
+    cm.reserve(n);
+    while ((int)cm.size() < n) {
+        int start = -1;
+        for (int a = 0; a < n; ++a)
+            if (!seen[a] && (start < 0 || deg[a] < deg[start])) start = a;
+        std::queue<int> q;
+        q.push(start);
+        seen[start] = 1;
+        while (!q.empty()) {
+            int a = q.front();
+            q.pop();
+            cm.push_back(a);
+            std::vector<int> nb;
+            for (int b : adj[a])
+                if (!seen[b]) { seen[b] = 1; nb.push_back(b); }
+            std::sort(nb.begin(), nb.end(), [&](int x, int y) { return deg[x] != deg[y] ? deg[x] < deg[y] : x < y; });
+            for (int b : nb) q.push(b);
+        }
+    }
+    order.assign(cm.rbegin(), cm.rend());
+    std::vector<int> pos(n);
+    for (int p = 0; p < n; ++p) pos[order[p]] = p;
+    int bw = 0;
+    for (int a = 0; a < n; ++a)
+        for (int b : adj[a]) bw = std::max(bw, std::abs(pos[a] - pos[b]));
+    return bw;
+}
+
+}  // namespace lbm
+
+using namespace lbm;
+
+struct LbmHandle {
+    LbmConfig cfg{};
+    std::string err;
+    DevState d{};
+    FusedConsts fc{};
+    int parity = 0;                 // fused path: 0 -> current planes in gA
+    float* planes[2] = {nullptr, nullptr};
+    cudaStream_t s_main = nullptr, s_ibm = nullptr;
+    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr;
+    std::vector<void*> allocs;
+    int64_t dev_bytes = 0;
+    int row_len = 4;
+    bool band_in_smem = false;
+    size_t ibm_smem = 0;
+    double* err_partial = nullptr;
+    double* err_out = nullptr;
+    bool fields_valid = false, err_valid = false;
+    // host copies
+    std::vector<double> xb0, yb0;
+    std::vector<int> ppw;
+    double* pinned = nullptr;       // small pinned staging buffer
+    size_t pinned_n = 0;
+    double* d_rowbuf = nullptr;     // device force rows
+    int rows_cap = 0;
+    // motion (mode.f90)
+    std::vector<double> table;
+    int64_t table_rows = 0;
+    int64_t motion_index = 1;
+    double* d_step_table = nullptr;
+    double* d_stream = nullptr;     // start row then target row
+    int32_t status_seen = 0;
+    // phase timers
+    bool timing = false;
+    std::vector<cudaEvent_t> evpool;
+    size_t evused = 0;
+    std::vector<std::pair<int, std::pair<size_t, size_t>>> marks;   // phase, (start ev, stop ev)
+    double phase_ms[4] = {0, 0, 0, 0};
+    long long timed_steps = 0;
+};
+
+namespace {
+
+int fail(LbmHandle* h, const std::string& msg) {
+    if (h) h->err = msg;
+    return -1;
+}
+
+int cuda_fail(LbmHandle* h, cudaError_t e, const char* where) {
+    return fail(h, std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);     \
+    } while (0)
+
+template <class T>
+int dalloc(LbmHandle* h, T** p, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+    h->allocs.push_back(*p);
+    h->dev_bytes += (int64_t)bytes;
+    return 0;
+}
+
+DevState current(const LbmHandle* h) {
+    DevState d = h->d;
+    if (d.precision != 0) {
+        d.gA = h->planes[h->parity];
+        d.gB = h->planes[1 - h->parity];
+    }
+    return d;
+}
+
+// interpolate_motion_row / lookup_motion_row (mode.f90:327-386)
+void lookup_motion_row(LbmHandle* h, double target, double* row) {
+    const int nc = 1 + 9 * h->cfg.wing_count;
+    const double tol = 1.0e-12;
+    const int64_t np = h->table_rows;
+    const double* T = h->table.data();
+    auto rowp = [&](int64_t i) { return T + (size_t)(i - 1) * nc; };
+    if (target <= rowp(1)[0] + tol) {
+        h->motion_index = 1;
+        std::memcpy(row, rowp(1), sizeof(double) * nc);
+        row[0] = target;
+        return;
+    }
+    if (target >= rowp(np)[0] - tol) {
+        h->motion_index = np;
+        std::memcpy(row, rowp(np), sizeof(double) * nc);
+        row[0] = target;
+        return;
+    }
+    h->motion_index = std::max<int64_t>(1, std::min<int64_t>(h->motion_index, np - 1));
+    while (h->motion_index > 1 && target <= rowp(h->motion_index)[0] + tol) h->motion_index -= 1;
+    while (h->motion_index < np - 1 && target > rowp(h->motion_index + 1)[0] + tol) h->motion_index += 1;
+    const double* r1 = rowp(h->motion_index);
+    const double* r2 = rowp(h->motion_index + 1);
+    double t1 = r1[0], t2 = r2[0], dt = t2 - t1;
+    if (std::fabs(dt) <= 1.0e-14) {
+        std::memcpy(row, r2, sizeof(double) * nc);
+        row[0] = target;
+        return;
+    }
+    double ratio = (target - t1) / dt;
+    ratio = std::min(std::max(ratio, 0.0), 1.0);
+    for (int c = 0; c < nc; ++c) row[c] = r1[c] + ratio * (r2[c] - r1[c]);
+    row[0] = target;
+}
+
+double smooth_r(double x) {
+    if (x < 0.0) return 0.0;
+    if (x <= 1.0) return 0.5 * x * x + (std::cos(2.0 * PAI * x) - 1.0) / (4.0 * PAI * PAI);
+    return x - 0.5;
+}
+double smooth_h(double x) {
+    if (x < 0.0) return 0.0;
+    if (x <= 1.0) return x - std::sin(2.0 * PAI * x) / (2.0 * PAI);
+    return 1.0;
+}
+double smooth_d(double x) {
+    if (x >= 0.0 && x <= 1.0) return 1.0 - std::cos(2.0 * PAI * x);
+    return 0.0;
+}
+void triplet(double s0, double v0, double v1, double dt, double lt, double* s, double* v, double* a) {
+    double dv = v1 - v0;
+    if (dt <= 1.0e-14) {
+        *s = (v0 + dv) * lt + s0;
+        *v = v0 + dv;
+        *a = 0.0;
+        return;
+    }
+    double x = lt / dt;
+    *s = dv * dt * smooth_r(x) + v0 * lt + s0;
+    *v = dv * smooth_h(x) + v0;
+    *a = dv / dt * smooth_d(x);
+}
+
+int init_state(LbmHandle* h) {
+    DevState d = current(h);
+    const size_t N = (size_t)d.plane;
+    if (d.precision == 0) {
+        // f = f0 = feq(1, UU, 0); rho = 1, u = u0 = UU, v = 0, pre = 1/3 (solution.f90:44-61)
+        std::vector<double> fe(9), buf(N);
+        for (int k = 0; k < 9; ++k) {
+            double eu = (double)ex(k) * d.uu + (double)ey(k) * 0.0;
+            double utwo = d.uu * d.uu + 0.0 * 0.0;
+            fe[k] = weight(k) * 1.0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * utwo);
+        }
+        for (int k = 0; k < 9; ++k) {
+            std::fill(buf.begin(), buf.end(), fe[k]);
+            CK(cudaMemcpy(d.f + k * N, buf.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(d.f0 + k * N, buf.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        auto fill = [&](double* p, double v) -> int {
+            std::fill(buf.begin(), buf.end(), v);
+            CK(cudaMemcpy(p, buf.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+            return 0;
+        };
+        if (fill(d.rho, 1.0) || fill(d.u, d.uu) || fill(d.u0, d.uu) || fill(d.v, 0.0) || fill(d.v0, 0.0) ||
+            fill(d.pre, 1.0 / 3.0) || fill(d.gfx, 0.0) || fill(d.gfy, 0.0))
+            return -1;
+    } else {
+        h->parity = 0;
+        d = current(h);
+        launch_fused_init(d, h->s_main);
+        CK(cudaGetLastError());
+    }
+    std::vector<int> em(N, BAND_EMPTY);
+    CK(cudaMemcpy(d.band_map, em.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.band_n, 0, 2 * sizeof(int)));
+    CK(cudaMemset(d.sum_row, 0, sizeof(double) * h->row_len));
+    CK(cudaMemset(d.sample_count, 0, sizeof(int)));
+    CK(cudaMemset(d.status, 0, sizeof(int)));
+    CK(cudaMemset(d.rel_pos, 0, sizeof(double) * std::max(1, d.wing_count)));
+    long long one = 1;
+    CK(cudaMemcpy(d.cycle, &one, sizeof(long long), cudaMemcpyHostToDevice));
+    h->d.movenum = 0;
+    h->fields_valid = false;
+    h->err_valid = false;
+    CK(cudaDeviceSynchronize());
+    return 0;
+}
+
+int ensure_rows(LbmHandle* h, int64_t n) {
+    if (n <= h->rows_cap) return 0;
+    if (h->d_rowbuf) {
+        cudaFree(h->d_rowbuf);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_rowbuf), h->allocs.end());
+        h->dev_bytes -= (int64_t)h->rows_cap * h->row_len * sizeof(double);
+    }
+    int cap = (int)std::max<int64_t>(n, 1024);
+    if (dalloc(h, &h->d_rowbuf, (size_t)cap * h->row_len)) return -1;
+    h->rows_cap = cap;
+    h->d.force_rows = h->d_rowbuf;
+    h->d.force_rows_cap = cap;
+    return 0;
+}
+
+int check_status(LbmHandle* h) {
+    int st = 0;
+    CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
+    h->status_seen |= st;
+    const int fatal = ST_BAND_OVERFLOW | ST_COVER_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION;
+    if (st & fatal) {
+        std::string m = "immersed boundary:";
+        if (st & ST_BAND_OVERFLOW) m += " band capacity exceeded;";
+        if (st & ST_COVER_OVERFLOW) m += " a band node is covered by too many segments;";
+        if (st & ST_BOX_OUTSIDE) m += " a wing's support box left the lattice;";
+        if (st & ST_MOTION) m += " no motion rows loaded;";
+        return fail(h, m);
+    }
+    return 0;
+}
+
+// Event marks around one phase when the phase timers are on.
+size_t next_event(LbmHandle* h) {
+    if (h->evused == h->evpool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->evpool.push_back(e);
+    }
+    return h->evused++;
+}
+struct PhaseMark {
+    LbmHandle* h;
+    int phase;
+    cudaStream_t st;
+    size_t a = 0;
+    PhaseMark(LbmHandle* h_, int p, cudaStream_t s) : h(h_), phase(p), st(s) {
+        if (h->timing) { a = next_event(h); cudaEventRecord(h->evpool[a], st); }
+    }
+    ~PhaseMark() {
+        if (!h->timing) return;
+        size_t b = next_event(h);
+        cudaEventRecord(h->evpool[b], st);
+        h->marks.push_back({phase, {a, b}});
+    }
+};
+
+void collect_phase_times(LbmHandle* h) {
+    for (auto& m : h->marks) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->evpool[m.second.first], h->evpool[m.second.second]) == cudaSuccess)
+            h->phase_ms[m.first] += ms;
+    }
+    h->marks.clear();
+    h->evused = 0;
+}
+
+// One evolution step (solution.f90:272-422) on the current parity.
+void enqueue_step(LbmHandle* h, bool fields) {
+    DevState d = current(h);
+    if (d.precision == 0) {
+        {
+            PhaseMark pm(h, 0, h->s_main);
+            launch_ibm_band(d, h->s_main);             // mode + move_boundary (:292-299)
+        }
+        {
+            PhaseMark pm(h, 1, h->s_main);
+            launch_plain_stream(d, h->s_main);         // streaming (:318)
+            launch_plain_moments(d, h->s_main);        // physical_variables (:321)
+        }
+        {
+            PhaseMark pm(h, 0, h->s_main);
+            launch_ibm_solve(d, h->ibm_smem, h->band_in_smem, h->s_main);  // immersed_boundary_wu (:325)
+        }
+        {
+            PhaseMark pm(h, 1, h->s_main);
+            launch_plain_collide(d, h->s_main);        // colission (:328)
+        }
+        {
+            PhaseMark pm(h, 3, h->s_main);
+            launch_outer_bc(d, h->s_main);             // boundary_condition1 (:420)
+        }
+        launch_step_advance(d, h->s_main);
+    } else {
+        // the IBM block overlaps the bulk kernel; both read only the current planes
+        cudaEventRecord(h->ev_main, h->s_main);
+        cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
+        {
+            PhaseMark pm(h, 0, h->s_ibm);
+            launch_ibm_full(d, h->ibm_smem, h->band_in_smem, h->s_ibm);
+        }
+        cudaEventRecord(h->ev_ibm, h->s_ibm);
+        {
+            PhaseMark pm(h, 1, h->s_main);
+            launch_fused_bulk(d, h->fc, fields, h->s_main);
+        }
+        cudaStreamWaitEvent(h->s_main, h->ev_ibm, 0);
+        {
+            PhaseMark pm(h, 2, h->s_main);
+            launch_fused_band(d, fields, h->s_main);
+        }
+        {
+            PhaseMark pm(h, 3, h->s_main);
+            launch_outer_bc(d, h->s_main);
+        }
+        launch_step_advance(d, h->s_main);
+        h->parity = 1 - h->parity;
+    }
+    if (h->timing) h->timed_steps += 1;
+}
+
+int copy_pitched_out(LbmHandle* h, const double* src, double* dst) {
+    const DevState& d = h->d;
+    CK(cudaMemcpy2D(dst, sizeof(double) * d.nx, src, sizeof(double) * d.pitch, sizeof(double) * d.nx, d.ny,
+                    cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+void lbm_config_default(LbmConfig* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->nx = 4001; c->ny = 2001; c->scale = 0.01; c->uu = 0.01; c->re = 500.0;
+    c->ox = -20.0; c->oy = -10.0;
+    const double s[9] = {0.0, 1.1, 1.05, 0.0, 1.2, 0.0, 1.2, 0.0, 0.0};
+    for (int k = 0; k < 9; ++k) c->s[k] = s[k];
+    c->wing_count = 2; c->wing_x_origin = 0.0; c->wing_x_spacing = 1.5; c->wing_y_origin = 0.5;
+    c->motion_source = LBM_MOTION_FILE; c->precision = LBM_PRECISION_FP64; c->device = 0;
+}
+
+int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* points_per_wing, LbmHandle** out) {
+    if (!out) return -1;
+    *out = nullptr;
+    LbmHandle* h = new LbmHandle();
+    *out = h;
+    if (!cfg) return fail(h, "null config");
+    h->cfg = *cfg;
+    const LbmConfig& c = *cfg;
+    if (c.nx < 6 || c.ny < 6) return fail(h, "lattice must be at least 6 x 6 nodes");
+    if (!(c.scale > 0.0) || !(c.uu > 0.0) || !(c.re > 0.0)) return fail(h, "scale, uu and re must be positive");
+    if (c.wing_count < 0 || c.wing_count > 16) return fail(h, "wing_count must be in [0, 16]");
+    if (c.precision != LBM_PRECISION_FP64 && c.precision != LBM_PRECISION_FP32)
+        return fail(h, "unknown precision");
+    if (c.motion_source != LBM_MOTION_FILE && c.motion_source != LBM_MOTION_STREAM)
+        return fail(h, "unknown motion source");
+    if (c.precision == LBM_PRECISION_FP32 && (c.s[0] != 0.0 || c.s[3] != 0.0 || c.s[5] != 0.0))
+        return fail(h, "the fused path relaxes only the non-conserved moments (s[0], s[3], s[5] must be 0)");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (c.device < 0 || c.device >= ndev) return fail(h, "CUDA device not available");
+    CK(cudaSetDevice(c.device));
+
+    DevState& d = h->d;
+    d.nx = c.nx; d.ny = c.ny;
+    d.pitch = (c.nx + 31) / 32 * 32;
+    d.plane = (long long)d.pitch * c.ny;
+    d.scale = c.scale; d.uu = c.uu; d.ox = c.ox; d.oy = c.oy;
+    // ini_mesh.f90:30-31, 59-67
+    const double niu = c.uu * (1.0 / c.scale) / c.re;
+    const double tau = 3.0 * niu + 0.5;
+    for (int k = 0; k < 9; ++k) d.s[k] = c.s[k];
+    if (d.s[7] <= 0.0) d.s[7] = 1.0 / tau;
+    if (d.s[8] <= 0.0) d.s[8] = 1.0 / tau;
+    gauss_jordan_inverse(d.minv);
+    d.precision = c.precision;
+    d.wing_count = c.wing_count;
+    d.wing_x_origin = c.wing_x_origin; d.wing_x_spacing = c.wing_x_spacing; d.wing_y_origin = c.wing_y_origin;
+    d.xc = c.xc; d.yc = c.yc;
+    d.motion_source = c.motion_source;
+    d.ncol = 1 + 9 * c.wing_count;
+    h->row_len = 4 + 12 * c.wing_count;
+
+    // geometry (airfoil.f90:207-242)
+    const int W = c.wing_count;
+    std::vector<int> pstart(W), sstart(W), npts(W), segw;
+    int np = 0, ns = 0;
+    for (int w = 0; w < W; ++w) {
+        if (!points_per_wing || points_per_wing[w] < 3) return fail(h, "each wing needs at least 3 points");
+        pstart[w] = np; sstart[w] = ns; npts[w] = points_per_wing[w];
+        np += points_per_wing[w];
+        ns += points_per_wing[w] - 1;
+        for (int k = 0; k < points_per_wing[w] - 1; ++k) segw.push_back(w);
+    }
+    if (W > 0 && !markers_xy) return fail(h, "markers_xy is null");
+    d.npts = np; d.nseg = ns;
+    h->xb0.resize(np); h->yb0.resize(np);
+    for (int p = 0; p < np; ++p) {
+        h->xb0[p] = markers_xy[2 * p] + (c.xc - 0.0);
+        h->yb0[p] = markers_xy[2 * p + 1] + (c.yc - 0.0);
+    }
+    // RCM order and half bandwidth per wing
+    std::vector<int> perm(ns), bw(W);
+    std::vector<long long> lofs(W);
+    long long ltot = 0;
+    for (int w = 0; w < W; ++w) {
+        const int nw = npts[w] - 1;
+        std::vector<double> mx(nw), my(nw);
+        for (int k = 0; k < nw; ++k) {
+            int p = pstart[w] + k;
+            mx[k] = 0.5 * (h->xb0[p + 1] + h->xb0[p]);
+            my[k] = 0.5 * (h->yb0[p + 1] + h->yb0[p]);
+        }
+        std::vector<int> ord;
+        bw[w] = rcm_order(mx, my, c.scale, ord);
+        for (int k = 0; k < nw; ++k) perm[sstart[w] + k] = sstart[w] + ord[k];
+        lofs[w] = ltot;
+        ltot += (long long)nw * (bw[w] + 1);
+    }
+
+    // allocations
+    const size_t N = (size_t)d.plane;
+    if (c.precision == LBM_PRECISION_FP64) {
+        if (dalloc(h, &d.f, 9 * N) || dalloc(h, &d.f0, 9 * N) || dalloc(h, &d.rho, N) || dalloc(h, &d.u, N) ||
+            dalloc(h, &d.v, N) || dalloc(h, &d.u0, N) || dalloc(h, &d.v0, N) || dalloc(h, &d.pre, N) ||
+            dalloc(h, &d.gfx, N) || dalloc(h, &d.gfy, N))
+            return -1;
+    } else {
+        if (dalloc(h, &h->planes[0], 9 * N) || dalloc(h, &h->planes[1], 9 * N) ||
+            dalloc(h, &d.edge_f0, 9 * (size_t)(2 * c.nx + 2 * c.ny)))
+            return -1;
+    }
+    if (dalloc(h, &d.band_map, N)) return -1;
+    d.band_cap = std::max(64, BOX_SLOTS * ns);
+    const int cap = d.band_cap;
+    int* band_n = nullptr;
+    if (dalloc(h, &band_n, 2) || dalloc(h, &d.band_ij, 2 * (size_t)cap) || dalloc(h, &d.band_wing, cap) ||
+        dalloc(h, &d.band_rho, cap) || dalloc(h, &d.band_us, cap) || dalloc(h, &d.band_vs, cap) ||
+        dalloc(h, &d.band_du, cap) || dalloc(h, &d.band_dv, cap) || dalloc(h, &d.cover_n, cap) ||
+        dalloc(h, &d.cover_list, (size_t)cap * MAX_COVER))
+        return -1;
+    d.band_n = band_n;
+    int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr;
+    long long* dlofs = nullptr;
+    double *xb0 = nullptr, *yb0 = nullptr;
+    const size_t nsz = std::max(1, ns), npz = std::max(1, np), wz = std::max(1, W);
+    if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
+        dalloc(h, &xb0, npz) || dalloc(h, &yb0, npz) || dalloc(h, &d.xb1, npz) || dalloc(h, &d.yb1, npz) ||
+        dalloc(h, &d.xb2, nsz) || dalloc(h, &d.yb2, nsz) || dalloc(h, &d.box, 4 * nsz) ||
+        dalloc(h, &d.claim_cnt, nsz + 1) || dalloc(h, &d.pw, nsz * BOX_SLOTS) || dalloc(h, &d.pb, nsz * BOX_SLOTS) ||
+        dalloc(h, &d.rx, nsz) || dalloc(h, &d.ry, nsz) || dalloc(h, &d.qx, nsz) || dalloc(h, &d.qy, nsz) ||
+        dalloc(h, &d.px, nsz) || dalloc(h, &d.py, nsz) || dalloc(h, &d.zx, nsz) || dalloc(h, &d.zy, nsz) ||
+        dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
+        dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &d.wm, wz) ||
+        dalloc(h, &d.rel_pos, wz) || dalloc(h, &d.cycle, 1) || dalloc(h, &d.row_index, 1) ||
+        dalloc(h, &d.sum_row, (size_t)h->row_len) || dalloc(h, &d.sample_count, 1) || dalloc(h, &d.status, 1) ||
+        dalloc(h, &d.wing_fm, 3 * wz) || dalloc(h, &d.ibm_resid, 2) || dalloc(h, &d.stream_start, (size_t)d.ncol) ||
+        dalloc(h, &d.stream_target, (size_t)d.ncol))
+        return -1;
+    if (dalloc(h, &h->err_partial, 2 * (size_t)err_partial_count()) || dalloc(h, &h->err_out, 1)) return -1;
+    if (W > 0) {
+        CK(cudaMemcpy(pst, pstart.data(), W * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(sst, sstart.data(), W * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(npw, npts.data(), W * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(sgw, segw.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(xb0, h->xb0.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(yb0, h->yb0.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dperm, perm.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dbw, bw.data(), W * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dlofs, lofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
+    }
+    d.wing_pstart = pst; d.wing_sstart = sst; d.wing_npts = npw; d.seg_wing = sgw;
+    d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs;
+    h->ppw.assign(npts.begin(), npts.end());
+    // banded factor storage: shared memory when it fits
+    const size_t lbytes = (size_t)ltot * sizeof(double);
+    h->band_in_smem = lbytes <= 160 * 1024;
+    h->ibm_smem = h->band_in_smem ? lbytes : 0;
+    if (h->band_in_smem && h->ibm_smem > 0) CK(ibm_set_smem_limit(h->ibm_smem));
+    if (ensure_rows(h, 1024)) return -1;
+    CK(cudaStreamCreateWithFlags(&h->s_main, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->s_ibm, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->ev_ibm, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->ev_main, cudaEventDisableTiming));
+    CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
+    h->pinned_n = 4096;
+    if (c.precision != LBM_PRECISION_FP64) h->fc = fused_consts(d);
+    if (init_state(h)) return -1;
+    return 0;
+}
+
+int lbm_reset(LbmHandle* h) {
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaDeviceSynchronize());
+    return init_state(h);
+}
+
+int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_t ncols) {
+    if (!h) return -1;
+    const int nc = 1 + 9 * h->cfg.wing_count;
+    if (ncols != nc) return fail(h, "motion table needs 1 + 9*wing_count columns");
+    if (nrows < 1 || !rows) return fail(h, "motion table is empty");
+    for (int64_t i = 1; i < nrows; ++i)
+        if (rows[i * nc] < rows[(i - 1) * nc]) return fail(h, "motion table times must be non-decreasing");
+    h->table.assign(rows, rows + (size_t)nrows * nc);
+    h->table_rows = nrows;
+    h->motion_index = 1;
+    // build_motion_step_table (mode.f90:388-412)
+    const double dt = h->cfg.scale * h->cfg.uu;
+    const double end_time = h->table[(size_t)(nrows - 1) * nc];
+    const int64_t steps = (int64_t)((end_time + 1.0e-12) / dt) + 1;
+    std::vector<double> st((size_t)steps * nc);
+    for (int64_t i = 1; i <= steps; ++i) lookup_motion_row(h, (double)(i - 1) * dt, &st[(size_t)(i - 1) * nc]);
+    CK(cudaSetDevice(h->cfg.device));
+    if (h->d_step_table) {
+        cudaFree(h->d_step_table);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_step_table), h->allocs.end());
+    }
+    if (dalloc(h, &h->d_step_table, st.size())) return -1;
+    CK(cudaMemcpy(h->d_step_table, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->d.step_table = h->d_step_table;
+    h->d.step_rows = steps;
+    h->d.motion_dt = dt;
+    return 0;
+}
+
+int lbm_set_stream_rows(LbmHandle* h, const double* start_row, const double* target_row) {
+    if (!h || !start_row || !target_row) return -1;
+    const int nc = h->d.ncol;
+    CK(cudaSetDevice(h->cfg.device));
+    std::memcpy(h->pinned, start_row, nc * sizeof(double));
+    std::memcpy(h->pinned + nc, target_row, nc * sizeof(double));
+    CK(cudaMemcpyAsync(h->d.stream_start, h->pinned, nc * sizeof(double), cudaMemcpyHostToDevice, h->s_main));
+    CK(cudaMemcpyAsync(h->d.stream_target, h->pinned + nc, nc * sizeof(double), cudaMemcpyHostToDevice, h->s_main));
+    CK(cudaStreamSynchronize(h->s_main));
+    return 0;
+}
+
+int lbm_build_stream_target_row(const LbmHandle* h, const double* start_row, double target_time,
+                                const double* delta_row, double* target_row) {
+    if (!h) return -1;
+    const double dt = target_time - start_row[0];
+    if (dt < -1.0e-12) return -2;
+    const int nc = 1 + 9 * h->cfg.wing_count;
+    std::memcpy(target_row, start_row, nc * sizeof(double));
+    target_row[0] = target_time;
+    for (int w = 0; w < h->cfg.wing_count; ++w) {
+        const int col = 1 + 9 * w, dcol = 1 + 3 * w;
+        for (int t = 0; t < 3; ++t) {
+            const int cc = col + 3 * t;
+            triplet(start_row[cc], start_row[cc + 1], start_row[cc + 1] + delta_row[dcol + t], dt, std::max(dt, 0.0),
+                    &target_row[cc], &target_row[cc + 1], &target_row[cc + 2]);
+        }
+    }
+    return 0;
+}
+
+int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_rows, int32_t flags) {
+    if (!h) return -1;
+    if (n_steps < 0) return fail(h, "n_steps must be >= 0");
+    if (first_cycle < 1) return fail(h, "cycles start at 1");
+    if (h->d.motion_source == LBM_MOTION_FILE && h->d.step_rows <= 0 && h->cfg.wing_count > 0)
+        return fail(h, "no motion table loaded");
+    CK(cudaSetDevice(h->cfg.device));
+    if (ensure_rows(h, n_steps)) return -1;
+    long long init[2] = {(long long)first_cycle, 0};
+    CK(cudaMemcpyAsync(h->d.cycle, &init[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
+    CK(cudaMemcpyAsync(h->d.row_index, &init[1], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
+    CK(cudaStreamSynchronize(h->s_main));
+    const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
+    const bool want_err = (flags & LBM_STEP_ERR) != 0;
+    for (int64_t n = 0; n < n_steps; ++n) {
+        const bool last = n == n_steps - 1, second_last = n == n_steps - 2;
+        bool fields = false;
+        if (h->d.precision != 0 && ((want_fields && last) || (want_err && (last || second_last)))) {
+            // fused path: materialise rho, u, v for this step
+            if (!h->d.fo_rho) {
+                const size_t N = (size_t)h->d.plane;
+                if (dalloc(h, &h->d.fo_rho, N) || dalloc(h, &h->d.fo_u, N) || dalloc(h, &h->d.fo_v, N) ||
+                    dalloc(h, &h->d.fo_u0, N) || dalloc(h, &h->d.fo_v0, N))
+                    return -1;
+            }
+            if (want_err && last) {   // previous step's velocity becomes u0
+                std::swap(h->d.fo_u, h->d.fo_u0);
+                std::swap(h->d.fo_v, h->d.fo_v0);
+            }
+            fields = true;
+        }
+        enqueue_step(h, fields);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(h->s_main));
+    CK(cudaGetLastError());
+    if (h->timing) collect_phase_times(h);
+    if (force_rows && n_steps > 0)
+        CK(cudaMemcpy(force_rows, h->d_rowbuf, sizeof(double) * h->row_len * n_steps, cudaMemcpyDeviceToHost));
+    if (n_steps > 0) {
+        h->fields_valid = h->d.precision == 0 || want_fields || want_err;
+        h->err_valid = h->d.precision == 0 ? true : (want_err && n_steps >= 2);
+    }
+    return check_status(h);
+}
+
+int lbm_get_sums(LbmHandle* h, double* sum_row, int32_t* sample_count, int32_t* row_len) {
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    if (sum_row) CK(cudaMemcpy(sum_row, h->d.sum_row, sizeof(double) * h->row_len, cudaMemcpyDeviceToHost));
+    if (sample_count) CK(cudaMemcpy(sample_count, h->d.sample_count, sizeof(int), cudaMemcpyDeviceToHost));
+    if (row_len) *row_len = h->row_len;
+    return 0;
+}
+
+int lbm_reset_sums(LbmHandle* h) {
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemset(h->d.sum_row, 0, sizeof(double) * h->row_len));
+    CK(cudaMemset(h->d.sample_count, 0, sizeof(int)));
+    return 0;
+}
+
+int lbm_get_fields(LbmHandle* h, double* rho, double* u, double* v, double* pre) {
+    if (!h) return -1;
+    if (!h->fields_valid) return fail(h, "fields are not available: step with LBM_STEP_FIELDS first");
+    CK(cudaSetDevice(h->cfg.device));
+    const DevState& d = h->d;
+    if (d.precision == 0) {
+        if (rho && copy_pitched_out(h, d.rho, rho)) return -1;
+        if (u && copy_pitched_out(h, d.u, u)) return -1;
+        if (v && copy_pitched_out(h, d.v, v)) return -1;
+        if (pre && copy_pitched_out(h, d.pre, pre)) return -1;
+    } else {
+        if (rho && copy_pitched_out(h, d.fo_rho, rho)) return -1;
+        if (u && copy_pitched_out(h, d.fo_u, u)) return -1;
+        if (v && copy_pitched_out(h, d.fo_v, v)) return -1;
+        if (pre) {
+            // pre = rho/3 from physical_variables; border nodes keep the
+            // value of their never-updated f0 (the BC changes rho, not pre)
+            std::vector<double> r((size_t)d.nx * d.ny);
+            if (copy_pitched_out(h, d.fo_rho, r.data())) return -1;
+            for (size_t k = 0; k < r.size(); ++k) pre[k] = r[k] / 3.0;
+            std::vector<double> e(9 * (size_t)(2 * d.nx + 2 * d.ny));
+            CK(cudaMemcpy(e.data(), d.edge_f0, e.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            const size_t per = 2 * (size_t)d.nx + 2 * (size_t)d.ny;
+            auto border_pre = [&](size_t eidx) {
+                double s = 0.0;
+                for (int k = 0; k < 9; ++k) s = s + e[k * per + eidx];
+                return s / 3.0;
+            };
+            for (int j = 0; j < d.ny; ++j) {
+                pre[(size_t)j * d.nx] = border_pre(j);
+                pre[(size_t)j * d.nx + d.nx - 1] = border_pre(d.ny + j);
+            }
+            for (int i = 0; i < d.nx; ++i) {
+                pre[i] = border_pre(2 * (size_t)d.ny + i);
+                pre[(size_t)(d.ny - 1) * d.nx + i] = border_pre(2 * (size_t)d.ny + d.nx + i);
+            }
+        }
+    }
+    return 0;
+}
+
+int lbm_err(LbmHandle* h, double* err) {
+    if (!h || !err) return -1;
+    if (!h->err_valid) return fail(h, "err is not available: step at least twice with LBM_STEP_ERR first");
+    CK(cudaSetDevice(h->cfg.device));
+    launch_err(current(h), h->err_partial, h->err_out, h->s_main);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s_main));
+    CK(cudaMemcpy(err, h->err_out, sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int lbm_get_f(LbmHandle* h, double* f) {
+    if (!h || !f) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    const DevState d = current(h);
+    const size_t nn = (size_t)d.nx * d.ny;
+    if (d.precision == 0) {
+        for (int k = 0; k < 9; ++k) {
+            CK(cudaMemcpy2D(f + k * nn, sizeof(double) * d.nx, d.f + k * d.plane, sizeof(double) * d.pitch,
+                            sizeof(double) * d.nx, d.ny, cudaMemcpyDeviceToHost));
+        }
+        return 0;
+    }
+    double* tmp = nullptr;
+    CK(cudaMalloc((void**)&tmp, 9 * nn * sizeof(double)));
+    launch_fused_export(d, d.gA, tmp, h->s_main);
+    cudaError_t e = cudaStreamSynchronize(h->s_main);
+    if (e == cudaSuccess) e = cudaMemcpy(f, tmp, 9 * nn * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lbm_get_f");
+    return 0;
+}
+
+int lbm_set_f(LbmHandle* h, const double* f) {
+    if (!h || !f) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    const DevState d = current(h);
+    const size_t nn = (size_t)d.nx * d.ny;
+    if (d.precision == 0) {
+        for (int k = 0; k < 9; ++k)
+            CK(cudaMemcpy2D(d.f + k * d.plane, sizeof(double) * d.pitch, f + k * nn, sizeof(double) * d.nx,
+                            sizeof(double) * d.nx, d.ny, cudaMemcpyHostToDevice));
+        return 0;
+    }
+    double* tmp = nullptr;
+    CK(cudaMalloc((void**)&tmp, 9 * nn * sizeof(double)));
+    cudaError_t e = cudaMemcpy(tmp, f, 9 * nn * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_fused_import(d, tmp, d.gA, h->s_main);
+        e = cudaStreamSynchronize(h->s_main);
+    }
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(h, e, "lbm_set_f");
+    return 0;
+}
+
+int lbm_get_band(LbmHandle* h, int32_t* n, int32_t* ij_wing, int32_t cap) {
+    if (!h || !n) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    int nb = 0;
+    CK(cudaMemcpy(&nb, h->d.band_n, sizeof(int), cudaMemcpyDeviceToHost));
+    *n = nb;
+    if (!ij_wing) return 0;
+    const int m = std::min(nb, cap);
+    std::vector<int> ij(2 * (size_t)std::max(m, 1)), w(std::max(m, 1));
+    if (m > 0) {
+        CK(cudaMemcpy(ij.data(), h->d.band_ij, 2 * m * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.data(), h->d.band_wing, m * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    for (int b = 0; b < m; ++b) {
+        ij_wing[3 * b] = ij[2 * b] + 1;
+        ij_wing[3 * b + 1] = ij[2 * b + 1] + 1;
+        ij_wing[3 * b + 2] = w[b] + 1;
+    }
+    return nb <= cap ? 0 : fail(h, "band larger than cap");
+}
+
+int lbm_get_markers(LbmHandle* h, double* xb1, double* yb1, double* xb2, double* yb2) {
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    const DevState& d = h->d;
+    if (xb1 && d.npts) CK(cudaMemcpy(xb1, d.xb1, d.npts * sizeof(double), cudaMemcpyDeviceToHost));
+    if (yb1 && d.npts) CK(cudaMemcpy(yb1, d.yb1, d.npts * sizeof(double), cudaMemcpyDeviceToHost));
+    if (xb2 && d.nseg) CK(cudaMemcpy(xb2, d.xb2, d.nseg * sizeof(double), cudaMemcpyDeviceToHost));
+    if (yb2 && d.nseg) CK(cudaMemcpy(yb2, d.yb2, d.nseg * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int lbm_move_mesh(LbmHandle* h, int32_t dr) {
+    if (!h) return -1;
+    if (dr != 1 && dr != -1) return fail(h, "dr must be +1 or -1");
+    CK(cudaSetDevice(h->cfg.device));
+    if (h->d.precision == 0) {
+        launch_plain_shift(h->d, dr, h->s_main);
+    } else {
+        launch_fused_shift(current(h), dr, h->s_main);
+        h->parity = 1 - h->parity;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s_main));
+    h->d.movenum += dr;
+    return 0;
+}
+
+int lbm_ibm_residual(LbmHandle* h, double* res) {
+    if (!h || !res) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    double r[2];
+    CK(cudaMemcpy(r, h->d.ibm_resid, sizeof(r), cudaMemcpyDeviceToHost));
+    *res = std::sqrt(r[0]) / (std::sqrt(r[1]) + 1e-300);
+    return 0;
+}
+
+int lbm_status(LbmHandle* h, int32_t* bits) {
+    if (!h || !bits) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    int st = 0;
+    CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(h->d.status, 0, sizeof(int)));
+    *bits = st | h->status_seen;
+    h->status_seen = 0;
+    return 0;
+}
+
+int lbm_set_timing(LbmHandle* h, int32_t enable) {
+    if (!h) return -1;
+    h->timing = enable != 0;
+    for (double& v : h->phase_ms) v = 0.0;
+    h->timed_steps = 0;
+    h->marks.clear();
+    h->evused = 0;
+    return 0;
+}
+
+int lbm_get_phase_times(LbmHandle* h, double* out5) {
+    if (!h || !out5) return -1;
+    for (int k = 0; k < 4; ++k) out5[k] = h->phase_ms[k];
+    out5[4] = (double)h->timed_steps;
+    return 0;
+}
+
+void* lbm_stream(LbmHandle* h) { return h ? (void*)h->s_main : nullptr; }
+
+int64_t lbm_device_bytes(const LbmHandle* h) { return h ? h->dev_bytes : 0; }
+
+const char* lbm_last_error(const LbmHandle* h) { return h ? h->err.c_str() : "null handle"; }
+
+void lbm_destroy(LbmHandle* h) {
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    cudaDeviceSynchronize();
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->s_main) cudaStreamDestroy(h->s_main);
+    if (h->s_ibm) cudaStreamDestroy(h->s_ibm);
+    if (h->ev_ibm) cudaEventDestroy(h->ev_ibm);
+    if (h->ev_main) cudaEventDestroy(h->ev_main);
+    for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+    delete h;
+}
+
+}  // extern "C"
