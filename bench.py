@@ -209,7 +209,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     prec = api.PRECISION_FP32 if args.precision == "fp32" else api.PRECISION_FP64
     K, Wm = args.steps, max(3, args.warmup)
-    ep = workload(args.workload, Wm + 2 * K + 4)
+    ep = workload(args.workload, Wm + K + min(K, 100) + SEG + 4)
     nodes = ep.nx * ep.ny
     sim = api.Simulation(ep, prec, device=local)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
@@ -219,7 +219,6 @@ def run_ours(args):
     # timed region: K steps, device time by CUDA events on the library stream
     barrier(world)
     torch.cuda.synchronize()
-    sim.set_timing(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
         e0.record(stream)
@@ -227,6 +226,11 @@ def run_ours(args):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    # phase breakdown and the bulk kernel's launch time: a second pass with
+    # CUDA events around every phase (kernels launched directly)
+    KP = min(K, 100)
+    sim.set_timing(True)
+    sim.step(KP, first_cycle=Wm + K + 1, rows=False)
     phases = sim.phase_times()
     sim.set_timing(False)
     ms_max = allmax(ms, world)
@@ -289,7 +293,8 @@ def run_ours(args):
                        "storage": "fp32 deviation" if prec == api.PRECISION_FP32 else "fp64 plain",
                        "l2": "planes 2 x %.0f MB exceed the 126 MB L2; no flush" % (9 * ep.nx * ep.ny * (4 if prec else 8) / 1e6),
                        "parallelism": f"{world} independent episodes"},
-            "phases_ms_per_step": {k: v / max(1, phases["steps"]) for k, v in phases.items() if k != "steps"},
+            "phases_ms_per_step": {k: v / max(1, phases["steps"]) for k, v in phases.items()
+                                   if k != "steps"},
             "roofline": roof,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "segment_steps": SEG},

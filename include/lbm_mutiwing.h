@@ -41,6 +41,9 @@ extern "C" {
 #define LBM_MOTION_FILE 1      /* per-step table built from motion_params.dat rows */
 #define LBM_MOTION_STREAM 2    /* online smooth ramp between two rows (ZeroMQ STEP) */
 
+/* LbmConfig.flags */
+#define LBM_FLAG_NO_GRAPHS 1   /* launch every kernel directly (no CUDA graph replay) */
+
 /* lbm_step flags */
 #define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */
 #define LBM_STEP_ERR 2         /* last two steps keep u, u0 so lbm_err is available */
@@ -64,7 +67,8 @@ typedef struct LbmConfig {
     int32_t motion_source;       /* LBM_MOTION_FILE or LBM_MOTION_STREAM */
     int32_t precision;           /* LBM_PRECISION_* */
     int32_t device;              /* CUDA device ordinal */
-    int32_t reserved[7];
+    int32_t flags;               /* LBM_FLAG_* */
+    int32_t reserved[6];
 } LbmConfig;
 
 /* Fill cfg with the reference defaults: 4001x2001 lattice, scale 0.01,
@@ -139,11 +143,15 @@ int lbm_status(LbmHandle* h, int32_t* bits);
 /* Phase timers, the device-side counterpart of the reference's cpu_time
  * phase totals (main.f90:384-392, 443-456).  When enabled, every step records
  * CUDA events around its kernels; lbm_get_phase_times returns, in ms summed
- * over the timed steps: [0] marker/band/IBM, [1] collide-stream (bulk or
- * stream+moments+collide), [2] band re-collision, [3] far-field boundary,
- * [4] number of steps timed.  Enabling (or disabling) clears the totals. */
+ * over the timed steps: [0] move_boundary (markers and band), [1]
+ * collide-stream (bulk kernel, or stream + moments + collide), [2] band
+ * re-collision, [3] far-field boundary, [4] immersed-boundary right-hand
+ * side, substitution, spread and forces, [5] assembly and factorisation of
+ * the immersed-boundary system, and [6] the number of steps timed.  On the
+ * FP32 path phases 0, 3, 4 and 5 overlap phase 1.  Enabling (or disabling)
+ * clears the totals.  n is the length of out (at most 7 values are written). */
 int lbm_set_timing(LbmHandle* h, int32_t enable);
-int lbm_get_phase_times(LbmHandle* h, double* out5);
+int lbm_get_phase_times(LbmHandle* h, double* out, int32_t n);
 
 /* The CUDA stream (cudaStream_t) the handle's step kernels are ordered on,
  * for callers that record their own events around lbm_step. */

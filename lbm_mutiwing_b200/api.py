@@ -26,6 +26,7 @@ MOTION_FILE = 1
 MOTION_STREAM = 2
 STEP_FIELDS = 1
 STEP_ERR = 2
+FLAG_NO_GRAPHS = 1
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}
@@ -40,7 +41,8 @@ class LbmConfig(C.Structure):
                 ("wing_count", C.c_int32), ("wing_x_origin", C.c_double),
                 ("wing_x_spacing", C.c_double), ("wing_y_origin", C.c_double),
                 ("xc", C.c_double), ("yc", C.c_double), ("motion_source", C.c_int32),
-                ("precision", C.c_int32), ("device", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("precision", C.c_int32), ("device", C.c_int32), ("flags", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 # (name, restype, argtypes) of every exported entry point
@@ -65,7 +67,7 @@ SIGNATURES = [
     ("lbm_ibm_residual", C.c_int, [C.c_void_p, D]),
     ("lbm_status", C.c_int, [C.c_void_p, I32]),
     ("lbm_set_timing", C.c_int, [C.c_void_p, C.c_int32]),
-    ("lbm_get_phase_times", C.c_int, [C.c_void_p, D]),
+    ("lbm_get_phase_times", C.c_int, [C.c_void_p, D, C.c_int32]),
     ("lbm_stream", C.c_void_p, [C.c_void_p]),
     ("lbm_device_bytes", C.c_int64, [C.c_void_p]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
@@ -107,8 +109,9 @@ def default_s() -> list:
 
 
 def make_config(ep, precision: int = PRECISION_FP64, motion_source: int = MOTION_FILE,
-                device: int = 0, s: Optional[Sequence[float]] = None) -> LbmConfig:
+                device: int = 0, s: Optional[Sequence[float]] = None, graphs: bool = True) -> LbmConfig:
     cfg = LbmConfig()
+    cfg.flags = 0 if graphs else FLAG_NO_GRAPHS
     cfg.nx, cfg.ny = ep.nx, ep.ny
     cfg.scale, cfg.uu, cfg.re = ep.scale, ep.uu, ep.re
     cfg.ox, cfg.oy = ep.ox, ep.oy
@@ -128,10 +131,11 @@ class Simulation:
     """One episode resident on one GPU."""
 
     def __init__(self, ep, precision: int = PRECISION_FP64, motion_source: int = MOTION_FILE,
-                 device: int = 0, s: Optional[Sequence[float]] = None, load_motion: bool = True):
+                 device: int = 0, s: Optional[Sequence[float]] = None, load_motion: bool = True,
+                 graphs: bool = True):
         self.L = load_library()
         self.ep = ep
-        self.cfg = make_config(ep, precision, motion_source, device, s)
+        self.cfg = make_config(ep, precision, motion_source, device, s, graphs)
         self.nx, self.ny, self.W = ep.nx, ep.ny, ep.wing_count
         self.precision = precision
         self.row_len = 4 + 12 * self.W
@@ -266,10 +270,10 @@ class Simulation:
         self._check(self.L.lbm_set_timing(self.h, 1 if enable else 0))
 
     def phase_times(self) -> dict:
-        out = np.zeros(5)
-        self._check(self.L.lbm_get_phase_times(self.h, _dp(out)))
-        return {"ibm_ms": out[0], "collide_stream_ms": out[1], "band_ms": out[2], "bc_ms": out[3],
-                "steps": int(out[4])}
+        out = np.zeros(7)
+        self._check(self.L.lbm_get_phase_times(self.h, _dp(out), 7))
+        return {"move_boundary_ms": out[0], "collide_stream_ms": out[1], "band_ms": out[2],
+                "bc_ms": out[3], "ibm_solve_ms": out[4], "ibm_factor_ms": out[5], "steps": int(out[6])}
 
     def stream(self) -> int:
         return int(self.L.lbm_stream(self.h) or 0)

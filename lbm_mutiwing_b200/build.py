@@ -1,9 +1,10 @@
 """Builds the CUDA library liblbm_b200.so in-tree with nvcc for sm_100a.
 
-Translation units holding FP64 reference-order arithmetic (plain path, far
-field, immersed boundary) are compiled with -fmad=false so each multiply and
-add rounds separately, as the reference's source order prescribes; the fused
-FP32 kernel keeps fused multiply-adds.
+The translation unit holding the FP64 reference-order lattice arithmetic
+(plain path, far field) is compiled with -fmad=false so each multiply and add
+rounds separately, as the reference's source order prescribes; the immersed
+boundary unit spells out its few rounding-sensitive operations with
+intrinsics, and the fused FP32 kernel keeps fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -19,7 +20,7 @@ LIB = os.path.join(HERE, "liblbm_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
-NO_FMA = {"kernels_fp64.cu", "ibm.cu"}
+NO_FMA = {"kernels_fp64.cu"}
 SOURCES = ["lbm_api.cu", "kernels_fp64.cu", "kernels_fp32.cu", "ibm.cu"]
 
 

@@ -1,5 +1,5 @@
 // Implicit velocity-correction immersed boundary step (bc_num = 4), on the
-// device in FP64, one thread block per simulation.
+// device in FP64, as short kernels on two streams.
 //
 // Reference: move_boundary (airfoil.f90:244-338) and immersed_boundary_Wu
 // (boundary_condition.f90:1512-1736), with the motion lookup of mode.f90.
@@ -8,41 +8,71 @@
 // xx2 = xx1^T diag(arc_l), forms A = xx1 xx2 with cublasDgemm and solves
 // A c = ub - xx1 u* with cuSOLVER LU.  Because A = X X^T D and the spread is
 // du = X^T D c, the arc lengths cancel: du = X^T y with (X X^T) y = ub - X u*.
-// Here X is kept sparse (each segment's 6 x 6 support box), G = X X^T is
-// assembled in a per-wing banded layout after a reverse Cuthill-McKee
-// ordering fixed at set-up (rigid wings keep their pairwise distances), and
-// factored by a banded Cholesky, one warp per wing.
+// Here X is kept sparse: segment s touches only the nodes of its support box
+// (at most 6 x 6), and the smoothed delta kernel is a product
+// phi(rx) phi(ry), so a segment needs 6 + 6 kernel values (kx, ky) and
+//   G(a, c) = [sum_i kx_a(i) kx_c(i)] [sum_j ky_a(j) ky_c(j)]
+// over the common node columns i and rows j of the two boxes.  G is
+// assembled per wing in a banded layout after a reverse Cuthill-McKee
+// ordering fixed at set-up (rigid wings keep their pairwise distances) and
+// factored as L' D L'^T, panel by panel, one thread block per wing.  G
+// depends on the geometry only, so assembly and factorisation run on a side
+// stream while the band list and the right-hand side are built.
 //
-// Determinism: the band list is built in the reference's first-claimant
-// order (segment, then i, then j) from an atomicMin claim pass plus a prefix
-// sum; the spread sums each band node's contributions in ascending segment
-// order; force sums use a fixed reduction tree.  Results are identical from
-// run to run.
+// Kernels of one step (main chain | side chain):
+//   geometry   motion, markers, midpoints, support boxes, kernel values,
+//              clearing of the previous band             (move_boundary)
+//   claim      lowest segment index claims each box node   | assemble  G
+//   count      claims per segment                          | factor    L' D L'^T
+//   scan       band-list offsets, coupled-wing check       |
+//   list       band list in the reference's order (segment, i, j)
+//   ustar      u*, rho at band nodes; zeroed spread accumulators
+//   rhs        r = ub - X u* (one warp per segment)
+//   solve      forward and backward substitution (waits for the factor)
+//   spread     du = X^T y with fixed-point integer atomics
+//   finish     du, body force, per-block force partials
+//   forces     per-wing force and moment, force row
 //
-// Built with -fmad=false: the box scan compares node distances against 2.5
-// spacings with the reference's rounding.
+// Determinism: the band list is built in first-claimant order from an
+// atomicMin claim pass plus a prefix sum; the spread rounds every
+// contribution once to a 64-bit fixed-point number and adds integers
+// (associative, hence order-independent); all other sums use fixed trees.
+// Results are identical from run to run.
+//
+// The box scan compares node distances against 2.5 spacings: marker,
+// midpoint and node coordinates are formed with explicitly rounded
+// multiplies and adds in the reference's order so that band membership
+// matches it.
 #include <cstdio>
 
 #include "lbm_kernels.h"
 
 namespace lbm {
 
-constexpr int IBM_THREADS = 512;
-constexpr int IBM_WARPS = IBM_THREADS / 32;
 constexpr int MAX_WINGS = 16;
-
-int ibm_threads() { return IBM_THREADS; }
-
-struct IbmShared {
-    WingMotion wm[MAX_WINGS];
-    double xbase[MAX_WINGS], ybase[MAX_WINGS];
-    int scan[IBM_THREADS];
-    double red[IBM_WARPS][MAX_WINGS][3];
-    double fm[MAX_WINGS][3];
-    int nb;
-};
+constexpr int FACTOR_THREADS = 128;     // threads of a factorisation block
+constexpr int PANEL = IBM_PANEL;        // columns per factorisation panel
+constexpr int ROWS_PER_LANE = 3;        // register panel rows per lane: bw + PANEL <= 96
+constexpr int FINISH_THREADS = 256;
+constexpr int BORDER_GAP = 3;           // support boxes keep this many nodes off the border
 
 __device__ inline void set_status(const DevState& d, int bit) { atomicOr(d.status, bit); }
+
+// Exactly rounded FP64 steps for the marker and box arithmetic.
+__device__ inline double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ inline double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ inline double sub(double a, double b) { return __dsub_rn(a, b); }
+// node coordinate ox + scale * (i - 1) as the reference rounds it
+__device__ inline double node_x(double o, double scale, int i) { return add(o, mul(scale, (double)(i - 1))); }
+
+// 1/x from a single-precision seed and two Newton steps (relative error
+// below 1e-16 for the positive pivots met here).
+__device__ inline double fast_recip(double x) {
+    double r = (double)__frcp_rn((float)x);
+    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
+    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
+    return r;
+}
 
 // smooth ramp functions of the online motion (mode.f90:220-261)
 __device__ inline double smooth_r(double x) {
@@ -75,9 +105,15 @@ __device__ inline void triplet(double s0, double v0, double v1, double dt, doubl
     a = dv / dt * smooth_d(x);
 }
 
+__device__ inline double step_time(const DevState& d) {
+    return mul((double)(*d.cycle - 1), mul(d.scale, d.uu));   // solution.f90:292
+}
+
 // mode + apply_motion_row for wing w at the current cycle (mode.f90:451-471,
-// 180-218, 414-449).
-__device__ void wing_motion(const DevState& d, int w, double time, WingMotion& m) {
+// 180-218, 414-449) and update_body_extra_from_rel (mode.f90:473-495),
+// whose relative motion is zero unless rigid-body dynamics are enabled.
+__device__ WingMotion wing_motion(const DevState& d, int w) {
+    const double time = step_time(d);
     double v[9];
     if (d.motion_source == 2) {
         const double t1 = d.stream_start[0], t2 = d.stream_target[0], dt = t2 - t1;
@@ -96,6 +132,7 @@ __device__ void wing_motion(const DevState& d, int w, double time, WingMotion& m
         const double* row = d.step_table + (idx - 1) * d.ncol + 1 + 9 * w;
         for (int c = 0; c < 9; ++c) v[c] = row[c];
     }
+    WingMotion m;
     m.angle = v[0]; m.omega = v[1]; m.omgac = v[2];
     m.sa = v[3]; m.sau = v[4]; m.saac = v[5];
     m.sb = v[6]; m.sbv = v[7]; m.sbac = v[8];
@@ -103,6 +140,12 @@ __device__ void wing_motion(const DevState& d, int w, double time, WingMotion& m
         m.sa = m.sa - (d.wing_x_origin + (double)w * d.wing_x_spacing);
         m.sb = m.sb - d.wing_y_origin;
     }
+    double ap = 0.0;
+    for (int k = 0; k <= w; ++k) ap = add(ap, d.rel_pos[k]);
+    m.extra_v = 0.0;
+    m.extra_s = 0.0;
+    m.extra_pos = ap;
+    return m;
 }
 
 __device__ inline int wing_of_point(const DevState& d, int p) {
@@ -111,438 +154,619 @@ __device__ inline int wing_of_point(const DevState& d, int p) {
     return w;
 }
 
-// ------------------------------------------------------------------ phases
-// move_boundary: motion, markers, band rebuild.
-__device__ void phase_band(const DevState& d, IbmShared& sh) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const long long cycle = *d.cycle;
-    const double time = (double)(cycle - 1) * (d.scale * d.uu);
-    if (tid < d.wing_count) {
-        WingMotion m;
-        wing_motion(d, tid, time, m);
-        // update_body_extra_from_rel (mode.f90:473-495); relative motion is
-        // zero unless rigid-body dynamics are enabled.
-        double av = 0.0, as = 0.0, ap = 0.0;
-        for (int w = 0; w <= tid; ++w) { ap = ap + d.rel_pos[w]; }
-        m.extra_v = av; m.extra_s = as; m.extra_pos = ap;
-        sh.wm[tid] = m;
-        d.wm[tid] = m;
+// marker point p of wing w (airfoil.f90:260-264)
+__device__ inline void marker(const DevState& d, const WingMotion& m, int w, int p, double& x, double& y) {
+    double ca, sn;
+    sincos(m.angle, &sn, &ca);
+    x = add(mul(ca, d.xb0[p]), mul(sn, d.yb0[p]));
+    x = add(add(add(add(x, d.wing_x_origin), mul((double)w, d.wing_x_spacing)), m.sa), d.xc);
+    x = sub(add(x, m.extra_s / (1.0 / d.scale)), mul((double)d.movenum, d.scale));
+    y = add(-mul(sn, d.xb0[p]), mul(ca, d.yb0[p]));
+    y = add(add(add(y, d.wing_y_origin), m.sb), d.yc);
+}
+
+// ---------------------------------------------------------------- kernels
+// move_boundary part 1: markers, midpoints, support boxes (airfoil.f90:288-321),
+// separable delta values (boundary_condition.f90:1580-1603), and the clearing
+// of the previous band (airfoil.f90:276-284).  Twelve threads per segment:
+// thread (s, axis, k) scans its axis for the box and evaluates the kernel at
+// the box's k-th node column or row.
+__global__ void ibm_geometry_kernel(DevState d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < d.wing_count) d.wm[t] = wing_motion(d, t);
+    if (t < d.npts) {
+        const int w = wing_of_point(d, t);
+        const WingMotion m = wing_motion(d, w);
+        double x, y;
+        marker(d, m, w, t, x, y);
+        d.xb1[t] = x;
+        d.yb1[t] = y;
     }
-    if (tid == 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
-    __syncthreads();
-    // markers (airfoil.f90:254-265)
-    for (int p = tid; p < d.npts; p += nt) {
-        int w = wing_of_point(d, p);
-        const WingMotion& m = sh.wm[w];
-        double ca = cos(m.angle), sn = sin(m.angle);
-        d.xb1[p] = ca * d.xb0[p] + sn * d.yb0[p] + d.wing_x_origin + (double)w * d.wing_x_spacing + m.sa +
-                   d.xc + m.extra_s / (1.0 / d.scale) - (double)d.movenum * d.scale;
-        d.yb1[p] = -(sn * d.xb0[p]) + ca * d.yb0[p] + d.wing_y_origin + m.sb + d.yc;
+    if (t < d.nseg * 12) {
+        const int s = t / 12, q = t % 12, axis = q / 6, k = q % 6;
+        const int w = d.seg_wing[s];
+        const WingMotion m = wing_motion(d, w);
+        const int p = d.wing_pstart[w] + (s - d.wing_sstart[w]);
+        double xa, ya, xb, yb;
+        marker(d, m, w, p + 1, xb, yb);
+        marker(d, m, w, p, xa, ya);
+        const double c2 = axis == 0 ? mul(0.5, add(xb, xa)) : mul(0.5, add(yb, ya));
+        const double o = axis == 0 ? d.ox : d.oy;
+        const int n = axis == 0 ? d.nx : d.ny;
+        int lo = (int)(add((c2 - o) / d.scale, 1.0));
+        for (int i = lo; i >= 1; --i)
+            if (fabs((node_x(o, d.scale, i) - c2) / d.scale) > 2.5) { lo = i + 1; break; }
+        int hi = (int)(add((c2 - o) / d.scale, 1.0));
+        for (int i = hi; i <= n; ++i)
+            if (fabs((node_x(o, d.scale, i) - c2) / d.scale) > 2.5) { hi = i - 1; break; }
+        // the far-field boundary reads the moments of the first three rows
+        // and columns, which must stay outside every support box
+        if (lo < 1 + BORDER_GAP || hi > n - BORDER_GAP || hi - lo > 5 || hi < lo) {
+            if (k == 0) set_status(d, ST_BOX_OUTSIDE);
+            lo = 1; hi = 0;   // empty box
+        }
+        (axis == 0 ? d.kx : d.ky)[6 * s + k] =
+            (lo + k <= hi) ? delta_phi(fabs((node_x(o, d.scale, lo + k) - c2) / d.scale)) : 0.0;
+        if (k == 0) {
+            d.box[4 * s + 2 * axis] = lo;
+            d.box[4 * s + 2 * axis + 1] = hi;
+            (axis == 0 ? d.xb2 : d.yb2)[s] = c2;
+        }
     }
-    // clear the previous band (airfoil.f90:276-284)
-    const int nb_old = d.band_n[0];
-    for (int b = tid; b < nb_old; b += nt) {
-        int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
-        long long p = pidx(d, i, j);
+    if (t < d.band_n[0]) {
+        const long long p = pidx(d, d.band_ij[2 * t], d.band_ij[2 * t + 1]);
         d.band_map[p] = BAND_EMPTY;
         if (d.precision == 0) { d.gfx[p] = 0.0; d.gfy[p] = 0.0; }
     }
-    __syncthreads();
-    // midpoints (airfoil.f90:267-270) and support boxes (:288-321)
-    for (int s = tid; s < d.nseg; s += nt) {
-        int w = d.seg_wing[s];
-        int p = d.wing_pstart[w] + (s - d.wing_sstart[w]);
-        double x2 = 0.5 * (d.xb1[p + 1] + d.xb1[p]);
-        double y2 = 0.5 * (d.yb1[p + 1] + d.yb1[p]);
-        d.xb2[s] = x2;
-        d.yb2[s] = y2;
-        int i1 = (int)((x2 - d.ox) / d.scale + 1.0);
-        for (int i = i1; i >= 1; --i) {
-            double t = d.ox + (double)(i - 1) * d.scale;
-            if (fabs((t - x2) / d.scale) > 2.5) { i1 = i + 1; break; }
-        }
-        int i2 = (int)((x2 - d.ox) / d.scale + 1.0);
-        for (int i = i2; i <= d.nx; ++i) {
-            double t = d.ox + (double)(i - 1) * d.scale;
-            if (fabs((t - x2) / d.scale) > 2.5) { i2 = i - 1; break; }
-        }
-        int j2 = (int)((y2 - d.oy) / d.scale + 1.0);
-        for (int i = j2; i <= d.ny; ++i) {
-            double t = d.oy + (double)(i - 1) * d.scale;
-            if (fabs((t - y2) / d.scale) > 2.5) { j2 = i - 1; break; }
-        }
-        int j1 = (int)((y2 - d.oy) / d.scale + 1.0);
-        for (int i = j1; i >= 1; --i) {
-            double t = d.oy + (double)(i - 1) * d.scale;
-            if (fabs((t - y2) / d.scale) > 2.5) { j1 = i + 1; break; }
-        }
-        if (i1 < 1 || j1 < 1 || i2 > d.nx || j2 > d.ny || i2 - i1 > 5 || j2 - j1 > 5 || i2 < i1 || j2 < j1) {
-            set_status(d, ST_BOX_OUTSIDE);
-            i1 = 1; i2 = 0; j1 = 1; j2 = 0;   // empty box
-        }
-        d.box[4 * s] = i1; d.box[4 * s + 1] = i2; d.box[4 * s + 2] = j1; d.box[4 * s + 3] = j2;
-    }
-    __syncthreads();
-    // claim: lowest segment index wins (airfoil.f90:322-333)
-    for (int t = tid; t < d.nseg * BOX_SLOTS; t += nt) {
-        int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
-        int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
-        if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
-    }
-    __syncthreads();
-    for (int s = tid; s < d.nseg; s += nt) {
-        int c = 0;
+    if (t == 0 && d.wing_count > 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
+}
+
+__device__ inline bool box_empty(const DevState& d, int s) {
+    return d.box[4 * s + 1] < d.box[4 * s] || d.box[4 * s + 3] < d.box[4 * s + 2];
+}
+
+// claims: lowest segment index wins (airfoil.f90:322-333)
+__global__ void ibm_claim_kernel(DevState d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nseg * BOX_SLOTS) return;
+    const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+    if (box_empty(d, s)) return;
+    const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
+    if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
+}
+
+__global__ void ibm_count_kernel(DevState d) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.nseg) return;
+    int c = 0;
+    if (!box_empty(d, s))
         for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
-            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j)
-                c += (d.band_map[pidx(d, i - 1, j - 1)] == s);
-        d.claim_cnt[s] = c;
-    }
-    __syncthreads();
-    // exclusive prefix sum over segments
+            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) c += (d.band_map[pidx(d, i - 1, j - 1)] == s);
+    d.claim_cnt[s] = c;
+}
+
+// Exclusive scan of the claim counts (one block), band size, and the check
+// whether two wings' supports overlap (coupled solve).
+__global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) {
+    __shared__ int wsum[32];
+    __shared__ int wbox[MAX_WINGS][4];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < d.wing_count) { wbox[tid][0] = 0x7fffffff; wbox[tid][1] = -1; wbox[tid][2] = 0x7fffffff; wbox[tid][3] = -1; }
     const int per = (d.nseg + nt - 1) / nt;
+    const int lo = min(d.nseg, tid * per), hi = min(d.nseg, lo + per);
     int lsum = 0;
-    for (int s = tid * per; s < min(d.nseg, (tid + 1) * per); ++s) lsum += d.claim_cnt[s];
-    sh.scan[tid] = lsum;
-    __syncthreads();
-    for (int off = 1; off < nt; off <<= 1) {
-        int v = tid >= off ? sh.scan[tid - off] : 0;
-        __syncthreads();
-        sh.scan[tid] += v;
-        __syncthreads();
+    for (int s = lo; s < hi; ++s) lsum += d.claim_cnt[s];
+    int x = lsum;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    int run = sh.scan[tid] - lsum;
-    for (int s = tid * per; s < min(d.nseg, (tid + 1) * per); ++s) {
-        int c = d.claim_cnt[s];
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int base = 0, tot = 0;
+    for (int k = 0; k < (nt >> 5); ++k) {
+        if (k < warp) base += wsum[k];
+        tot += wsum[k];
+    }
+    int run = base + x - lsum;
+    for (int s = lo; s < hi; ++s) {
+        const int c = d.claim_cnt[s];
         d.claim_cnt[s] = run;
         run += c;
-    }
-    if (tid == nt - 1) {
-        int nb = sh.scan[nt - 1];
-        if (nb > d.band_cap) { set_status(d, ST_BAND_OVERFLOW); nb = d.band_cap; }
-        sh.nb = nb;
-    }
-    __syncthreads();
-    const int nb = sh.nb;
-    for (int s = tid; s < d.nseg; s += nt) {
-        int b = d.claim_cnt[s];
-        int w = d.seg_wing[s];
-        for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
-            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j)
-                if (d.band_map[pidx(d, i - 1, j - 1)] == s) {
-                    if (b < nb) {
-                        d.band_ij[2 * b] = i - 1;
-                        d.band_ij[2 * b + 1] = j - 1;
-                        d.band_wing[b] = w;
-                    }
-                    ++b;
-                }
-    }
-    __syncthreads();
-    for (int b = tid; b < nb; b += nt) d.band_map[pidx(d, d.band_ij[2 * b], d.band_ij[2 * b + 1])] = -(b + 2);
-    if (tid == 0) d.band_n[0] = nb;
-    __syncthreads();
-}
-
-// u* and rho at band nodes: fields of the plain path, or the moments of the
-// pulled distributions of the fused path.
-template <bool FUSED>
-__device__ void phase_ustar(const DevState& d, int nb) {
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
-        const long long p = pidx(d, i, j);
-        if (!FUSED) {
-            d.band_rho[b] = d.rho[p];
-            d.band_us[b] = d.u[p];
-            d.band_vs[b] = d.v[p];
-        } else {
-            double trho = 0.0, tu = 0.0, tv = 0.0;
-            const bool border = i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1;
-            const long long per = 2LL * d.ny + 2LL * d.nx;
-            for (int k = 0; k < 9; ++k) {
-                double t;
-                if (border) {
-                    long long e = (i == 0) ? j : (i == d.nx - 1) ? d.ny + j : (j == 0) ? 2LL * d.ny + i
-                                                                                        : 2LL * d.ny + d.nx + i;
-                    t = d.edge_f0[k * per + e];
-                } else {
-                    t = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
-                }
-                trho = trho + t;
-                tu = tu + (double)ex(k) * t;
-                tv = tv + (double)ey(k) * t;
-            }
-            d.band_rho[b] = trho;
-            d.band_us[b] = tu / trho;
-            d.band_vs[b] = tv / trho;
+        if (!box_empty(d, s)) {
+            const int w = d.seg_wing[s];
+            atomicMin(&wbox[w][0], d.box[4 * s]); atomicMax(&wbox[w][1], d.box[4 * s + 1]);
+            atomicMin(&wbox[w][2], d.box[4 * s + 2]); atomicMax(&wbox[w][3], d.box[4 * s + 3]);
         }
     }
+    __syncthreads();
+    if (tid == 0) {
+        const int nb = min(tot, d.band_cap);
+        if (tot > d.band_cap) set_status(d, ST_BAND_OVERFLOW);
+        d.band_n[0] = nb;
+        d.claim_cnt[d.nseg] = nb;
+        int coupled = 0;
+        for (int a = 0; a < d.wing_count; ++a)
+            for (int b = a + 1; b < d.wing_count; ++b)
+                if (wbox[a][0] <= wbox[b][1] && wbox[b][0] <= wbox[a][1] && wbox[a][2] <= wbox[b][3] &&
+                    wbox[b][2] <= wbox[a][3])
+                    coupled = 1;
+        d.ibm_flags[0] = coupled;
+        if (coupled) set_status(d, ST_WINGS_COUPLED);
+    }
 }
 
-// Delta weights per (segment, slot), band index per slot, cover lists,
-// right-hand sides r = ub - X u* (boundary_condition.f90:1540-1629).
-__device__ void phase_weights_rhs(const DevState& d, IbmShared& sh, int nb) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int b = tid; b < nb; b += nt) d.cover_n[b] = 0;
-    __syncthreads();
-    for (int t = tid; t < d.nseg * BOX_SLOTS; t += nt) {
-        int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
-        int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
-        double wv = 0.0;
+// Band list in the reference's order (segment, then i, then j) and the
+// band_map encoding -(b + 2); a node still holding its claimer's index is
+// never confused with another segment's index, so encoding as we go is safe.
+__global__ void ibm_list_kernel(DevState d) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.nseg || box_empty(d, s)) return;
+    const int nb = d.band_n[0];
+    const int w = d.seg_wing[s];
+    int b = d.claim_cnt[s];
+    for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
+        for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
+            const long long p = pidx(d, i - 1, j - 1);
+            if (d.band_map[p] != s) continue;
+            if (b < nb) {
+                d.band_ij[2 * b] = i - 1;
+                d.band_ij[2 * b + 1] = j - 1;
+                d.band_wing[b] = w;
+                d.band_claimer[b] = s;
+                d.band_map[p] = -(b + 2);
+            }
+            ++b;
+        }
+}
+
+// u*, rho at band nodes (solution.f90:510-554): the moment fields of the
+// plain path, or the moments of the pulled distributions of the fused path
+// (band nodes are interior nodes: boxes keep off the border).  Also zeroes
+// the spread accumulators.
+template <bool FUSED>
+__global__ void ibm_ustar_kernel(DevState d) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= d.band_n[0]) return;
+    const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
+    const long long p = pidx(d, i, j);
+    reinterpret_cast<unsigned long long*>(d.band_du)[b] = 0ull;
+    reinterpret_cast<unsigned long long*>(d.band_dv)[b] = 0ull;
+    if (!FUSED) {
+        d.band_rho[b] = d.rho[p];
+        d.band_us[b] = d.u[p];
+        d.band_vs[b] = d.v[p];
+        return;
+    }
+    double f[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
+    double trho = 0.0, tu = 0.0, tv = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        trho = trho + f[k];
+        tu = tu + (double)ex(k) * f[k];
+        tv = tv + (double)ey(k) * f[k];
+    }
+    d.band_rho[b] = trho;
+    d.band_us[b] = tu / trho;
+    d.band_vs[b] = tv / trho;
+}
+
+// r = ub - X u* (boundary_condition.f90:1540-1555, 1609-1629) and the band
+// index of each (segment, slot); one warp per segment, slots 0..35 over the
+// lanes, summed by a fixed butterfly.
+__global__ void ibm_rhs_kernel(DevState d) {
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= d.nseg) return;
+    const int nb = d.band_n[0];
+    const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
+    double bu = 0.0, bv = 0.0;
+    for (int slot = lane; slot < BOX_SLOTS; slot += 32) {
+        const int a = slot / 6, c = slot % 6;
+        const int i = i1 + a, j = j1 + c;
         int bi = -1;
-        if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) {
-            int bm = d.band_map[pidx(d, i - 1, j - 1)];
+        if (i <= i2 && j <= j2) {
+            const int bm = d.band_map[pidx(d, i - 1, j - 1)];
             bi = (bm <= -2) ? -(bm + 2) : -1;
-            if (bi < 0 || bi >= nb) {
-                bi = -1;
+            if (bi >= nb) bi = -1;
+            if (bi < 0) {
                 set_status(d, ST_BAND_OVERFLOW);
             } else {
-                double x0 = d.ox + d.scale * (double)(i - 1);
-                double y0 = d.oy + d.scale * (double)(j - 1);
-                double k1 = delta_phi(fabs((x0 - d.xb2[s]) / d.scale));
-                double k2 = delta_phi(fabs((y0 - d.yb2[s]) / d.scale));
-                wv = k1 * k2;
-                int pos = atomicAdd(&d.cover_n[bi], 1);
-                if (pos < MAX_COVER) d.cover_list[(long long)bi * MAX_COVER + pos] = t;
-                else set_status(d, ST_COVER_OVERFLOW);
+                const double wv = d.kx[6 * s + a] * d.ky[6 * s + c];
+                bu = bu + wv * d.band_us[bi];
+                bv = bv + wv * d.band_vs[bi];
             }
         }
-        d.pw[t] = wv;
-        d.pb[t] = bi;
+        d.pb[s * BOX_SLOTS + slot] = bi;
     }
-    __syncthreads();
-    for (int s = tid; s < d.nseg; s += nt) {
+    for (int o = 16; o > 0; o >>= 1) {
+        bu += __shfl_xor_sync(0xffffffffu, bu, o);
+        bv += __shfl_xor_sync(0xffffffffu, bv, o);
+    }
+    if (lane == 0) {
         const int w = d.seg_wing[s];
-        const WingMotion& m = sh.wm[w];
+        const WingMotion m = d.wm[w];
         const int p = d.wing_pstart[w] + (s - d.wing_sstart[w]);
-        const double sn = sin(m.angle), cs = cos(m.angle);
+        double sn, cs;
+        sincos(m.angle, &sn, &cs);
         const double xs = d.xb0[p + 1] + d.xb0[p], ys = d.yb0[p + 1] + d.yb0[p];
         const double ub = d.uu * (-(m.omega * sn * 0.5 * xs) + m.omega * cs * 0.5 * ys + m.sau) + m.extra_v;
         const double vb = d.uu * (-(m.omega * cs * 0.5 * xs) - m.omega * sn * 0.5 * ys + m.sbv);
-        double bu = 0.0, bv = 0.0;
-        for (int slot = 0; slot < BOX_SLOTS; ++slot) {
-            int bi = d.pb[s * BOX_SLOTS + slot];
-            if (bi < 0) continue;
-            double wv = d.pw[s * BOX_SLOTS + slot];
-            bu = bu + wv * d.band_us[bi];
-            bv = bv + wv * d.band_vs[bi];
-        }
         d.rx[s] = ub - bu;
         d.ry[s] = vb - bv;
-        d.qx[s] = ub - bu;   // keep r for the residual diagnostic
+        d.qx[s] = ub - bu;   // kept for the residual diagnostic
         d.qy[s] = vb - bv;
     }
-    __syncthreads();
 }
 
-// G(a, c) = sum over the common support of segments a and c.
+// G(a, c) = Sx(a, c) Sy(a, c), the delta kernel being separable.
 __device__ inline double gram(const DevState& d, int a, int c) {
     const int ai1 = d.box[4 * a], ai2 = d.box[4 * a + 1], aj1 = d.box[4 * a + 2], aj2 = d.box[4 * a + 3];
     const int ci1 = d.box[4 * c], ci2 = d.box[4 * c + 1], cj1 = d.box[4 * c + 2], cj2 = d.box[4 * c + 3];
-    const int i1 = max(ai1, ci1), i2 = min(ai2, ci2), j1 = max(aj1, cj1), j2 = min(aj2, cj2);
-    double g = 0.0;
-    for (int i = i1; i <= i2; ++i)
-        for (int j = j1; j <= j2; ++j)
-            g = g + d.pw[a * BOX_SLOTS + (i - ai1) * 6 + (j - aj1)] * d.pw[c * BOX_SLOTS + (i - ci1) * 6 + (j - cj1)];
-    return g;
+    double sx = 0.0, sy = 0.0;
+    for (int i = max(ai1, ci1); i <= min(ai2, ci2); ++i) sx = sx + d.kx[6 * a + i - ai1] * d.kx[6 * c + i - ci1];
+    for (int j = max(aj1, cj1); j <= min(aj2, cj2); ++j) sy = sy + d.ky[6 * a + j - aj1] * d.ky[6 * c + j - cj1];
+    return sx * sy;
 }
 
-// Banded G per wing in RCM order: L[w][p][dd] holds G(p, p - dd).
-__device__ void phase_assemble(const DevState& d, double* lband) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int w = 0; w < d.wing_count; ++w) {
-        const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], s0 = d.wing_sstart[w];
-        double* L = lband + d.wing_lofs[w];
-        const int tot = nw * (bw + 1);
-        for (int t = tid; t < tot; t += nt) {
-            int p = t / (bw + 1), dd = t % (bw + 1), q = p - dd;
-            L[t] = (q >= 0) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
-        }
+// Banded G per wing in RCM order (layout of ibm_wing_storage): row p of
+// wing w starts at lband[lofs_w + (p + 1) * ld]; entry dd holds G(p, p - dd).
+// Every slot of the storage is written, zero zones included.
+__global__ void ibm_assemble_kernel(DevState d, long long total) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int w = 0;
+    while (w + 1 < d.wing_count && t >= d.wing_lofs[w + 1]) ++w;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+    const long long r = t - d.wing_lofs[w];
+    const int p = (int)(r / ld) - 1, dd = (int)(r % ld), q = p - dd;
+    d.lband[t] = (p >= 0 && p < nw && q >= 0 && dd <= bw) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
+}
+
+// Right-looking banded L' D L'^T of wing w's G (RCM order), PANEL columns at
+// a time, one block of FACTOR_THREADS per wing.  Warp 0 factors a panel with
+// its PANEL + bw rows held in registers (ROWS_PER_LANE per lane, column
+// entries exchanged by warp shuffles); the block then applies the panel's
+// rank-PANEL update to the trailing window from a staged copy in shared
+// memory.  On exit lband holds d_k (clamped) on the diagonal and
+// L'(i,k) = A(i,k) / d_k below it.  Pivots below 1e-15 of the largest
+// diagonal are clamped (numerically singular systems made by marker clusters
+// finer than the lattice).
+__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) {
+    extern __shared__ double smem[];
+    const int w = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
+    constexpr int SP = PANEL + 1;   // odd row stride of the staged panel
+    double* Ps = smem;                        // [bw][SP] scaled rows below the panel
+    double* Pu = Ps + SP * d.bw_max;          // [bw][SP] unscaled rows
+    short2* pairs = reinterpret_cast<short2*>(Pu + SP * d.bw_max);
+    __shared__ double red[FACTOR_THREADS / 32];
+    __shared__ double pinv[PANEL];
+    const long long wsize = ibm_wing_storage(nw, bw);
+    double* gS = d.lband + d.wing_lofs[w];
+    double* S = gS;
+    if (d.factor_in_smem) {
+        S = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + d.factor_smem_off);
+        for (long long t = tid; t < wsize; t += FACTOR_THREADS) S[t] = gS[t];
+    }
+    double* A = S + ld;   // row 0
+    const int P = bw * (bw + 1) / 2;
+    for (int t = tid; t < P; t += FACTOR_THREADS) {
+        int r1 = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        while (r1 * (r1 + 1) / 2 > t) --r1;
+        while ((r1 + 1) * (r1 + 2) / 2 <= t) ++r1;
+        pairs[t] = make_short2((short)r1, (short)(t - r1 * (r1 + 1) / 2));
     }
     __syncthreads();
+    double mx = 0.0;
+    for (int p = tid; p < nw; p += FACTOR_THREADS) mx = fmax(mx, A[p * ld]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    mx = 0.0;
+    for (int k = 0; k < FACTOR_THREADS / 32; ++k) mx = fmax(mx, red[k]);
+    const double fl = mx > 0.0 ? 1e-15 * mx : 1.0;
+    bool clamped = false;
+
+    for (int k0 = 0; k0 < nw; k0 += PANEL) {
+        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
+        if (warp == 0) {
+            // rows k0 + r, r = lane + 32 h; entry c is A(k0 + r, k0 + c) at
+            // offset r - c of the row (zero zones make every read valid)
+            double pr[ROWS_PER_LANE][PANEL];
+#pragma unroll
+            for (int h = 0; h < ROWS_PER_LANE; ++h) {
+                const int r = lane + 32 * h;
+                const double* row = A + (k0 + r) * ld + r;
+#pragma unroll
+                for (int c = 0; c < PANEL; ++c) pr[h][c] = (r < PANEL + bw) ? row[-c] : 0.0;
+            }
+            double icv[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) {
+                // column k0 + c: pivot in lane c (h = 0), A(k0 + j, k0 + c) in lane j
+                double dc = __shfl_sync(0xffffffffu, pr[0][c], c);
+                double col[PANEL];
+#pragma unroll
+                for (int j = c + 1; j < PANEL; ++j) col[j] = __shfl_sync(0xffffffffu, pr[0][c], j);
+                icv[c] = 0.0;
+                if (c < np) {
+                    if (!(dc > fl)) { dc = fl; clamped = true; }
+                    const double ic = fast_recip(dc);
+                    icv[c] = ic;
+                    if (lane == c) pr[0][c] = dc;
+#pragma unroll
+                    for (int h = 0; h < ROWS_PER_LANE; ++h) {
+                        const int r = lane + 32 * h;
+                        if (h == 0 && r <= c) continue;
+                        const double a = pr[h][c] * ic;
+#pragma unroll
+                        for (int j = c + 1; j < PANEL; ++j)
+                            if (h > 0 || j <= r) pr[h][j] = pr[h][j] - a * col[j];
+                    }
+                }
+            }
+            // d on the diagonal, the scaled L' below it; the rows below the
+            // panel are staged (scaled and unscaled) for the trailing update
+#pragma unroll
+            for (int h = 0; h < ROWS_PER_LANE; ++h) {
+                const int r = lane + 32 * h;
+                if (r >= PANEL + bw) continue;
+                double* row = A + (k0 + r) * ld + r;
+#pragma unroll
+                for (int c = 0; c < PANEL; ++c) {
+                    if (h == 0 && r < c) continue;   // above the diagonal
+                    row[-c] = (h == 0 && r == c) ? pr[h][c] : pr[h][c] * icv[c];
+                }
+                const int rb = r - np;   // row k1 + rb of the trailing window
+                if (rb >= 0 && rb < bw) {
+#pragma unroll
+                    for (int c = 0; c < PANEL; ++c) {
+                        Pu[rb * SP + c] = pr[h][c];
+                        Ps[rb * SP + c] = pr[h][c] * icv[c];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // trailing update (zero rows past the end absorb the updates of the
+        // last panels)
+        for (int t = tid; t < P; t += FACTOR_THREADS) {
+            const short2 pq = pairs[t];
+            const double* a = Ps + pq.x * SP;
+            const double* b = Pu + pq.y * SP;
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) acc = acc + a[c] * b[c];
+            double* e = A + (k1 + pq.x) * ld + (pq.x - pq.y);
+            *e = *e - acc;
+        }
+        __syncthreads();
+    }
+    if (clamped) set_status(d, ST_PIVOT_CLAMPED);
+    if (d.factor_in_smem)
+        for (long long t = tid; t < wsize; t += FACTOR_THREADS) gS[t] = S[t];
 }
 
-// Banded Cholesky and two triangular solves for wing w, one warp.
-__device__ void wing_factor_solve(const DevState& d, double* lband, int w, bool factor) {
-    const int lane = threadIdx.x & 31;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], s0 = d.wing_sstart[w];
-    const int ld = bw + 1;
-    double* L = lband + d.wing_lofs[w];
-    if (factor) {
-        double maxdiag = 0.0;
-        for (int p = lane; p < nw; p += 32) maxdiag = fmax(maxdiag, L[p * ld]);
-        for (int o = 16; o > 0; o >>= 1) maxdiag = fmax(maxdiag, __shfl_xor_sync(0xffffffffu, maxdiag, o));
-        const double floor_piv = 1e-15 * maxdiag;
-        for (int k = 0; k < nw; ++k) {
-            double dkk = L[k * ld];
-            if (!(dkk > floor_piv)) {
-                dkk = floor_piv > 0.0 ? floor_piv : 1.0;
-                if (lane == 0) set_status(d, ST_PIVOT_CLAMPED);
-            }
-            const double lkk = sqrt(dkk);
-            const int m = min(bw, nw - 1 - k);
-            __syncwarp();
-            for (int r = lane; r < m; r += 32) {
-                const int i = k + 1 + r;
-                L[i * ld + (i - k)] = L[i * ld + (i - k)] / lkk;
-            }
-            __syncwarp();
-            if (lane == 0) L[k * ld] = lkk;
-            const int P = m * (m + 1) / 2;
-            for (int t = lane; t < P; t += 32) {
-                int r1 = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-                while (r1 * (r1 + 1) / 2 > t) --r1;
-                while ((r1 + 1) * (r1 + 2) / 2 <= t) ++r1;
-                const int r2 = t - r1 * (r1 + 1) / 2;
-                const int i = k + 1 + r1, j = k + 1 + r2;
-                L[i * ld + (i - j)] = L[i * ld + (i - j)] - L[i * ld + (i - k)] * L[j * ld + (j - k)];
-            }
-            __syncwarp();
-        }
-    }
-    // forward: L z = r (RCM order, z held in qx/qy work arrays as zx/zy)
-    double* zx = d.zx + s0;
-    double* zy = d.zy + s0;
-    for (int p = lane; p < nw; p += 32) {
-        zx[p] = d.rx[d.perm[s0 + p]];
-        zy[p] = d.ry[d.perm[s0 + p]];
-    }
+// Forward and backward substitution with the factor of wing w: warp 0 solves
+// for the x component, warp 1 for the y component.  Panel rows sit in
+// registers; within a panel the unknowns pass by shuffles; the forward sweep
+// updates the rows below a panel, the backward sweep the rows above it.
+__global__ void __launch_bounds__(64) ibm_solve_kernel(DevState d) {
+    extern __shared__ double zsh[];
+    const int w = blockIdx.x;
+    const int lane = threadIdx.x & 31, comp = threadIdx.x >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
+    double* rr = comp == 0 ? d.rx : d.ry;
+    double* z = zsh + comp * (d.nw_max + PANEL + d.bw_max);   // zero tail past nw
+    for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? rr[d.perm[s0 + p]] : 0.0;
     __syncwarp();
-    for (int k = 0; k < nw; ++k) {
-        const double lkk = L[k * ld];
-        const double ax = zx[k] / lkk, ay = zy[k] / lkk;
-        const int m = min(bw, nw - 1 - k);
-        __syncwarp();
-        for (int r = lane; r < m; r += 32) {
-            const int i = k + 1 + r;
-            const double lik = L[i * ld + (i - k)];
-            zx[i] = zx[i] - lik * ax;
-            zy[i] = zy[i] - lik * ay;
+    // L' D v = r
+    for (int k0 = 0; k0 < nw; k0 += PANEL) {
+        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
+        double zr[ROWS_PER_LANE], lr[ROWS_PER_LANE][PANEL];
+#pragma unroll
+        for (int h = 0; h < ROWS_PER_LANE; ++h) {
+            const int r = lane + 32 * h, i = k0 + r;
+            const bool ok = r < PANEL + bw;
+            zr[h] = ok ? z[i] : 0.0;
+            const double* row = A + i * ld + r;
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c)   // L'(i, k0 + c), zero on and above the diagonal
+                lr[h][c] = (ok && c < np && (h > 0 || r > c)) ? row[-c] : 0.0;
         }
-        if (lane == 0) { zx[k] = ax; zy[k] = ay; }
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) {
+            const double wc = __shfl_sync(0xffffffffu, zr[0], c);
+#pragma unroll
+            for (int h = 0; h < ROWS_PER_LANE; ++h) zr[h] = zr[h] - lr[h][c] * wc;
+        }
+#pragma unroll
+        for (int h = 0; h < ROWS_PER_LANE; ++h) {
+            const int r = lane + 32 * h, i = k0 + r;
+            if (r < PANEL + bw) z[i] = (r < np) ? zr[h] * fast_recip(A[i * ld]) : zr[h];
+        }
         __syncwarp();
     }
-    // backward: L^T y = z
-    for (int k = nw - 1; k >= 0; --k) {
-        const double lkk = L[k * ld];
-        const double ax = zx[k] / lkk, ay = zy[k] / lkk;
-        const int m = min(bw, k);
-        __syncwarp();
-        for (int r = lane; r < m; r += 32) {
-            const int j = k - 1 - r;
-            const double lkj = L[k * ld + (k - j)];
-            zx[j] = zx[j] - lkj * ax;
-            zy[j] = zy[j] - lkj * ay;
+    // L'^T y = v
+    const int last0 = ((nw - 1) / PANEL) * PANEL;
+    for (int k0 = last0; k0 >= 0; k0 -= PANEL) {
+        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
+        double y = lane < np ? z[k0 + lane] : 0.0;
+#pragma unroll
+        for (int e = PANEL - 1; e >= 0; --e) {
+            const double ye = __shfl_sync(0xffffffffu, y, e);
+            if (e < np && lane < e && e - lane <= bw) y = y - A[(k0 + e) * ld + (e - lane)] * ye;
         }
-        if (lane == 0) { zx[k] = ax; zy[k] = ay; }
+        double yc[PANEL];
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, y, c);
+        if (lane < np) z[k0 + lane] = y;
+        for (int r = lane; r < bw; r += 32) {
+            const int j = k0 - 1 - r;   // rows above the panel
+            if (j < 0) break;
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) {
+                const int dd = k0 + c - j;
+                if (c < np && dd <= bw) acc = acc + A[(k0 + c) * ld + dd] * yc[c];
+            }
+            z[j] = z[j] - acc;
+        }
         __syncwarp();
     }
+    double ym = 0.0;
     for (int p = lane; p < nw; p += 32) {
-        d.rx[d.perm[s0 + p]] = zx[p];
-        d.ry[d.perm[s0 + p]] = zy[p];
+        rr[d.perm[s0 + p]] = z[p];
+        ym = fmax(ym, fabs(z[p]));
     }
-    __syncwarp();
+    for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
+    if (lane == 0) d.ymax[2 * w + comp] = ym;
 }
 
-// du = X^T y, summed per band node in ascending (segment, slot) order.
-__device__ void phase_spread(const DevState& d, int nb) {
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        int n = min(d.cover_n[b], MAX_COVER);
-        int* lst = d.cover_list + (long long)b * MAX_COVER;
-        for (int a = 1; a < n; ++a) {   // insertion sort: run-to-run deterministic order
-            int v = lst[a], c = a - 1;
-            while (c >= 0 && lst[c] > v) { lst[c + 1] = lst[c]; --c; }
-            lst[c + 1] = v;
-        }
-        double sx = 0.0, sy = 0.0;
-        int w0 = -1;
-        bool coupled = false;
-        for (int a = 0; a < n; ++a) {
-            int t = lst[a], s = t / BOX_SLOTS;
-            double wv = d.pw[t];
-            sx = sx + wv * d.rx[s];
-            sy = sy + wv * d.ry[s];
-            int w = d.seg_wing[s];
-            if (w0 < 0) w0 = w; else if (w != w0) coupled = true;
-        }
-        if (coupled) set_status(d, ST_WINGS_COUPLED);
-        d.band_du[b] = sx;
-        d.band_dv[b] = sy;
-    }
+// Fixed-point exponent shared by the spread and the finish kernels: every
+// contribution is below 2^(62 - 10) in magnitude after scaling, so sums of up
+// to 1024 of them cannot overflow.
+__device__ inline int spread_exponent(const DevState& d) {
+    double ym = 0.0;
+    for (int w = 0; w < 2 * d.wing_count; ++w) ym = fmax(ym, d.ymax[w]);
+    int e2 = 0;
+    frexp(ym > 0.0 ? 1024.0 * ym : 1.0, &e2);
+    return 62 - e2;
 }
 
-// Velocity correction, body force, per-wing force and moment, force row.
+// du = X^T y: every (segment, slot) contribution is rounded once to a 64-bit
+// fixed-point number and added with an integer atomic.
+__global__ void ibm_spread_kernel(DevState d) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nseg * BOX_SLOTS) return;
+    const int bi = d.pb[t];
+    if (bi < 0) return;
+    const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+    const int e = spread_exponent(d);
+    const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.band_du) + bi,
+              (unsigned long long)__double2ll_rn(ldexp(wv * d.rx[s], e)));
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.band_dv) + bi,
+              (unsigned long long)__double2ll_rn(ldexp(wv * d.ry[s], e)));
+}
+
+// du back to FP64, velocity correction and body force (plain path fields),
+// and per-block partial sums of each wing's force and moment over the
+// block's contiguous slice of the band list (each wing owns a contiguous
+// range: claim order).
 template <bool FUSED>
-__device__ void phase_finish(const DevState& d, IbmShared& sh, int nb) {
-    const int tid = threadIdx.x, nt = blockDim.x, W = d.wing_count;
-    double acc[MAX_WINGS][3];
-    for (int w = 0; w < W; ++w) acc[w][0] = acc[w][1] = acc[w][2] = 0.0;
-    for (int b = tid; b < nb; b += nt) {
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) {
+    constexpr int NWARP = FINISH_THREADS / 32;
+    __shared__ double red[NWARP][3];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nb = d.band_n[0];
+    const int b = blockIdx.x * FINISH_THREADS + tid;
+    const int e = spread_exponent(d);
+    double t1 = 0.0, t2 = 0.0;
+    int myw = -1;
+    double x0 = 0.0, y0 = 0.0;
+    if (b < nb) {
+        const double du = ldexp((double)reinterpret_cast<long long*>(d.band_du)[b], -e);
+        const double dv = ldexp((double)reinterpret_cast<long long*>(d.band_dv)[b], -e);
+        d.band_du[b] = du;
+        d.band_dv[b] = dv;
         const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
-        const double rh = d.band_rho[b], du = d.band_du[b], dv = d.band_dv[b];
-        const double t1 = 2.0 * rh * du, t2 = 2.0 * rh * dv;
+        const double rh = d.band_rho[b];
+        t1 = 2.0 * rh * du;
+        t2 = 2.0 * rh * dv;
         if (!FUSED) {
-            long long p = pidx(d, i, j);
+            const long long p = pidx(d, i, j);
             d.u[p] = d.band_us[b] + du;
             d.v[p] = d.band_vs[b] + dv;
             d.gfx[p] = t1;
             d.gfy[p] = t2;
         }
-        const int w = d.band_wing[b];
-        const WingMotion& m = sh.wm[w];
-        double x0 = (d.ox + d.scale * (double)i - (d.xc + d.wing_x_origin + (double)w * d.wing_x_spacing + m.sa)) / d.scale -
-                    m.extra_pos;
-        double y0 = (d.oy + d.scale * (double)j - (d.yc + d.wing_y_origin + m.sb)) / d.scale;
-        for (int ww = 0; ww < W; ++ww) {   // register-resident accumulators
-            if (ww == w) {
-                acc[ww][0] = acc[ww][0] - t1;
-                acc[ww][1] = acc[ww][1] - t2;
-                acc[ww][2] = acc[ww][2] - x0 * t2 + y0 * t1;
-            }
-        }
+        myw = d.band_wing[b];
+        const WingMotion m = d.wm[myw];
+        const double xw = d.xc + d.wing_x_origin + (double)myw * d.wing_x_spacing + m.sa;
+        const double yw = d.yc + d.wing_y_origin + m.sb;
+        x0 = (d.ox + d.scale * (double)i - xw) / d.scale - m.extra_pos;
+        y0 = (d.oy + d.scale * (double)j - yw) / d.scale;
     }
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int w = 0; w < W; ++w)
-        for (int c = 0; c < 3; ++c) {
-            double v = acc[w][c];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) sh.red[warp][w][c] = v;
+    const int b0 = blockIdx.x * FINISH_THREADS;
+    const int b1 = min(nb, b0 + FINISH_THREADS) - 1;
+    const int wlo = b0 < nb ? d.band_wing[b0] : 0, whi = b0 < nb ? d.band_wing[b1] : -1;
+    for (int w = 0; w < d.wing_count; ++w) {
+        double* out = d.force_part + ((long long)blockIdx.x * d.wing_count + w) * 3;
+        if (w < wlo || w > whi) {
+            if (tid < 3) out[tid] = 0.0;
+            continue;
         }
-    // no-slip residual diagnostic |X du - r|^2 and |r|^2
-    double e2 = 0.0, r2 = 0.0;
-    for (int s = tid; s < d.nseg; s += nt) {
-        double ax = 0.0, ay = 0.0;
-        for (int slot = 0; slot < BOX_SLOTS; ++slot) {
-            int bi = d.pb[s * BOX_SLOTS + slot];
-            if (bi < 0) continue;
-            ax = ax + d.pw[s * BOX_SLOTS + slot] * d.band_du[bi];
-            ay = ay + d.pw[s * BOX_SLOTS + slot] * d.band_dv[bi];
+        double fx = 0.0, fy = 0.0, mz = 0.0;
+        if (myw == w) {
+            fx = -t1;
+            fy = -t2;
+            mz = -x0 * t2 + y0 * t1;
         }
-        e2 += (ax - d.qx[s]) * (ax - d.qx[s]) + (ay - d.qy[s]) * (ay - d.qy[s]);
-        r2 += d.qx[s] * d.qx[s] + d.qy[s] * d.qy[s];
+        for (int o = 16; o > 0; o >>= 1) {
+            fx += __shfl_down_sync(0xffffffffu, fx, o);
+            fy += __shfl_down_sync(0xffffffffu, fy, o);
+            mz += __shfl_down_sync(0xffffffffu, mz, o);
+        }
+        if (lane == 0) { red[warp][0] = fx; red[warp][1] = fy; red[warp][2] = mz; }
+        __syncthreads();
+        if (tid < 3) {
+            double v = 0.0;
+            for (int k = 0; k < NWARP; ++k) v += red[k][tid];
+            out[tid] = v;
+        }
+        __syncthreads();
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        e2 += __shfl_down_sync(0xffffffffu, e2, o);
-        r2 += __shfl_down_sync(0xffffffffu, r2, o);
-    }
-    __shared__ double res_s[IBM_WARPS][2];
-    if (lane == 0) { res_s[warp][0] = e2; res_s[warp][1] = r2; }
-    __syncthreads();
-    if (tid < W * 3) {
-        int w = tid / 3, c = tid % 3;
+}
+
+// Per-wing force and moment from the block partials (in block order), the
+// no-slip residual when diagnostics are on, and the force row.
+__global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks) {
+    __shared__ double fm[MAX_WINGS][3];
+    __shared__ double red[8][2];
+    const int tid = threadIdx.x, W = d.wing_count;
+    if (tid < 3 * W) {
+        const int w = tid / 3, c = tid % 3;
         double v = 0.0;
-        for (int k = 0; k < (nt >> 5); ++k) v += sh.red[k][w][c];
-        sh.fm[w][c] = v;
+        for (int k = 0; k < nblocks; ++k) v += d.force_part[((long long)k * W + w) * 3 + c];
+        fm[w][c] = v;
+    }
+    if (d.diag) {
+        double e2 = 0.0, r2 = 0.0;
+        for (int s = tid; s < d.nseg; s += blockDim.x) {
+            double ax = 0.0, ay = 0.0;
+            for (int slot = 0; slot < BOX_SLOTS; ++slot) {
+                const int bi = d.pb[s * BOX_SLOTS + slot];
+                if (bi < 0) continue;
+                const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
+                ax = ax + wv * d.band_du[bi];
+                ay = ay + wv * d.band_dv[bi];
+            }
+            e2 += (ax - d.qx[s]) * (ax - d.qx[s]) + (ay - d.qy[s]) * (ay - d.qy[s]);
+            r2 += d.qx[s] * d.qx[s] + d.qy[s] * d.qy[s];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            e2 += __shfl_down_sync(0xffffffffu, e2, o);
+            r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        }
+        if ((tid & 31) == 0) { red[tid >> 5][0] = e2; red[tid >> 5][1] = r2; }
     }
     __syncthreads();
     if (tid == 0) {
-        double a = 0.0, b = 0.0;
-        for (int k = 0; k < (nt >> 5); ++k) { a += res_s[k][0]; b += res_s[k][1]; }
-        d.ibm_resid[0] = a;
-        d.ibm_resid[1] = b;
+        if (d.diag) {
+            double a = 0.0, b = 0.0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += red[k][0]; b += red[k][1]; }
+            d.ibm_resid[0] = a;
+            d.ibm_resid[1] = b;
+        }
         // force normalisation and force row (solution.f90:330-385)
         const double uu = d.uu, sc = d.scale;
-        const long long cycle = *d.cycle;
-        const double time = (double)(cycle - 1) * (sc * uu);
+        const double time = step_time(d);
         const long long ri = *d.row_index;
         const int rl = 4 + 12 * W;
         double* row = (d.force_rows && ri < d.force_rows_cap) ? d.force_rows + ri * rl : nullptr;
@@ -551,12 +775,12 @@ __device__ void phase_finish(const DevState& d, IbmShared& sh, int nb) {
         rowv[0] = time;
         int col = 1;
         for (int w = 0; w < W; ++w) {
-            double Fx = 2.0 * sh.fm[w][0] / (uu * uu * (1.0 / sc));
-            double Fy = 2.0 * sh.fm[w][1] / (uu * uu * (1.0 / sc));
-            double Mz = -(2.0 * sh.fm[w][2] / (uu * uu * (1.0 / (sc * sc))));
-            d.wing_fm[3 * w] = sh.fm[w][0];
-            d.wing_fm[3 * w + 1] = sh.fm[w][1];
-            d.wing_fm[3 * w + 2] = sh.fm[w][2];
+            const double Fx = 2.0 * fm[w][0] / (uu * uu * (1.0 / sc));
+            const double Fy = 2.0 * fm[w][1] / (uu * uu * (1.0 / sc));
+            const double Mz = -(2.0 * fm[w][2] / (uu * uu * (1.0 / (sc * sc))));
+            d.wing_fm[3 * w] = fm[w][0];
+            d.wing_fm[3 * w + 1] = fm[w][1];
+            d.wing_fm[3 * w + 2] = fm[w][2];
             rowv[col] = Fx; rowv[col + 1] = Fy; rowv[col + 2] = Mz;
             col += 3;
         }
@@ -565,10 +789,10 @@ __device__ void phase_finish(const DevState& d, IbmShared& sh, int nb) {
         rowv[col] = fx; rowv[col + 1] = fy; rowv[col + 2] = mt;
         col += 3;
         for (int w = 0; w < W; ++w) {
-            const WingMotion& m = sh.wm[w];
-            rowv[col] = d.wing_x_origin + (double)w * d.wing_x_spacing + m.sa + m.extra_s / (1.0 / sc);
+            const WingMotion m = d.wm[w];
+            rowv[col] = add(add(add(d.wing_x_origin, mul((double)w, d.wing_x_spacing)), m.sa), m.extra_s / (1.0 / sc));
             rowv[col + 1] = m.sau; rowv[col + 2] = m.saac;
-            rowv[col + 3] = d.wing_y_origin + m.sb;
+            rowv[col + 3] = add(d.wing_y_origin, m.sb);
             rowv[col + 4] = m.sbv; rowv[col + 5] = m.sbac;
             rowv[col + 6] = m.angle; rowv[col + 7] = m.omega; rowv[col + 8] = m.omgac;
             col += 9;
@@ -581,41 +805,6 @@ __device__ void phase_finish(const DevState& d, IbmShared& sh, int nb) {
     }
 }
 
-template <bool FUSED>
-__device__ void phase_solve(const DevState& d, IbmShared& sh, double* lband) {
-    const int nb = d.band_n[0];
-    phase_ustar<FUSED>(d, nb);
-    __syncthreads();
-    phase_weights_rhs(d, sh, nb);
-    phase_assemble(d, lband);
-    const int warp = threadIdx.x >> 5;
-    for (int w = warp; w < d.wing_count; w += IBM_WARPS) wing_factor_solve(d, lband, w, true);
-    __syncthreads();
-    phase_spread(d, nb);
-    __syncthreads();
-    phase_finish<FUSED>(d, sh, nb);
-}
-
-__global__ void __launch_bounds__(IBM_THREADS) ibm_band_kernel(DevState d) {
-    __shared__ IbmShared sh;
-    phase_band(d, sh);
-}
-
-__global__ void __launch_bounds__(IBM_THREADS) ibm_solve_plain_kernel(DevState d, int band_in_smem) {
-    __shared__ IbmShared sh;
-    extern __shared__ double dyn[];
-    if (threadIdx.x < d.wing_count) sh.wm[threadIdx.x] = d.wm[threadIdx.x];
-    __syncthreads();
-    phase_solve<false>(d, sh, band_in_smem ? dyn : d.lband);
-}
-
-__global__ void __launch_bounds__(IBM_THREADS) ibm_full_fused_kernel(DevState d, int band_in_smem) {
-    __shared__ IbmShared sh;
-    extern __shared__ double dyn[];
-    phase_band(d, sh);
-    phase_solve<true>(d, sh, band_in_smem ? dyn : d.lband);
-}
-
 __global__ void step_advance_kernel(DevState d) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         *d.cycle += 1;
@@ -623,21 +812,51 @@ __global__ void step_advance_kernel(DevState d) {
     }
 }
 
-void launch_ibm_band(const DevState& d, cudaStream_t st) {
-    ibm_band_kernel<<<1, IBM_THREADS, 0, st>>>(d);
-}
-void launch_ibm_solve(const DevState& d, size_t smem, bool band_in_smem, cudaStream_t st) {
-    ibm_solve_plain_kernel<<<1, IBM_THREADS, smem, st>>>(d, band_in_smem ? 1 : 0);
-}
-void launch_ibm_full(const DevState& d, size_t smem, bool band_in_smem, cudaStream_t st) {
-    ibm_full_fused_kernel<<<1, IBM_THREADS, smem, st>>>(d, band_in_smem ? 1 : 0);
-}
-void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kernel<<<1, 32, 0, st>>>(d); }
+// ------------------------------------------------------------ host side
+static inline int blocks(long long n, int t) { return (int)std::max<long long>(1, (n + t - 1) / t); }
 
-cudaError_t ibm_set_smem_limit(size_t bytes) {
-    cudaError_t e = cudaFuncSetAttribute(ibm_solve_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(ibm_full_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+cudaError_t ibm_prepare(size_t factor_smem) {
+    return cudaFuncSetAttribute(ibm_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem);
 }
+
+int ibm_finish_blocks(const DevState& d) { return blocks(d.band_cap, FINISH_THREADS); }
+
+void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done) {
+    const long long n1 = std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap);
+    ibm_geometry_kernel<<<blocks(n1, 128), 128, 0, st>>>(d);
+    if (geometry_done) cudaEventRecord(geometry_done, st);
+    ibm_claim_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
+    ibm_count_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
+    ibm_scan_kernel<<<1, 1024, 0, st>>>(d);
+    ibm_list_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
+}
+
+void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
+    const long long total = d.lband_total;
+    ibm_assemble_kernel<<<blocks(total, 256), 256, 0, st>>>(d, total);
+    if (d.wing_count > 0) ibm_factor_kernel<<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
+}
+
+void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
+    if (fused)
+        ibm_ustar_kernel<true><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
+    else
+        ibm_ustar_kernel<false><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
+    ibm_rhs_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
+}
+
+void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st) {
+    if (d.wing_count > 0)
+        ibm_solve_kernel<<<d.wing_count, 64, 2 * (d.nw_max + PANEL + d.bw_max) * sizeof(double), st>>>(d);
+    ibm_spread_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
+    const int nbk = ibm_finish_blocks(d);
+    if (fused)
+        ibm_finish_kernel<true><<<nbk, FINISH_THREADS, 0, st>>>(d);
+    else
+        ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
+    ibm_forces_kernel<<<1, 256, 0, st>>>(d, nbk);
+}
+
+void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kernel<<<1, 32, 0, st>>>(d); }
 
 }  // namespace lbm

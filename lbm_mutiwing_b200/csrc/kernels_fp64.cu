@@ -33,8 +33,7 @@ struct PlainAcc {
 };
 
 // Fused path: f0 is the pull of the previous post-collision planes (gA) for
-// interior nodes and the border store for border nodes; the moments of band
-// nodes carry the immersed-boundary velocity correction.
+// interior nodes and the border store for border nodes.
 struct FusedAcc {
     DevState d;
     __device__ bool border(int i, int j) const {
@@ -60,14 +59,9 @@ struct FusedAcc {
             tu = tu + (double)ex(k) * t;
             tv = tv + (double)ey(k) * t;
         }
-        Mom m{trho, tu / trho, tv / trho};
-        int bm = d.band_map[pidx(d, i, j)];
-        if (bm <= -2) {
-            int b = -(bm + 2);
-            m.u = d.band_us[b] + d.band_du[b];
-            m.v = d.band_vs[b] + d.band_dv[b];
-        }
-        return m;
+        // support boxes keep three nodes off the border, so no node the far
+        // field reads is an immersed-boundary band node
+        return Mom{trho, tu / trho, tv / trho};
     }
     __device__ void write_f(int i, int j, const double* f) const {
         long long p = pidx(d, i, j);
@@ -75,7 +69,7 @@ struct FusedAcc {
         for (int k = 0; k < 9; ++k) d.gB[k * d.plane + p] = (float)(f[k] - weight(k));
     }
     __device__ void write_fields(int i, int j, Mom m) const {
-        if (!d.fo_rho) return;
+        if (!d.write_fields || !d.fo_rho) return;
         long long p = pidx(d, i, j);
         d.fo_rho[p] = m.r;
         d.fo_u[p] = m.u;

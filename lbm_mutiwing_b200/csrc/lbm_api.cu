@@ -13,7 +13,6 @@
 #include "lbm_kernels.h"
 
 namespace lbm {
-cudaError_t ibm_set_smem_limit(size_t bytes);
 
 // nizhen (solution.f90:1474-1529): Gauss-Jordan inverse of M as the reference
 // computes it, so the plain path multiplies by the same M^-1 entries.
@@ -104,6 +103,10 @@ static int rcm_order(const std::vector<double>& mx, const std::vector<double>& m
 
 using namespace lbm;
 
+// phase timers: move_boundary, collide-stream, band re-collision, far field,
+// immersed-boundary solve
+constexpr int NPHASE = 6;
+
 struct LbmHandle {
     LbmConfig cfg{};
     std::string err;
@@ -111,13 +114,15 @@ struct LbmHandle {
     FusedConsts fc{};
     int parity = 0;                 // fused path: 0 -> current planes in gA
     float* planes[2] = {nullptr, nullptr};
-    cudaStream_t s_main = nullptr, s_ibm = nullptr;
-    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr;
+    // streams of one fused step: main (bulk kernel, band re-collision),
+    // ibm (band list, right-hand side, solve), aux (assembly and
+    // factorisation of G), bc (far field)
+    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_aux = nullptr, s_bc = nullptr;
+    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_geom = nullptr, ev_fact = nullptr, ev_bc = nullptr;
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
     int row_len = 4;
-    bool band_in_smem = false;
-    size_t ibm_smem = 0;
+    size_t factor_smem = 0;         // dynamic shared memory of the factorisation kernel
     double* err_partial = nullptr;
     double* err_out = nullptr;
     bool fields_valid = false, err_valid = false;
@@ -140,11 +145,16 @@ struct LbmHandle {
     std::vector<cudaEvent_t> evpool;
     size_t evused = 0;
     std::vector<std::pair<int, std::pair<size_t, size_t>>> marks;   // phase, (start ev, stop ev)
-    double phase_ms[4] = {0, 0, 0, 0};
+    double phase_ms[NPHASE] = {0, 0, 0, 0, 0, 0};
     long long timed_steps = 0;
+    // CUDA graphs of two consecutive steps, one per starting parity; any
+    // change of a pointer or value baked into DevState drops them
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
 };
 
 namespace {
+
+void drop_graphs(LbmHandle* h);
 
 int fail(LbmHandle* h, const std::string& msg) {
     if (h) h->err = msg;
@@ -301,6 +311,7 @@ int ensure_rows(LbmHandle* h, int64_t n) {
     if (dalloc(h, &h->d_rowbuf, (size_t)cap * h->row_len)) return -1;
     h->rows_cap = cap;
     h->d.force_rows = h->d_rowbuf;
+    drop_graphs(h);
     h->d.force_rows_cap = cap;
     return 0;
 }
@@ -309,11 +320,10 @@ int check_status(LbmHandle* h) {
     int st = 0;
     CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
     h->status_seen |= st;
-    const int fatal = ST_BAND_OVERFLOW | ST_COVER_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION;
+    const int fatal = ST_BAND_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION;
     if (st & fatal) {
         std::string m = "immersed boundary:";
         if (st & ST_BAND_OVERFLOW) m += " band capacity exceeded;";
-        if (st & ST_COVER_OVERFLOW) m += " a band node is covered by too many segments;";
         if (st & ST_BOX_OUTSIDE) m += " a wing's support box left the lattice;";
         if (st & ST_MOTION) m += " no motion rows loaded;";
         return fail(h, m);
@@ -357,12 +367,14 @@ void collect_phase_times(LbmHandle* h) {
 }
 
 // One evolution step (solution.f90:272-422) on the current parity.
-void enqueue_step(LbmHandle* h, bool fields) {
+void enqueue_step(LbmHandle* h, bool fields, bool diag) {
     DevState d = current(h);
+    d.diag = diag ? 1 : 0;
+    d.write_fields = fields ? 1 : 0;
     if (d.precision == 0) {
         {
             PhaseMark pm(h, 0, h->s_main);
-            launch_ibm_band(d, h->s_main);             // mode + move_boundary (:292-299)
+            launch_ibm_band(d, h->s_main, nullptr);    // mode + move_boundary (:292-299)
         }
         {
             PhaseMark pm(h, 1, h->s_main);
@@ -370,8 +382,13 @@ void enqueue_step(LbmHandle* h, bool fields) {
             launch_plain_moments(d, h->s_main);        // physical_variables (:321)
         }
         {
-            PhaseMark pm(h, 0, h->s_main);
-            launch_ibm_solve(d, h->ibm_smem, h->band_in_smem, h->s_main);  // immersed_boundary_wu (:325)
+            PhaseMark pm(h, 5, h->s_main);             // immersed_boundary_wu (:325)
+            launch_ibm_factor(d, h->factor_smem, h->s_main);
+        }
+        {
+            PhaseMark pm(h, 4, h->s_main);
+            launch_ibm_rhs(d, false, h->s_main);
+            launch_ibm_solve(d, false, h->s_main);
         }
         {
             PhaseMark pm(h, 1, h->s_main);
@@ -383,12 +400,34 @@ void enqueue_step(LbmHandle* h, bool fields) {
         }
         launch_step_advance(d, h->s_main);
     } else {
-        // the IBM block overlaps the bulk kernel; both read only the current planes
+        // The immersed boundary (two high-priority streams) and the far field
+        // overlap the bulk kernel: all read only the current planes, and the
+        // writes go to disjoint nodes of the next planes (interior, band,
+        // border).  Support boxes keep off the border rows and columns the far
+        // field reads, so it needs nothing from the immersed boundary.
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
+        cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
         {
             PhaseMark pm(h, 0, h->s_ibm);
-            launch_ibm_full(d, h->ibm_smem, h->band_in_smem, h->s_ibm);
+            launch_ibm_band(d, h->s_ibm, h->ev_geom);
+        }
+        cudaStreamWaitEvent(h->s_aux, h->ev_geom, 0);
+        {
+            PhaseMark pm(h, 5, h->s_aux);
+            launch_ibm_factor(d, h->factor_smem, h->s_aux);
+        }
+        cudaEventRecord(h->ev_fact, h->s_aux);
+        {
+            PhaseMark pm(h, 3, h->s_bc);
+            launch_outer_bc(d, h->s_bc);
+        }
+        cudaEventRecord(h->ev_bc, h->s_bc);
+        {
+            PhaseMark pm(h, 4, h->s_ibm);
+            launch_ibm_rhs(d, true, h->s_ibm);
+            cudaStreamWaitEvent(h->s_ibm, h->ev_fact, 0);
+            launch_ibm_solve(d, true, h->s_ibm);
         }
         cudaEventRecord(h->ev_ibm, h->s_ibm);
         {
@@ -400,14 +439,37 @@ void enqueue_step(LbmHandle* h, bool fields) {
             PhaseMark pm(h, 2, h->s_main);
             launch_fused_band(d, fields, h->s_main);
         }
-        {
-            PhaseMark pm(h, 3, h->s_main);
-            launch_outer_bc(d, h->s_main);
-        }
+        cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
         launch_step_advance(d, h->s_main);
         h->parity = 1 - h->parity;
     }
     if (h->timing) h->timed_steps += 1;
+}
+
+void drop_graphs(LbmHandle* h) {
+    for (auto& g : h->gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Two steps starting at parity p, captured from both streams (the second
+// stream joins and leaves through events, as in eager launches).
+int build_graph(LbmHandle* h, int p) {
+    const int saved = h->parity;
+    h->parity = p;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->s_main, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, false, false);
+    enqueue_step(h, false, false);
+    cudaError_t e = cudaStreamEndCapture(h->s_main, &g);
+    h->parity = saved;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->gexec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    return 0;
 }
 
 int copy_pitched_out(LbmHandle* h, const double* src, double* dst) {
@@ -494,7 +556,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         h->yb0[p] = markers_xy[2 * p + 1] + (c.yc - 0.0);
     }
     // RCM order and half bandwidth per wing
-    std::vector<int> perm(ns), bw(W);
+    std::vector<int> perm(ns), bw(W), rpos(ns);
     std::vector<long long> lofs(W);
     long long ltot = 0;
     for (int w = 0; w < W; ++w) {
@@ -507,9 +569,12 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         }
         std::vector<int> ord;
         bw[w] = rcm_order(mx, my, c.scale, ord);
-        for (int k = 0; k < nw; ++k) perm[sstart[w] + k] = sstart[w] + ord[k];
-        lofs[w] = ltot;
-        ltot += (long long)nw * (bw[w] + 1);
+        for (int k = 0; k < nw; ++k) {
+            perm[sstart[w] + k] = sstart[w] + ord[k];
+            rpos[sstart[w] + ord[k]] = k;
+        }
+        lofs[w] = ltot;   // start of the wing's storage (its leading zero row)
+        ltot += ibm_wing_storage(nw, bw[w]);
     }
 
     // allocations
@@ -530,18 +595,19 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     int* band_n = nullptr;
     if (dalloc(h, &band_n, 2) || dalloc(h, &d.band_ij, 2 * (size_t)cap) || dalloc(h, &d.band_wing, cap) ||
         dalloc(h, &d.band_rho, cap) || dalloc(h, &d.band_us, cap) || dalloc(h, &d.band_vs, cap) ||
-        dalloc(h, &d.band_du, cap) || dalloc(h, &d.band_dv, cap) || dalloc(h, &d.cover_n, cap) ||
-        dalloc(h, &d.cover_list, (size_t)cap * MAX_COVER))
+        dalloc(h, &d.band_du, cap) || dalloc(h, &d.band_dv, cap) )
         return -1;
     d.band_n = band_n;
-    int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr;
+    int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr,
+        *drpos = nullptr;
     long long* dlofs = nullptr;
     double *xb0 = nullptr, *yb0 = nullptr;
     const size_t nsz = std::max(1, ns), npz = std::max(1, np), wz = std::max(1, W);
     if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
         dalloc(h, &xb0, npz) || dalloc(h, &yb0, npz) || dalloc(h, &d.xb1, npz) || dalloc(h, &d.yb1, npz) ||
         dalloc(h, &d.xb2, nsz) || dalloc(h, &d.yb2, nsz) || dalloc(h, &d.box, 4 * nsz) ||
-        dalloc(h, &d.claim_cnt, nsz + 1) || dalloc(h, &d.pw, nsz * BOX_SLOTS) || dalloc(h, &d.pb, nsz * BOX_SLOTS) ||
+        dalloc(h, &d.claim_cnt, nsz + 1) || dalloc(h, &d.kx, 6 * nsz) || dalloc(h, &d.ky, 6 * nsz) ||
+        dalloc(h, &d.pb, nsz * BOX_SLOTS) || dalloc(h, &drpos, nsz) || dalloc(h, &d.band_claimer, (size_t)cap) ||
         dalloc(h, &d.rx, nsz) || dalloc(h, &d.ry, nsz) || dalloc(h, &d.qx, nsz) || dalloc(h, &d.qy, nsz) ||
         dalloc(h, &d.px, nsz) || dalloc(h, &d.py, nsz) || dalloc(h, &d.zx, nsz) || dalloc(h, &d.zy, nsz) ||
         dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
@@ -560,22 +626,51 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         CK(cudaMemcpy(xb0, h->xb0.data(), np * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(yb0, h->yb0.data(), np * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dperm, perm.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(drpos, rpos.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dbw, bw.data(), W * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dlofs, lofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
     }
     d.wing_pstart = pst; d.wing_sstart = sst; d.wing_npts = npw; d.seg_wing = sgw;
-    d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs;
+    d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs; d.rpos = drpos;
     h->ppw.assign(npts.begin(), npts.end());
-    // banded factor storage: shared memory when it fits
-    const size_t lbytes = (size_t)ltot * sizeof(double);
-    h->band_in_smem = lbytes <= 160 * 1024;
-    h->ibm_smem = h->band_in_smem ? lbytes : 0;
-    if (h->band_in_smem && h->ibm_smem > 0) CK(ibm_set_smem_limit(h->ibm_smem));
+    // dynamic shared memory of the factorisation kernel (one block per wing):
+    // [staged panel rows][pair table][the wing's banded factor, if it fits]
+    int bwmax = 1, nwmax = 1;
+    long long wmax = 0;
+    for (int w = 0; w < W; ++w) {
+        bwmax = std::max(bwmax, bw[w]);
+        nwmax = std::max(nwmax, npts[w] - 1);
+        wmax = std::max<long long>(wmax, ibm_wing_storage(npts[w] - 1, bw[w]));
+    }
+    if (bwmax > IBM_MAX_BANDWIDTH)
+        return fail(h, "immersed boundary: markers too dense for the banded solver (half bandwidth " +
+                           std::to_string(bwmax) + " > " + std::to_string(IBM_MAX_BANDWIDTH) + ")");
+    d.bw_max = bwmax;
+    d.nw_max = nwmax;
+    d.lband_total = ltot;
+    size_t base = (size_t)2 * (IBM_PANEL + 1) * bwmax * sizeof(double) + (size_t)bwmax * (bwmax + 1) / 2 * 4;
+    base = (base + 15) / 16 * 16;
+    const size_t smem_cap = 200 * 1024;
+    d.factor_smem_off = (long long)base;
+    d.factor_in_smem = base + (size_t)wmax * sizeof(double) <= smem_cap ? 1 : 0;
+    h->factor_smem = d.factor_in_smem ? base + (size_t)wmax * sizeof(double) : base;
+    if (h->factor_smem > smem_cap) return fail(h, "immersed boundary: too many segments for one factorisation block");
+    CK(ibm_prepare(h->factor_smem));
+    if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
+        dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
+        return -1;
     if (ensure_rows(h, 1024)) return -1;
-    CK(cudaStreamCreateWithFlags(&h->s_main, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&h->s_ibm, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&h->ev_ibm, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&h->ev_main, cudaEventDisableTiming));
+    // the immersed-boundary chain is latency-bound and on the critical path:
+    // its streams get the highest priority so their blocks are scheduled
+    // ahead of waiting bulk blocks
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&h->s_main, cudaStreamNonBlocking, prio_lo));
+    CK(cudaStreamCreateWithPriority(&h->s_ibm, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&h->s_aux, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, prio_lo));
+    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_geom, &h->ev_fact, &h->ev_bc})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
     h->pinned_n = 4096;
     if (c.precision != LBM_PRECISION_FP64) h->fc = fused_consts(d);
@@ -614,6 +709,7 @@ int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_
     if (dalloc(h, &h->d_step_table, st.size())) return -1;
     CK(cudaMemcpy(h->d_step_table, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->d.step_table = h->d_step_table;
+    drop_graphs(h);
     h->d.step_rows = steps;
     h->d.motion_dt = dt;
     return 0;
@@ -664,7 +760,17 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     CK(cudaStreamSynchronize(h->s_main));
     const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
     const bool want_err = (flags & LBM_STEP_ERR) != 0;
-    for (int64_t n = 0; n < n_steps; ++n) {
+    // all but the last two steps replay a two-step CUDA graph; the last two
+    // may write fields or diagnostics and are launched directly
+    const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
+    int64_t n = 0;
+    if (graphs) {
+        for (; n + 2 < n_steps - 1; n += 2) {
+            if (!h->gexec[h->parity] && build_graph(h, h->parity)) return -1;
+            CK(cudaGraphLaunch(h->gexec[h->parity], h->s_main));
+        }
+    }
+    for (; n < n_steps; ++n) {
         const bool last = n == n_steps - 1, second_last = n == n_steps - 2;
         bool fields = false;
         if (h->d.precision != 0 && ((want_fields && last) || (want_err && (last || second_last)))) {
@@ -681,7 +787,7 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
             }
             fields = true;
         }
-        enqueue_step(h, fields);
+        enqueue_step(h, fields, last);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->s_main));
@@ -855,6 +961,7 @@ int lbm_move_mesh(LbmHandle* h, int32_t dr) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s_main));
     h->d.movenum += dr;
+    drop_graphs(h);
     return 0;
 }
 
@@ -888,10 +995,12 @@ int lbm_set_timing(LbmHandle* h, int32_t enable) {
     return 0;
 }
 
-int lbm_get_phase_times(LbmHandle* h, double* out5) {
-    if (!h || !out5) return -1;
-    for (int k = 0; k < 4; ++k) out5[k] = h->phase_ms[k];
-    out5[4] = (double)h->timed_steps;
+int lbm_get_phase_times(LbmHandle* h, double* out, int32_t n) {
+    if (!h || !out) return -1;
+    double v[NPHASE + 1] = {0};
+    for (int k = 0; k < NPHASE; ++k) v[k] = h->phase_ms[k];
+    v[NPHASE] = (double)h->timed_steps;
+    for (int k = 0; k < n && k <= NPHASE; ++k) out[k] = v[k];
     return 0;
 }
 
@@ -909,9 +1018,14 @@ void lbm_destroy(LbmHandle* h) {
     if (h->pinned) cudaFreeHost(h->pinned);
     if (h->s_main) cudaStreamDestroy(h->s_main);
     if (h->s_ibm) cudaStreamDestroy(h->s_ibm);
+    if (h->s_aux) cudaStreamDestroy(h->s_aux);
+    if (h->s_bc) cudaStreamDestroy(h->s_bc);
+    for (cudaEvent_t e : {h->ev_geom, h->ev_fact, h->ev_bc})
+        if (e) cudaEventDestroy(e);
     if (h->ev_ibm) cudaEventDestroy(h->ev_ibm);
     if (h->ev_main) cudaEventDestroy(h->ev_main);
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+    drop_graphs(h);
     delete h;
 }
 

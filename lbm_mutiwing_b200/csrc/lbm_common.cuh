@@ -45,7 +45,6 @@ __host__ __device__ constexpr int mrt_m(int r, int q) {
 // Status bits written by kernels into DevState::status.
 enum StatusBits : int {
     ST_BAND_OVERFLOW = 1,      // band list exceeded its capacity
-    ST_COVER_OVERFLOW = 2,     // a band node is covered by too many segments
     ST_BOX_OUTSIDE = 4,        // a segment box left the lattice
     ST_PIVOT_CLAMPED = 8,      // Cholesky pivot clamped (numerically singular IBM system)
     ST_WINGS_COUPLED = 16,     // two wings share band nodes; block solve refined iteratively
@@ -54,7 +53,6 @@ enum StatusBits : int {
 };
 
 constexpr int BOX_SLOTS = 36;   // a +-2.5 spacing box spans at most 6 x 6 nodes
-constexpr int MAX_COVER = 96;   // segments that may cover one band node
 constexpr int BAND_EMPTY = 0x7fffffff;
 
 // delta kernel phi(r), smooth = 1 branch (boundary_condition.f90:1580-1600),
@@ -105,8 +103,6 @@ struct DevState {
     int* band_ij;                // 2 * cap (i, j) 0-based
     int* band_wing;              // cap
     double *band_rho, *band_us, *band_vs, *band_du, *band_dv;   // cap each
-    int* cover_n;                // cap
-    int* cover_list;             // cap * MAX_COVER (pair id = seg * 36 + slot)
     // markers
     int wing_count, npts, nseg;
     const int* wing_pstart;      // W
@@ -116,16 +112,29 @@ struct DevState {
     const double *xb0, *yb0;     // npts, body frame
     double *xb1, *yb1, *xb2, *yb2;
     int* box;                    // 4 * nseg: i1 i2 j1 j2 (1-based, inclusive)
-    int* claim_cnt;              // nseg + 1 (exclusive scan in place)
-    double* pw;                  // nseg * 36 delta weights
+    int* claim_cnt;              // nseg + 1: band-list offset of each segment's claims
+    double *kx, *ky;             // 6 * nseg: delta values of each box column / row
     int* pb;                     // nseg * 36 band index per slot (-1 outside box)
+    int* band_claimer;           // cap: segment that claimed each band node
+    const int* rpos;             // nseg: position of each segment in its wing's RCM order
+    int diag;                    // compute the no-slip residual this step
+    int write_fields;            // fused path: this step writes rho, u, v fields
     double *rx, *ry;             // nseg right-hand sides, overwritten by solutions
     double *qx, *qy, *px, *py, *zx, *zy;  // nseg work vectors for coupled refinement
     // banded Cholesky per wing (RCM order)
     const int* perm;             // nseg: local position -> global segment
     const int* wing_bw;          // W half bandwidths
     const long long* wing_lofs;  // W offsets into lband
-    double* lband;               // sum_w nw*(bw+1)
+    double* lband;               // sum_w nw*(bw+1), used when not in shared memory
+    long long lband_total;       // doubles in lband
+    double* piv_floor;           // W pivot floors of the last factorisation
+    double* ymax;                // 2 W largest |y| of the last solve, per component (spread scale)
+    int* ibm_flags;              // [0] wings with overlapping supports this step
+    double* force_part;          // per-block partial force sums: blocks x W x 3
+    int bw_max;                  // largest half bandwidth
+    int nw_max;                  // largest segment count of a wing
+    int factor_in_smem;          // a wing's banded factor fits in shared memory
+    long long factor_smem_off;   // its byte offset in the factor kernel's shared memory
     // configuration of wing placement
     double wing_x_origin, wing_x_spacing, wing_y_origin, xc, yc;
     // motion source

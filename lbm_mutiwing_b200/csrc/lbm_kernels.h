@@ -28,10 +28,30 @@ void launch_fused_export(const DevState& d, const float* g, double* f, cudaStrea
 void launch_fused_import(const DevState& d, const double* f, float* g, cudaStream_t st);
 
 // immersed boundary (ibm.cu)
-void launch_ibm_band(const DevState& d, cudaStream_t st);            // move_boundary
-void launch_ibm_solve(const DevState& d, size_t smem, bool band_in_smem, cudaStream_t st);
-void launch_ibm_full(const DevState& d, size_t smem, bool band_in_smem, cudaStream_t st);
+// move_boundary: motion, markers, boxes, band list; geometry_done (may be
+// null) is recorded once the boxes and kernel values exist
+void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done);
+// assembly and factorisation of G (needs the geometry only)
+void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st);
+// u*, right-hand side (needs the band list; on the plain path also the moments)
+void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st);
+// substitution, spread, velocity correction, forces (needs rhs and factor)
+void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st);
+cudaError_t ibm_prepare(size_t factor_smem);
+int ibm_finish_blocks(const DevState& d);
+constexpr int IBM_PANEL = 8;           // columns per factorisation panel
+constexpr int IBM_MAX_BANDWIDTH = 88;  // register panel: bandwidth + panel <= 96 rows
+// Banded storage of a wing's G: row p holds G(p, p - dd) at dd = 0..bw.
+// The row stride covers bw + IBM_PANEL + 1 entries, so the entries past bw
+// form a zero zone, and a zero row precedes row 0 and IBM_PANEL + bw zero
+// rows follow the last: a panel's rows and columns can then be read without
+// bounds tests (entries above the diagonal alias the previous row's zero
+// zone).  The stride is even, so the diagonal-major accesses of a warp hit
+// distinct shared-memory banks.
+inline __host__ __device__ int ibm_ld(int bw) { return (bw + IBM_PANEL + 2) & ~1; }
+inline __host__ __device__ long long ibm_wing_storage(int nw, int bw) {
+    return (long long)(1 + nw + IBM_PANEL + bw) * ibm_ld(bw);
+}
 void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle += 1
-int ibm_threads();
 
 }  // namespace lbm

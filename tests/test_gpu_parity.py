@@ -195,3 +195,16 @@ def test_fused_move_mesh(gpu_lib):
             s.move_mesh(-1)
             s.step(4, first_cycle=5, rows=False)
         assert rel(s32.f(), s64.f()) < 1e-6
+
+
+def test_graph_replay_matches_direct_launches(gpu_lib):
+    ep = episode_b(13)
+    out = []
+    for graphs in (True, False):
+        for prec in (api.PRECISION_FP64, api.PRECISION_FP32):
+            with api.Simulation(ep, prec, graphs=graphs) as s:
+                rows = s.step(13)
+                out.append((prec, rows, s.f()))
+    for k in range(2):
+        assert np.array_equal(out[k][1], out[k + 2][1])
+        assert np.array_equal(out[k][2], out[k + 2][2])
