@@ -50,9 +50,6 @@
 namespace lbm {
 
 constexpr int MAX_WINGS = 16;
-constexpr int FACTOR_THREADS = 128;     // threads of a factorisation block
-constexpr int PANEL = IBM_PANEL;        // columns per factorisation panel
-constexpr int ROWS_PER_LANE = 3;        // register panel rows per lane: bw + PANEL <= 96
 constexpr int FINISH_THREADS = 256;
 constexpr int BORDER_GAP = 3;           // support boxes keep this many nodes off the border
 
@@ -64,15 +61,6 @@ __device__ inline double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ inline double sub(double a, double b) { return __dsub_rn(a, b); }
 // node coordinate ox + scale * (i - 1) as the reference rounds it
 __device__ inline double node_x(double o, double scale, int i) { return add(o, mul(scale, (double)(i - 1))); }
-
-// 1/x from a single-precision seed and two Newton steps (relative error
-// below 1e-16 for the positive pivots met here).
-__device__ inline double fast_recip(double x) {
-    double r = (double)__frcp_rn((float)x);
-    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
-    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
-    return r;
-}
 
 // smooth ramp functions of the online motion (mode.f90:220-261)
 __device__ inline double smooth_r(double x) {
@@ -425,209 +413,6 @@ __global__ void ibm_assemble_kernel(DevState d, long long total) {
     d.lband[t] = (p >= 0 && p < nw && q >= 0 && dd <= bw) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
 }
 
-// Right-looking banded L' D L'^T of wing w's G (RCM order), PANEL columns at
-// a time, one block of FACTOR_THREADS per wing.  Warp 0 factors a panel with
-// its PANEL + bw rows held in registers (ROWS_PER_LANE per lane, column
-// entries exchanged by warp shuffles); the block then applies the panel's
-// rank-PANEL update to the trailing window from a staged copy in shared
-// memory.  On exit lband holds d_k (clamped) on the diagonal and
-// L'(i,k) = A(i,k) / d_k below it.  Pivots below 1e-15 of the largest
-// diagonal are clamped (numerically singular systems made by marker clusters
-// finer than the lattice).
-__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) {
-    extern __shared__ double smem[];
-    const int w = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
-    constexpr int SP = PANEL + 1;   // odd row stride of the staged panel
-    double* Ps = smem;                        // [bw][SP] scaled rows below the panel
-    double* Pu = Ps + SP * d.bw_max;          // [bw][SP] unscaled rows
-    short2* pairs = reinterpret_cast<short2*>(Pu + SP * d.bw_max);
-    __shared__ double red[FACTOR_THREADS / 32];
-    __shared__ double pinv[PANEL];
-    const long long wsize = ibm_wing_storage(nw, bw);
-    double* gS = d.lband + d.wing_lofs[w];
-    double* S = gS;
-    if (d.factor_in_smem) {
-        S = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + d.factor_smem_off);
-        for (long long t = tid; t < wsize; t += FACTOR_THREADS) S[t] = gS[t];
-    }
-    double* A = S + ld;   // row 0
-    const int P = bw * (bw + 1) / 2;
-    for (int t = tid; t < P; t += FACTOR_THREADS) {
-        int r1 = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-        while (r1 * (r1 + 1) / 2 > t) --r1;
-        while ((r1 + 1) * (r1 + 2) / 2 <= t) ++r1;
-        pairs[t] = make_short2((short)r1, (short)(t - r1 * (r1 + 1) / 2));
-    }
-    __syncthreads();
-    double mx = 0.0;
-    for (int p = tid; p < nw; p += FACTOR_THREADS) mx = fmax(mx, A[p * ld]);
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) red[warp] = mx;
-    __syncthreads();
-    mx = 0.0;
-    for (int k = 0; k < FACTOR_THREADS / 32; ++k) mx = fmax(mx, red[k]);
-    const double fl = mx > 0.0 ? 1e-15 * mx : 1.0;
-    bool clamped = false;
-
-    for (int k0 = 0; k0 < nw; k0 += PANEL) {
-        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
-        if (warp == 0) {
-            // rows k0 + r, r = lane + 32 h; entry c is A(k0 + r, k0 + c) at
-            // offset r - c of the row (zero zones make every read valid)
-            double pr[ROWS_PER_LANE][PANEL];
-#pragma unroll
-            for (int h = 0; h < ROWS_PER_LANE; ++h) {
-                const int r = lane + 32 * h;
-                const double* row = A + (k0 + r) * ld + r;
-#pragma unroll
-                for (int c = 0; c < PANEL; ++c) pr[h][c] = (r < PANEL + bw) ? row[-c] : 0.0;
-            }
-            double icv[PANEL];
-#pragma unroll
-            for (int c = 0; c < PANEL; ++c) {
-                // column k0 + c: pivot in lane c (h = 0), A(k0 + j, k0 + c) in lane j
-                double dc = __shfl_sync(0xffffffffu, pr[0][c], c);
-                double col[PANEL];
-#pragma unroll
-                for (int j = c + 1; j < PANEL; ++j) col[j] = __shfl_sync(0xffffffffu, pr[0][c], j);
-                icv[c] = 0.0;
-                if (c < np) {
-                    if (!(dc > fl)) { dc = fl; clamped = true; }
-                    const double ic = fast_recip(dc);
-                    icv[c] = ic;
-                    if (lane == c) pr[0][c] = dc;
-#pragma unroll
-                    for (int h = 0; h < ROWS_PER_LANE; ++h) {
-                        const int r = lane + 32 * h;
-                        if (h == 0 && r <= c) continue;
-                        const double a = pr[h][c] * ic;
-#pragma unroll
-                        for (int j = c + 1; j < PANEL; ++j)
-                            if (h > 0 || j <= r) pr[h][j] = pr[h][j] - a * col[j];
-                    }
-                }
-            }
-            // d on the diagonal, the scaled L' below it; the rows below the
-            // panel are staged (scaled and unscaled) for the trailing update
-#pragma unroll
-            for (int h = 0; h < ROWS_PER_LANE; ++h) {
-                const int r = lane + 32 * h;
-                if (r >= PANEL + bw) continue;
-                double* row = A + (k0 + r) * ld + r;
-#pragma unroll
-                for (int c = 0; c < PANEL; ++c) {
-                    if (h == 0 && r < c) continue;   // above the diagonal
-                    row[-c] = (h == 0 && r == c) ? pr[h][c] : pr[h][c] * icv[c];
-                }
-                const int rb = r - np;   // row k1 + rb of the trailing window
-                if (rb >= 0 && rb < bw) {
-#pragma unroll
-                    for (int c = 0; c < PANEL; ++c) {
-                        Pu[rb * SP + c] = pr[h][c];
-                        Ps[rb * SP + c] = pr[h][c] * icv[c];
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        // trailing update (zero rows past the end absorb the updates of the
-        // last panels)
-        for (int t = tid; t < P; t += FACTOR_THREADS) {
-            const short2 pq = pairs[t];
-            const double* a = Ps + pq.x * SP;
-            const double* b = Pu + pq.y * SP;
-            double acc = 0.0;
-#pragma unroll
-            for (int c = 0; c < PANEL; ++c) acc = acc + a[c] * b[c];
-            double* e = A + (k1 + pq.x) * ld + (pq.x - pq.y);
-            *e = *e - acc;
-        }
-        __syncthreads();
-    }
-    if (clamped) set_status(d, ST_PIVOT_CLAMPED);
-    if (d.factor_in_smem)
-        for (long long t = tid; t < wsize; t += FACTOR_THREADS) gS[t] = S[t];
-}
-
-// Forward and backward substitution with the factor of wing w: warp 0 solves
-// for the x component, warp 1 for the y component.  Panel rows sit in
-// registers; within a panel the unknowns pass by shuffles; the forward sweep
-// updates the rows below a panel, the backward sweep the rows above it.
-__global__ void __launch_bounds__(64) ibm_solve_kernel(DevState d) {
-    extern __shared__ double zsh[];
-    const int w = blockIdx.x;
-    const int lane = threadIdx.x & 31, comp = threadIdx.x >> 5;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
-    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
-    double* rr = comp == 0 ? d.rx : d.ry;
-    double* z = zsh + comp * (d.nw_max + PANEL + d.bw_max);   // zero tail past nw
-    for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? rr[d.perm[s0 + p]] : 0.0;
-    __syncwarp();
-    // L' D v = r
-    for (int k0 = 0; k0 < nw; k0 += PANEL) {
-        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
-        double zr[ROWS_PER_LANE], lr[ROWS_PER_LANE][PANEL];
-#pragma unroll
-        for (int h = 0; h < ROWS_PER_LANE; ++h) {
-            const int r = lane + 32 * h, i = k0 + r;
-            const bool ok = r < PANEL + bw;
-            zr[h] = ok ? z[i] : 0.0;
-            const double* row = A + i * ld + r;
-#pragma unroll
-            for (int c = 0; c < PANEL; ++c)   // L'(i, k0 + c), zero on and above the diagonal
-                lr[h][c] = (ok && c < np && (h > 0 || r > c)) ? row[-c] : 0.0;
-        }
-#pragma unroll
-        for (int c = 0; c < PANEL; ++c) {
-            const double wc = __shfl_sync(0xffffffffu, zr[0], c);
-#pragma unroll
-            for (int h = 0; h < ROWS_PER_LANE; ++h) zr[h] = zr[h] - lr[h][c] * wc;
-        }
-#pragma unroll
-        for (int h = 0; h < ROWS_PER_LANE; ++h) {
-            const int r = lane + 32 * h, i = k0 + r;
-            if (r < PANEL + bw) z[i] = (r < np) ? zr[h] * fast_recip(A[i * ld]) : zr[h];
-        }
-        __syncwarp();
-    }
-    // L'^T y = v
-    const int last0 = ((nw - 1) / PANEL) * PANEL;
-    for (int k0 = last0; k0 >= 0; k0 -= PANEL) {
-        const int k1 = min(k0 + PANEL, nw), np = k1 - k0;
-        double y = lane < np ? z[k0 + lane] : 0.0;
-#pragma unroll
-        for (int e = PANEL - 1; e >= 0; --e) {
-            const double ye = __shfl_sync(0xffffffffu, y, e);
-            if (e < np && lane < e && e - lane <= bw) y = y - A[(k0 + e) * ld + (e - lane)] * ye;
-        }
-        double yc[PANEL];
-#pragma unroll
-        for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, y, c);
-        if (lane < np) z[k0 + lane] = y;
-        for (int r = lane; r < bw; r += 32) {
-            const int j = k0 - 1 - r;   // rows above the panel
-            if (j < 0) break;
-            double acc = 0.0;
-#pragma unroll
-            for (int c = 0; c < PANEL; ++c) {
-                const int dd = k0 + c - j;
-                if (c < np && dd <= bw) acc = acc + A[(k0 + c) * ld + dd] * yc[c];
-            }
-            z[j] = z[j] - acc;
-        }
-        __syncwarp();
-    }
-    double ym = 0.0;
-    for (int p = lane; p < nw; p += 32) {
-        rr[d.perm[s0 + p]] = z[p];
-        ym = fmax(ym, fabs(z[p]));
-    }
-    for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
-    if (lane == 0) d.ymax[2 * w + comp] = ym;
-}
-
 // Fixed-point exponent shared by the spread and the finish kernels: every
 // contribution is below 2^(62 - 10) in magnitude after scaling, so sums of up
 // to 1024 of them cannot overflow.
@@ -815,10 +600,6 @@ __global__ void step_advance_kernel(DevState d) {
 // ------------------------------------------------------------ host side
 static inline int blocks(long long n, int t) { return (int)std::max<long long>(1, (n + t - 1) / t); }
 
-cudaError_t ibm_prepare(size_t factor_smem) {
-    return cudaFuncSetAttribute(ibm_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem);
-}
-
 int ibm_finish_blocks(const DevState& d) { return blocks(d.band_cap, FINISH_THREADS); }
 
 void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done) {
@@ -834,7 +615,7 @@ void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_do
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
     const long long total = d.lband_total;
     ibm_assemble_kernel<<<blocks(total, 256), 256, 0, st>>>(d, total);
-    if (d.wing_count > 0) ibm_factor_kernel<<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
+    launch_ibm_factor_blocks(d, factor_smem, st);
 }
 
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
@@ -846,8 +627,7 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
 }
 
 void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st) {
-    if (d.wing_count > 0)
-        ibm_solve_kernel<<<d.wing_count, 64, 2 * (d.nw_max + PANEL + d.bw_max) * sizeof(double), st>>>(d);
+    launch_ibm_substitution(d, (size_t)d.solve_smem, st);
     ibm_spread_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
     const int nbk = ibm_finish_blocks(d);
     if (fused)

@@ -1,0 +1,452 @@
+// Banded L' D L'^T factorisation and substitution for the immersed-boundary
+// system G y = r of each wing (G = X X^T in reverse Cuthill-McKee order; see
+// ibm.cu for how G arises from immersed_boundary_Wu,
+// boundary_condition.f90:1558-1640).
+//
+// Blocked right-looking algorithm, PANEL = 8 columns at a time, one thread
+// block per wing, the wing's banded matrix held in shared memory (brought in
+// and written back with bulk copies).  Per panel p, two phases separated by
+// block barriers:
+//   B  every row below the panel (bw of them, one thread each) becomes
+//      L'(i, p) = A(i, p) L_pp^-T D_p^-1 by an 8-step forward substitution;
+//      a spare warp forms the inverse of L_pp for the substitution kernel;
+//   A  the rank-8 update of the trailing window, in 4 x 4 register tiles by
+//      warps 1.., while warp 0 updates the next panel's 8 x 8 diagonal block
+//      first and one thread factors it in registers (look-ahead: the
+//      sequential pivot chain of panel p + 1 overlaps panel p's update).
+// The substitution applies each panel through its stored 8 x 8 inverse and
+// reciprocal pivots and updates the rows below (forward) or above
+// (backward) it, one warp per velocity component.
+//
+// The zero zones of the banded storage (entries past the bandwidth, rows past
+// the last segment) make every panel-shaped read in bounds and zero where it
+// falls outside the matrix, so the inner loops load without conditions.
+#include "bulk_copy.cuh"
+#include "lbm_kernels.h"
+
+namespace lbm {
+
+constexpr int PANEL = IBM_PANEL;
+constexpr int FACTOR_THREADS = 256;
+constexpr int FACTOR_WARPS = FACTOR_THREADS / 32;
+constexpr int SOLVE_THREADS = 64;
+constexpr int SP = PANEL + 1;           // odd row stride of staged panel rows
+constexpr int TILE = 4;                 // register tile of the trailing update
+static_assert(IBM_MAX_BANDWIDTH <= FACTOR_THREADS - 32, "rows below a panel leave the last warp free");
+static_assert(PANEL == 2 * TILE, "the next diagonal block is three tiles");
+
+__device__ inline void solver_status(const DevState& d, int bit) { atomicOr(d.status, bit); }
+
+// 1/x by Newton-Raphson (r <- r + r (1 - x r), twice) from the hardware
+// approximation rcp.approx.ftz.f64; the relative error of the seed squares
+// at each step, ending at the rounding level for the positive normal pivots
+// met here.
+__device__ inline double recip(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
+    r = __fma_rn(r, __fma_rn(-x, r, 1.0), r);
+    return r;
+}
+
+// Packed lower triangle.
+__host__ __device__ constexpr int tri(int x, int y) { return x * (x + 1) / 2 + y; }
+// Row of packed index t.
+__device__ inline int tri_row(int t) {
+    int r = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (r * (r + 1) / 2 > t) --r;
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    return r;
+}
+inline int round_tile(int n) { return (n + TILE - 1) / TILE * TILE; }
+
+// One thread factors the diagonal block of the panel at k0 (np columns, the
+// rest zero rows) held in storage and leaves the strictly lower part of its
+// unit factor in Lpp and the reciprocal pivots (zero past np) in idp.
+// Pivots not above fl are clamped to fl; returns whether any was.
+__device__ inline bool factor_diagonal_block(const double* A, int ld, int k0, int np, double fl, double (*Lpp)[SP],
+                                             double* idp) {
+    double a[tri(PANEL, 0)];
+#pragma unroll
+    for (int x = 0; x < PANEL; ++x)
+#pragma unroll
+        for (int y = 0; y <= x; ++y) a[tri(x, y)] = A[(k0 + x) * ld + (x - y)];
+    bool clamped = false;
+#pragma unroll
+    for (int c = 0; c < PANEL; ++c) {
+        const bool live = c < np;
+        double dc = a[tri(c, c)];
+        const bool low = live && !(dc > fl);
+        clamped |= low;
+        dc = low ? fl : dc;
+        double ic = recip(dc);
+        ic = live ? ic : 0.0;
+        idp[c] = ic;
+        double l[PANEL];
+#pragma unroll
+        for (int x = c + 1; x < PANEL; ++x) l[x] = a[tri(x, c)] * ic;
+#pragma unroll
+        for (int x = c + 1; x < PANEL; ++x)
+#pragma unroll
+            for (int y = c + 1; y <= x; ++y) a[tri(x, y)] = a[tri(x, y)] - l[x] * a[tri(y, c)];
+#pragma unroll
+        for (int x = c + 1; x < PANEL; ++x) a[tri(x, c)] = l[x];
+    }
+#pragma unroll
+    for (int x = 1; x < PANEL; ++x)
+#pragma unroll
+        for (int y = 0; y < x; ++y) Lpp[x][y] = a[tri(x, y)];
+    return clamped;
+}
+
+// Storage (ibm_wing_storage): row p of wing w at S + (p + 1) * ld, entry dd
+// holding column p - dd.  On exit: L'(i, k) for every entry below the
+// diagonal blocks, and per panel the inverse of its unit lower diagonal
+// block and the reciprocal pivots in d.linv (the diagonal blocks of the
+// storage are left as scratch).  Pivots below 1e-15 of the largest diagonal
+// are clamped (numerically singular systems made by marker clusters finer
+// than the lattice).
+__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) {
+    extern __shared__ __align__(16) double smem[];
+    const int w = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
+    const int bwr = (d.bw_max + TILE - 1) / TILE * TILE;
+    double* Ps = smem;                        // [bwr][SP] rows below the panel, scaled (L')
+    double* Pu = Ps + SP * bwr;               // [bwr][SP] unscaled (L' D)
+    short2* tiles = reinterpret_cast<short2*>(Pu + SP * bwr);   // tiles of the remaining rows
+    __shared__ double red[FACTOR_WARPS];
+    __shared__ double Lpp[PANEL][SP];         // strictly lower part of the panel's unit lower block
+    __shared__ double idp[PANEL];             // reciprocal pivots of the panel
+    __shared__ uint64_t bar;
+    const long long wsize = ibm_wing_storage(nw, bw);
+    double* gS = d.lband + d.wing_lofs[w];
+    double* S = gS;
+    const bool in_smem = d.factor_in_smem != 0;
+    if (in_smem) {
+        S = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + d.factor_smem_off);
+        if (tid == 0) {
+            mbar_init(&bar, 1);
+            mbar_arrive_expect_tx(&bar, (uint32_t)(wsize * 8));
+            bulk_load_all(S, gS, wsize * 8, &bar);
+        }
+    }
+    double* A = S + ld;   // row 0
+    double* aux = d.linv + d.wing_linv_ofs[w];
+    for (int t = tid; t < 2 * SP * bwr; t += FACTOR_THREADS) Ps[t] = 0.0;   // rows past bw stay zero
+    // the next diagonal block: entries (x, y), y <= x < b8; the remaining
+    // rows of the trailing window in TILE x TILE tiles (X, Y), Y <= X,
+    // X >= PANEL / TILE
+    const int b8 = min(bw, PANEL), n8 = tri(b8, 0);
+    const int nt = (bw + TILE - 1) / TILE;
+    const int nrem = nt > PANEL / TILE ? tri(nt, 0) - tri(PANEL / TILE, 0) : 0;
+    for (int t = tid; t < nrem; t += FACTOR_THREADS) {
+        const int tt = t + tri(PANEL / TILE, 0), X = tri_row(tt);
+        tiles[t] = make_short2((short)X, (short)(tt - tri(X, 0)));
+    }
+    int ex[2], ey[2];   // warp 0: entries lane and lane + 32 of the next diagonal block
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int t = min(lane + 32 * h, tri(PANEL, 0) - 1);
+        ex[h] = tri_row(t);
+        ey[h] = t - tri(ex[h], 0);
+    }
+    __syncthreads();
+    if (in_smem) {
+        const bool ok = mbar_wait(&bar, 0);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+            mbar_wait(&bar, 0);   // let a late copy land before the block exits
+            return;
+        }
+    }
+    double mx = 0.0;
+    for (int p = tid; p < nw; p += FACTOR_THREADS) mx = fmax(mx, A[p * ld]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    mx = 0.0;
+    for (int k = 0; k < FACTOR_WARPS; ++k) mx = fmax(mx, red[k]);
+    const double fl = mx > 0.0 ? 1e-15 * mx : 1.0;
+    bool clamped = false;
+    if (tid == 0) clamped = factor_diagonal_block(A, ld, 0, min(PANEL, nw), fl, Lpp, idp);
+    __syncthreads();
+
+    const int npan = (nw + PANEL - 1) / PANEL;
+    for (int pan = 0; pan < npan; ++pan) {
+        const int k0 = pan * PANEL, k1 = min(k0 + PANEL, nw);
+        // B. rows below the panel: u = A(i, p) L_pp^-T, L'(i, p) = u / d
+        // (past the last segment the rows and the pivots are zero)
+        if (tid < bw) {
+            const int rb = tid, i = k1 + rb;
+            double* rw = A + i * ld + (i - k0);   // entry of column k0 + c at rw[-c]
+            double u[PANEL], lo[tri(PANEL, 0)], ip[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) u[c] = rw[-c];
+#pragma unroll
+            for (int c = 1; c < PANEL; ++c)
+#pragma unroll
+                for (int k = 0; k < c; ++k) lo[tri(c, k)] = Lpp[c][k];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) ip[c] = idp[c];
+#pragma unroll
+            for (int c = 1; c < PANEL; ++c)
+#pragma unroll
+                for (int k = 0; k < c; ++k) u[c] = u[c] - lo[tri(c, k)] * u[k];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) {
+                const double lv = u[c] * ip[c];
+                Pu[rb * SP + c] = u[c];
+                Ps[rb * SP + c] = lv;
+                rw[-c] = lv;
+            }
+        } else if (warp == FACTOR_WARPS - 1 && lane < PANEL) {
+            // inverse of the unit lower block, column lane, and the pivots
+            const int l = lane;
+            double x[PANEL];
+#pragma unroll
+            for (int k = 0; k < PANEL; ++k) {
+                double s = (k == l) ? 1.0 : 0.0;
+#pragma unroll
+                for (int m = 0; m < k; ++m) s = s - Lpp[k][m] * x[m];
+                x[k] = (k < l) ? 0.0 : s;
+            }
+            double* blk = aux + (long long)pan * IBM_PANEL_AUX;
+#pragma unroll
+            for (int k = 0; k < PANEL; ++k) blk[k * PANEL + l] = x[k];
+            blk[PANEL * PANEL + l] = idp[l];
+        }
+        __syncthreads();
+        if (pan + 1 == npan) break;   // later updates only touch the zero rows past the end
+        // A. trailing update; warp 0 takes the next diagonal block first
+        if (warp == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (lane + 32 * h >= n8) break;
+                const int x = ex[h], y = ey[h];
+                const double* pa = Ps + x * SP;
+                const double* pb = Pu + y * SP;
+                double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    acc0 = acc0 + pa[c] * pb[c];
+                    acc1 = acc1 + pa[c + PANEL / 2] * pb[c + PANEL / 2];
+                }
+                double* e = A + (k1 + x) * ld + (x - y);
+                *e = *e - (acc0 + acc1);
+            }
+            __syncwarp();
+            if (lane == 0) clamped |= factor_diagonal_block(A, ld, k1, min(PANEL, nw - k1), fl, Lpp, idp);
+        } else {
+          for (int t = tid - 32; t < nrem; t += FACTOR_THREADS - 32) {
+            const short2 tl = tiles[t];
+            const int x0 = TILE * tl.x, y0 = TILE * tl.y;
+            double acc[TILE][TILE];
+#pragma unroll
+            for (int r = 0; r < TILE; ++r)
+#pragma unroll
+                for (int s = 0; s < TILE; ++s) acc[r][s] = 0.0;
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) {
+                double pa[TILE], pb[TILE];
+#pragma unroll
+                for (int r = 0; r < TILE; ++r) {
+                    pa[r] = Ps[(x0 + r) * SP + c];
+                    pb[r] = Pu[(y0 + r) * SP + c];
+                }
+#pragma unroll
+                for (int r = 0; r < TILE; ++r)
+#pragma unroll
+                    for (int s = 0; s < TILE; ++s) acc[r][s] = acc[r][s] + pa[r] * pb[s];
+            }
+#pragma unroll
+            for (int r = 0; r < TILE; ++r)
+#pragma unroll
+                for (int s = 0; s < TILE; ++s) {
+                    const int x = x0 + r, y = y0 + s;
+                    if (x < bw && y <= x) {
+                        double* e = A + (k1 + x) * ld + (x - y);
+                        *e = *e - acc[r][s];
+                    }
+                }
+          }
+        }
+        __syncthreads();
+    }
+    if (clamped) solver_status(d, ST_PIVOT_CLAMPED);
+    if (in_smem) {
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) bulk_store_all(gS, S, wsize * 8);
+    }
+}
+
+// Forward and backward substitution with the factor of wing w: warp 0 solves
+// for the x component, warp 1 for the y component, on shared-memory copies
+// of the per-panel inverses and pivots, of the factor (when it fits) and of
+// the right-hand sides.  Shared memory: [2 right-hand sides with zero tails]
+// [permutation][per-panel inverse blocks and pivots][factor].  Each lane
+// updates rows lane and lane + 32 below or above a panel (bw <= 64) or loops.
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ uint64_t bar;
+    const int w = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+    const int npan = (nw + PANEL - 1) / PANEL;
+    const int zlen = d.nw_max + PANEL + d.bw_max;
+    double* z = sm + comp * zlen;
+    int* perm = reinterpret_cast<int*>(sm + 2 * zlen);
+    double* Lsh = reinterpret_cast<double*>(perm + ((d.nw_max + 3) & ~3));
+    double* Sm = Lsh + ibm_linv_storage(d.nw_max);
+    const double* gS = d.lband + d.wing_lofs[w];
+    const long long lbytes = (long long)npan * IBM_PANEL_AUX * 8;
+    const long long sbytes = d.solve_in_smem ? ibm_wing_storage(nw, bw) * 8 : 0;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, (uint32_t)(lbytes + sbytes));
+        bulk_load_all(Lsh, d.linv + d.wing_linv_ofs[w], lbytes, &bar);
+        if (sbytes) bulk_load_all(Sm, gS, sbytes, &bar);
+    }
+#pragma unroll 4
+    for (int p = tid; p < nw; p += SOLVE_THREADS) perm[p] = d.perm[s0 + p];
+    __syncthreads();
+    double* rr = comp == 0 ? d.rx : d.ry;
+#pragma unroll 8
+    for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? rr[perm[p]] : 0.0;
+    const bool ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+        mbar_wait(&bar, 0);
+        return;
+    }
+    const double* A = (d.solve_in_smem ? Sm : gS) + ld;   // row 0
+    const int li = lane & (PANEL - 1);
+    // L' D v = r: per panel w_p = Li_p z_p, v_p = w_p / d, rows below -= L' w_p
+    for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {
+        const int np = min(PANEL, nw - k0);
+        const double* Li = Lsh + pan * IBM_PANEL_AUX;
+        double zk[PANEL], lk[PANEL];
+#pragma unroll
+        for (int k = 0; k < PANEL; ++k) {
+            zk[k] = z[k0 + k];
+            lk[k] = Li[li * PANEL + k];
+        }
+        double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < PANEL / 2; ++k) {
+            w0 = w0 + lk[k] * zk[k];
+            w1 = w1 + lk[k + PANEL / 2] * zk[k + PANEL / 2];
+        }
+        const double wl = w0 + w1;
+        double wc[PANEL];
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
+        for (int rb0 = 0; rb0 < bw; rb0 += 64) {
+            double acc[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rb = min(rb0 + lane + 32 * h, bw - 1);
+                const int i = k0 + np + rb;
+                const double* row = A + i * ld + (i - k0);
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + row[-c] * wc[c];
+                    a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
+                }
+                acc[h] = a0 + a1;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rb = rb0 + lane + 32 * h;
+                if (rb < bw) z[k0 + np + rb] -= acc[h];
+            }
+        }
+        if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
+        __syncwarp();
+    }
+    // L'^T y = v: per panel (last first) y_p = Li_p^T v_p, rows above -= L'^T y_p
+    for (int pan = npan - 1; pan >= 0; --pan) {
+        const int k0 = pan * PANEL;
+        const double* Li = Lsh + pan * IBM_PANEL_AUX;
+        double vk[PANEL], lk[PANEL];
+#pragma unroll
+        for (int k = 0; k < PANEL; ++k) {
+            vk[k] = z[k0 + k];
+            lk[k] = Li[k * PANEL + li];
+        }
+        double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < PANEL / 2; ++k) {
+            y0 = y0 + lk[k] * vk[k];
+            y1 = y1 + lk[k + PANEL / 2] * vk[k + PANEL / 2];
+        }
+        const double yl = y0 + y1;
+        double yc[PANEL];
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
+        const int above = min(bw, k0);   // rows k0 - above .. k0 - 1
+        for (int r0 = 0; r0 < above; r0 += 64) {
+            double acc[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = min(r0 + lane + 32 * h, above - 1);
+                const int j = k0 - 1 - r;
+                const double* col = A + k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + col[c * (ld + 1)] * yc[c];
+                    a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
+                }
+                acc[h] = a0 + a1;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + lane + 32 * h;
+                if (r < above) z[k0 - 1 - r] -= acc[h];
+            }
+        }
+        if (lane < PANEL) z[k0 + lane] = yl;
+        __syncwarp();
+    }
+    double ym = 0.0;
+#pragma unroll 4
+    for (int p = lane; p < nw; p += 32) {
+        rr[perm[p]] = z[p];
+        ym = fmax(ym, fabs(z[p]));
+    }
+    for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
+    if (lane == 0) d.ymax[2 * w + comp] = ym;
+}
+
+size_t ibm_factor_staging_bytes(int bw_max) {
+    const int nt = round_tile(bw_max) / TILE;
+    const size_t rows = (size_t)2 * SP * round_tile(bw_max) * sizeof(double);   // a multiple of 16
+    const size_t tl = (size_t)tri(nt, 0) * sizeof(short2);
+    return rows + (tl + 15) / 16 * 16;
+}
+
+size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool factor_in_smem) {
+    const size_t z = (size_t)2 * (nw_max + PANEL + bw_max) * sizeof(double);
+    const size_t perm = (size_t)((nw_max + 3) & ~3) * sizeof(int);
+    const size_t inv = (size_t)ibm_linv_storage(nw_max) * sizeof(double);
+    return z + perm + inv + (factor_in_smem ? (size_t)wing_storage_max * sizeof(double) : 0);
+}
+
+cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
+    cudaError_t e = cudaFuncSetAttribute(ibm_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(ibm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem);
+}
+
+void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st) {
+    if (d.wing_count > 0) ibm_factor_kernel<<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
+}
+
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st) {
+    if (d.wing_count > 0) ibm_solve_kernel<<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+}
+
+}  // namespace lbm

@@ -320,12 +320,13 @@ int check_status(LbmHandle* h) {
     int st = 0;
     CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
     h->status_seen |= st;
-    const int fatal = ST_BAND_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION;
+    const int fatal = ST_BAND_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION | ST_COPY_TIMEOUT;
     if (st & fatal) {
         std::string m = "immersed boundary:";
         if (st & ST_BAND_OVERFLOW) m += " band capacity exceeded;";
         if (st & ST_BOX_OUTSIDE) m += " a wing's support box left the lattice;";
         if (st & ST_MOTION) m += " no motion rows loaded;";
+        if (st & ST_COPY_TIMEOUT) m += " a shared-memory bulk copy timed out;";
         return fail(h, m);
     }
     return 0;
@@ -557,8 +558,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     // RCM order and half bandwidth per wing
     std::vector<int> perm(ns), bw(W), rpos(ns);
-    std::vector<long long> lofs(W);
-    long long ltot = 0;
+    std::vector<long long> lofs(W), iofs(W);
+    long long ltot = 0, itot = 0;
     for (int w = 0; w < W; ++w) {
         const int nw = npts[w] - 1;
         std::vector<double> mx(nw), my(nw);
@@ -575,6 +576,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         }
         lofs[w] = ltot;   // start of the wing's storage (its leading zero row)
         ltot += ibm_wing_storage(nw, bw[w]);
+        iofs[w] = itot;
+        itot += ibm_linv_storage(nw);
     }
 
     // allocations
@@ -600,7 +603,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.band_n = band_n;
     int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr,
         *drpos = nullptr;
-    long long* dlofs = nullptr;
+    long long *dlofs = nullptr, *diofs = nullptr;
     double *xb0 = nullptr, *yb0 = nullptr;
     const size_t nsz = std::max(1, ns), npz = std::max(1, np), wz = std::max(1, W);
     if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
@@ -611,7 +614,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         dalloc(h, &d.rx, nsz) || dalloc(h, &d.ry, nsz) || dalloc(h, &d.qx, nsz) || dalloc(h, &d.qy, nsz) ||
         dalloc(h, &d.px, nsz) || dalloc(h, &d.py, nsz) || dalloc(h, &d.zx, nsz) || dalloc(h, &d.zy, nsz) ||
         dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
-        dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &d.wm, wz) ||
+        dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &diofs, wz) ||
+        dalloc(h, &d.linv, (size_t)std::max<long long>(1, itot)) || dalloc(h, &d.wm, wz) ||
         dalloc(h, &d.rel_pos, wz) || dalloc(h, &d.cycle, 1) || dalloc(h, &d.row_index, 1) ||
         dalloc(h, &d.sum_row, (size_t)h->row_len) || dalloc(h, &d.sample_count, 1) || dalloc(h, &d.status, 1) ||
         dalloc(h, &d.wing_fm, 3 * wz) || dalloc(h, &d.ibm_resid, 2) || dalloc(h, &d.stream_start, (size_t)d.ncol) ||
@@ -629,9 +633,11 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         CK(cudaMemcpy(drpos, rpos.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dbw, bw.data(), W * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dlofs, lofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(diofs, iofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
     }
     d.wing_pstart = pst; d.wing_sstart = sst; d.wing_npts = npw; d.seg_wing = sgw;
     d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs; d.rpos = drpos;
+    d.wing_linv_ofs = diofs;
     h->ppw.assign(npts.begin(), npts.end());
     // dynamic shared memory of the factorisation kernel (one block per wing):
     // [staged panel rows][pair table][the wing's banded factor, if it fits]
@@ -648,14 +654,18 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.bw_max = bwmax;
     d.nw_max = nwmax;
     d.lband_total = ltot;
-    size_t base = (size_t)2 * (IBM_PANEL + 1) * bwmax * sizeof(double) + (size_t)bwmax * (bwmax + 1) / 2 * 4;
-    base = (base + 15) / 16 * 16;
+    const size_t base = ibm_factor_staging_bytes(bwmax);
     const size_t smem_cap = 200 * 1024;
     d.factor_smem_off = (long long)base;
     d.factor_in_smem = base + (size_t)wmax * sizeof(double) <= smem_cap ? 1 : 0;
     h->factor_smem = d.factor_in_smem ? base + (size_t)wmax * sizeof(double) : base;
     if (h->factor_smem > smem_cap) return fail(h, "immersed boundary: too many segments for one factorisation block");
-    CK(ibm_prepare(h->factor_smem));
+    // substitution: the wing's factor goes to shared memory when it fits
+    if (ibm_solve_smem(nwmax, bwmax, wmax, false) > smem_cap)
+        return fail(h, "immersed boundary: too many segments for one substitution block");
+    d.solve_in_smem = ibm_solve_smem(nwmax, bwmax, wmax, true) <= smem_cap ? 1 : 0;
+    d.solve_smem = (long long)ibm_solve_smem(nwmax, bwmax, wmax, d.solve_in_smem != 0);
+    CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
         return -1;

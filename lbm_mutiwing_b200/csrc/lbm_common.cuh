@@ -50,6 +50,7 @@ enum StatusBits : int {
     ST_WINGS_COUPLED = 16,     // two wings share band nodes; block solve refined iteratively
     ST_COUPLED_NOCONV = 32,    // refinement for coupled wings did not converge
     ST_MOTION = 64,            // no motion rows available
+    ST_COPY_TIMEOUT = 128,     // a bulk shared-memory copy did not complete within its wait limit
 };
 
 constexpr int BOX_SLOTS = 36;   // a +-2.5 spacing box spans at most 6 x 6 nodes
@@ -135,6 +136,10 @@ struct DevState {
     int nw_max;                  // largest segment count of a wing
     int factor_in_smem;          // a wing's banded factor fits in shared memory
     long long factor_smem_off;   // its byte offset in the factor kernel's shared memory
+    double* linv;                // inverses of the factor's diagonal blocks, per wing and panel
+    const long long* wing_linv_ofs;  // W offsets into linv
+    int solve_in_smem;           // the substitution copies the wing's factor to shared memory
+    long long solve_smem;        // dynamic shared memory of the substitution kernel (bytes)
     // configuration of wing placement
     double wing_x_origin, wing_x_spacing, wing_y_origin, xc, yc;
     // motion source

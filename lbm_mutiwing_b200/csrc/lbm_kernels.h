@@ -37,10 +37,18 @@ void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st);
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st);
 // substitution, spread, velocity correction, forces (needs rhs and factor)
 void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st);
-cudaError_t ibm_prepare(size_t factor_smem);
 int ibm_finish_blocks(const DevState& d);
-constexpr int IBM_PANEL = 8;           // columns per factorisation panel
-constexpr int IBM_MAX_BANDWIDTH = 88;  // register panel: bandwidth + panel <= 96 rows
+// banded L' D L'^T factorisation and substitution (ibm_solver.cu)
+cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem);
+// dynamic shared memory of the substitution kernel
+size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool factor_in_smem);
+// shared memory of the factorisation kernel ahead of the wing's storage
+// (a multiple of 16 bytes)
+size_t ibm_factor_staging_bytes(int bw_max);
+void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st);
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st);
+constexpr int IBM_PANEL = 8;            // columns per factorisation panel
+constexpr int IBM_MAX_BANDWIDTH = 160;  // staged panel rows and pair table stay within shared memory
 // Banded storage of a wing's G: row p holds G(p, p - dd) at dd = 0..bw.
 // The row stride covers bw + IBM_PANEL + 1 entries, so the entries past bw
 // form a zero zone, and a zero row precedes row 0 and IBM_PANEL + bw zero
@@ -51,6 +59,13 @@ constexpr int IBM_MAX_BANDWIDTH = 88;  // register panel: bandwidth + panel <= 9
 inline __host__ __device__ int ibm_ld(int bw) { return (bw + IBM_PANEL + 2) & ~1; }
 inline __host__ __device__ long long ibm_wing_storage(int nw, int bw) {
     return (long long)(1 + nw + IBM_PANEL + bw) * ibm_ld(bw);
+}
+// Per panel of a wing's factor: the inverse of its unit lower diagonal block
+// (row-major IBM_PANEL x IBM_PANEL) followed by the IBM_PANEL reciprocal
+// pivots (zero past the last segment).
+constexpr int IBM_PANEL_AUX = IBM_PANEL * IBM_PANEL + IBM_PANEL;
+inline __host__ __device__ long long ibm_linv_storage(int nw) {
+    return (long long)((nw + IBM_PANEL - 1) / IBM_PANEL) * IBM_PANEL_AUX;
 }
 void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle += 1
 
