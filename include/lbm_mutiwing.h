@@ -119,6 +119,28 @@ int lbm_get_fields(LbmHandle* h, double* rho, double* u, double* v, double* pre)
 /* erranalysis (solution.f90:77-130) on the fields of the last two steps. */
 int lbm_err(LbmHandle* h, double* err);
 
+/* No counterpart in the reference.  The same convergence error, on velocity
+ * fields the caller owns in device memory (u, v current; u0, v0 previous;
+ * node (i, j) at [j * pitch + i], 0 <= i < nx, 0 <= j < ny), computed
+ * without allocating anything: for callers that cannot let a library
+ * allocate device memory (the device handed to their own memory pool, or a
+ * serving loop where an allocation would synchronise the device and stall
+ * other streams).  Partial sums live in a fixed array inside the library,
+ * sized for at most LBM_NOALLOC_MAX_ROWS lattice rows; a larger ny is
+ * refused (-2).  Nothing has to start at zero: every partial sum a call reads
+ * is written by the same call.  The array is shared by every call on a
+ * device, so calls that overlap in time on one device race and must be
+ * serialised by the caller.  The first call on each device looks the array
+ * up (cudaGetSymbolAddress); make it before any stream capture begins.
+ * Kernels run on `stream` (a cudaStream_t, NULL for the default stream) of
+ * `device`; the call waits for them and writes err on the host.  Returns 0,
+ * or -1 (bad argument), -2 (too many rows), -3 (CUDA error) with the text in
+ * msg (msg_cap bytes, may be NULL).  The caller's current device is kept. */
+#define LBM_NOALLOC_MAX_ROWS 16384
+int lbm_err_fields_noalloc(const double* u, const double* v, const double* u0, const double* v0,
+                           int32_t nx, int32_t ny, int64_t pitch, int32_t device, void* stream,
+                           double* err, char* msg, int32_t msg_cap);
+
 /* Distributions f (9 planes, FP64) of the current state; set replaces them. */
 int lbm_get_f(LbmHandle* h, double* f);
 int lbm_set_f(LbmHandle* h, const double* f);

@@ -59,6 +59,8 @@ SIGNATURES = [
     ("lbm_reset_sums", C.c_int, [C.c_void_p]),
     ("lbm_get_fields", C.c_int, [C.c_void_p, D, D, D, D]),
     ("lbm_err", C.c_int, [C.c_void_p, D]),
+    ("lbm_err_fields_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
+                                         C.c_int64, C.c_int32, C.c_void_p, D, C.c_char_p, C.c_int32]),
     ("lbm_get_f", C.c_int, [C.c_void_p, D]),
     ("lbm_set_f", C.c_int, [C.c_void_p, D]),
     ("lbm_get_band", C.c_int, [C.c_void_p, I32, I32, C.c_int32]),

@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
 NO_FMA = {"kernels_fp64.cu"}
-SOURCES = ["lbm_api.cu", "kernels_fp64.cu", "kernels_fp32.cu", "ibm.cu", "ibm_solver.cu"]
+SOURCES = ["lbm_api.cu", "kernels_fp64.cu", "kernels_fp32.cu", "ibm.cu", "ibm_solver.cu", "err_noalloc.cu"]
 
 
 def nvcc() -> str:

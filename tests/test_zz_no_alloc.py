@@ -1,0 +1,115 @@
+"""lbm_err_fields_noalloc -- the convergence error of caller-owned device
+fields, computed with a fixed scratch array inside the library instead of any
+allocation -- against the handle's own lbm_err, two calls in a row.
+
+This file is collected last on purpose: the entry point looks its scratch up
+on the first call for a device, and the tests must pass both after the rest
+of the suite and alone in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from lbm_mutiwing_b200 import api
+from lbm_mutiwing_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _episode():
+    # one NACA0012 section, uniform markers, 201 x 101 lattice
+    return wl.tandem_pitch_heave("noalloc", 4.0, 2.0, 0.02, 100.0, -0.75, 0.0, 60, 20, n_wings=1,
+                                 spacing="uniform", pitch_deg=10.0, heave=0.2, freq=1.0)
+
+
+def _fields_and_err(precision):
+    """u, v after step 6, u0, v0 after step 5, and lbm_err of step 6."""
+    ep = _episode()
+    if precision == api.PRECISION_FP64:
+        with api.Simulation(ep, precision) as s:
+            s.step(5)
+            _, u0, v0, _ = s.fields()
+            s.step(1)
+            _, u, v, _ = s.fields()
+            ref = s.err()
+        return ep, u, v, u0, v0, ref
+    # the FP32 path keeps only the fields of its last two steps: take the
+    # step-5 fields from a second, identical run (the runs are deterministic)
+    with api.Simulation(ep, precision) as s:
+        s.step(5, flags=api.STEP_FIELDS)
+        _, u0, v0, _ = s.fields()
+    with api.Simulation(ep, precision) as s:
+        s.step(4)
+        s.step(2, flags=api.STEP_ERR)
+        _, u, v, _ = s.fields()
+        ref = s.err()
+    return ep, u, v, u0, v0, ref
+
+
+def _call(L, ptrs, nx, ny, pitch, stream=None):
+    err = C.c_double(-1.0)
+    msg = C.create_string_buffer(256)
+    rc = L.lbm_err_fields_noalloc(*ptrs, nx, ny, pitch, 0, stream, C.byref(err), msg, 256)
+    return rc, err.value, msg.value.decode()
+
+
+def _oracle_order(u, v, u0, v0):
+    """erranalysis (solution.f90:77-130) summed in the reference's loop order."""
+    du, dv = u[1:-1, 1:-1] - u0[1:-1, 1:-1], v[1:-1, 1:-1] - v0[1:-1, 1:-1]
+    a = np.sum((du * du + dv * dv).T)
+    b = np.sum((u[1:-1, 1:-1] ** 2 + v[1:-1, 1:-1] ** 2).T)
+    return np.sqrt(a) / (np.sqrt(b) + 1e-30)
+
+
+@pytest.mark.parametrize("precision", [api.PRECISION_FP64, api.PRECISION_FP32])
+def test_noalloc_err_matches_lbm_err_twice(precision):
+    ep, u, v, u0, v0, ref = _fields_and_err(precision)
+    assert ref > 0.0
+    ny, nx = u.shape
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (u, v, u0, v0)]
+    torch.cuda.synchronize()
+    L = api.load_library()
+    ptrs = [x.data_ptr() for x in t]
+    r1 = _call(L, ptrs, nx, ny, nx)
+    r2 = _call(L, ptrs, nx, ny, nx)
+    assert r1[0] == 0 and r2[0] == 0, (r1, r2)
+    assert r1[1] == r2[1]                       # deterministic from call to call
+    assert abs(r1[1] - ref) <= 1e-12 * ref      # same sums as lbm_err, other order
+    assert abs(r1[1] - _oracle_order(u, v, u0, v0)) <= 1e-12 * ref
+
+
+def test_noalloc_err_pitched_fields_on_a_side_stream():
+    """Padded rows (NaN in the padding) and a non-default stream."""
+    ep, u, v, u0, v0, ref = _fields_and_err(api.PRECISION_FP64)
+    ny, nx = u.shape
+    pitch = nx + 13
+    dev = torch.device("cuda", 0)
+    t = []
+    for a in (u, v, u0, v0):
+        p = np.full((ny, pitch), np.nan)
+        p[:, :nx] = a
+        t.append(torch.from_numpy(p).to(dev))
+    torch.cuda.synchronize()
+    L = api.load_library()
+    ptrs = [x.data_ptr() for x in t]
+    side = torch.cuda.Stream(device=dev)
+    r1 = _call(L, ptrs, nx, ny, pitch, C.c_void_p(side.cuda_stream))
+    r2 = _call(L, ptrs, nx, ny, pitch, C.c_void_p(side.cuda_stream))
+    assert r1[0] == 0 and r2[0] == 0, (r1, r2)
+    assert r1[1] == r2[1]
+    assert abs(r1[1] - ref) <= 1e-12 * ref
+
+
+def test_noalloc_err_refuses_more_rows_than_its_scratch():
+    dev = torch.device("cuda", 0)
+    x = torch.zeros(8, device=dev, dtype=torch.float64)
+    L = api.load_library()
+    ptrs = [x.data_ptr()] * 4
+    rc, err, msg = _call(L, ptrs, 3, 16385, 3)
+    assert rc == -2 and "16384" in msg
+    assert err == -1.0                          # result untouched
+    rc, _, msg = _call(L, ptrs, 2, 3, 2)
+    assert rc == -1 and "nx >= 3" in msg
