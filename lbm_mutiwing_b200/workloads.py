@@ -155,28 +155,28 @@ def tandem_pitch_heave(name: str, width: float, height: float, scale: float, re:
     return ep
 
 
-def config1(steps: int = 2000, scale_factor: int = 1) -> Episode:
+def tandem_800x400(steps: int = 2000, scale_factor: int = 1) -> Episode:
     """800x400 lattice (8x4 chords, dx = 0.01), Re 200, NACA0012 tandem at
     corner-frame x = 2.0 / 3.5, y = 2.0 (centred frame -2.0 / -0.5, 0.0),
     200 cosine-spaced markers per wing.  ``scale_factor`` > 1 coarsens the
     lattice for quick tests (dx = 0.01 * scale_factor)."""
-    return tandem_pitch_heave("cfg1_800x400_re200", 8.0, 4.0, 0.01 * scale_factor, 200.0,
+    return tandem_pitch_heave("tandem_800x400_re200", 8.0, 4.0, 0.01 * scale_factor, 200.0,
                               -2.0, 0.0, 200 // scale_factor, steps)
 
 
-def config2(steps: int = 10000) -> Episode:
+def tandem_4000x2000(steps: int = 10000) -> Episode:
     """4000x2000 lattice (40x20 chords, dx = 0.01), Re 1000, NACA0012 at the
     reference's default wing offsets x = 0.0 / 1.5, y = 0.5, 200 markers."""
-    return tandem_pitch_heave("cfg2_4000x2000_re1000", 40.0, 20.0, 0.01, 1000.0,
+    return tandem_pitch_heave("tandem_4000x2000_re1000", 40.0, 20.0, 0.01, 1000.0,
                               0.0, 0.5, 200, steps)
 
 
-def config5(steps: int = 20000) -> Episode:
+def formation_16000x8000(steps: int = 20000) -> Episode:
     """16000x8000 lattice (dx = 0.0025), Re 5000, four NACA0012 wings with 800
     markers each in a 2x2 staggered formation (absolute positions set through
     the motion table's x and y columns)."""
     nx, ny, ox, oy = lattice(40.0, 20.0, 0.0025)
-    ep = Episode(name="cfg5_16000x8000_re5000", nx=nx, ny=ny, scale=0.0025, re=5000.0,
+    ep = Episode(name="formation_16000x8000_re5000", nx=nx, ny=ny, scale=0.0025, re=5000.0,
                  ox=ox, oy=oy, wing_x_origin=0.0, wing_x_spacing=1.5, wing_y_origin=0.5,
                  steps=steps)
     ep.markers = [naca_loop(0.12, 800) for _ in range(4)]
@@ -187,8 +187,8 @@ def config5(steps: int = 20000) -> Episode:
     return ep
 
 
-def batched_mix(count: int = 64, seed: int = 20261203, steps: int = 1000) -> List[Episode]:
-    """Config-3 style mix: grids from {400x200, 800x400, 1200x600, 2000x1000}
+def mixed_batch(count: int = 64, seed: int = 20261203, steps: int = 1000) -> List[Episode]:
+    """Mixed batch: grids from {400x200, 800x400, 1200x600, 2000x1000}
     nodes at dx = 0.01, 1-4 NACA00xx wings (thickness 8-18 %, 100-300
     markers), pitch 5-25 deg, heave 0.1-0.6 chord, f 0.2-1.0."""
     rng = np.random.default_rng(seed)

@@ -30,8 +30,8 @@ def episode_a(steps=80):
 
 
 def episode_b(steps=60):
-    """Config-1 style tandem at dx = 0.04 with cosine-spaced markers."""
-    return wl.config1(steps=steps, scale_factor=4)
+    """The 800x400 tandem coarsened to dx = 0.04, cosine-spaced markers."""
+    return wl.tandem_800x400(steps=steps, scale_factor=4)
 
 
 def rel(a, b):

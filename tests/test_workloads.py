@@ -25,8 +25,8 @@ def test_reference_geometry_file_matches_layout():
     assert abs(pts[:, 0].min() + 0.25) < 1e-8 and abs(pts[:, 0].max() - 0.75) < 1e-8
 
 
-def test_config1_geometry():
-    ep = wl.config1(steps=10)
+def test_tandem_800x400_geometry():
+    ep = wl.tandem_800x400(steps=10)
     assert (ep.nx, ep.ny) == (801, 401)
     assert (ep.ox, ep.oy) == (-4.0, -2.0)
     assert ep.wing_count == 2 and ep.markers[0].shape == (201, 2)
@@ -38,9 +38,9 @@ def test_config1_geometry():
     assert np.allclose(ep.motion[:, 4], -2.0) and np.allclose(ep.motion[:, 13], -0.5)
 
 
-def test_batched_mix_is_seeded():
-    a = wl.batched_mix(8, seed=5, steps=10)
-    b = wl.batched_mix(8, seed=5, steps=10)
+def test_mixed_batch_is_seeded():
+    a = wl.mixed_batch(8, seed=5, steps=10)
+    b = wl.mixed_batch(8, seed=5, steps=10)
     assert [e.nx for e in a] == [e.nx for e in b]
     assert all(np.array_equal(x.motion, y.motion) for x, y in zip(a, b))
-    assert {e.nx for e in wl.batched_mix(64, steps=2)} <= {401, 801, 1201, 2001}
+    assert {e.nx for e in wl.mixed_batch(64, steps=2)} <= {401, 801, 1201, 2001}
