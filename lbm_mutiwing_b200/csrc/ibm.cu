@@ -94,7 +94,7 @@ __device__ inline void triplet(double s0, double v0, double v1, double dt, doubl
 }
 
 __device__ inline double step_time(const DevState& d) {
-    return mul((double)(*d.cycle - 1), mul(d.scale, d.uu));   // solution.f90:292
+    return mul((double)(*d.cycle + d.cycle_ahead - 1), mul(d.scale, d.uu));   // solution.f90:292
 }
 
 // mode + apply_motion_row for wing w at the current cycle (mode.f90:451-471,

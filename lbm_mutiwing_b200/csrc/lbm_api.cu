@@ -107,6 +107,34 @@ using namespace lbm;
 // immersed-boundary solve
 constexpr int NPHASE = 6;
 
+// Immersed-boundary geometry of one step: motion, markers, support boxes,
+// kernel values, band list and map, and the factorised G.  The fused path
+// keeps two sets so that the geometry of step n + 1 (which depends only on
+// the motion) is built while step n still reads its own.
+struct GeoSet {
+    WingMotion* wm = nullptr;
+    double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
+    int *box = nullptr, *claim_cnt = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
+    int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
+    double *lband = nullptr, *linv = nullptr;
+};
+
+static GeoSet geo_of(const DevState& d) {
+    GeoSet g;
+    g.wm = d.wm; g.xb1 = d.xb1; g.yb1 = d.yb1; g.xb2 = d.xb2; g.yb2 = d.yb2; g.kx = d.kx; g.ky = d.ky;
+    g.box = d.box; g.claim_cnt = d.claim_cnt; g.pb = d.pb; g.band_claimer = d.band_claimer;
+    g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
+    g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv;
+    return g;
+}
+
+static void use_geo(DevState& d, const GeoSet& g) {
+    d.wm = g.wm; d.xb1 = g.xb1; d.yb1 = g.yb1; d.xb2 = g.xb2; d.yb2 = g.yb2; d.kx = g.kx; d.ky = g.ky;
+    d.box = g.box; d.claim_cnt = g.claim_cnt; d.pb = g.pb; d.band_claimer = g.band_claimer;
+    d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
+    d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv;
+}
+
 struct LbmHandle {
     LbmConfig cfg{};
     std::string err;
@@ -114,11 +142,16 @@ struct LbmHandle {
     FusedConsts fc{};
     int parity = 0;                 // fused path: 0 -> current planes in gA
     float* planes[2] = {nullptr, nullptr};
+    GeoSet geo[2];                  // geometry sets (the plain path uses set 0)
+    int gset = 0;                   // fused path: set of the next step
+    int last_gset = 0;              // set of the last completed step
     // streams of one fused step: main (bulk kernel, band re-collision),
-    // ibm (band list, right-hand side, solve), aux (assembly and
-    // factorisation of G), bc (far field)
-    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_aux = nullptr, s_bc = nullptr;
-    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_geom = nullptr, ev_fact = nullptr, ev_bc = nullptr;
+    // ibm (right-hand side, solve, spread, forces), aux (the next step's
+    // motion, markers and band list), aux2 (its assembly and factorisation
+    // of G), bc (far field)
+    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_aux = nullptr, s_aux2 = nullptr, s_bc = nullptr;
+    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_geom = nullptr, ev_fact = nullptr, ev_bc = nullptr,
+                ev_list = nullptr;
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
     int row_len = 4;
@@ -186,7 +219,15 @@ DevState current(const LbmHandle* h) {
     if (d.precision != 0) {
         d.gA = h->planes[h->parity];
         d.gB = h->planes[1 - h->parity];
+        use_geo(d, h->geo[h->gset]);
     }
+    return d;
+}
+
+// The geometry of the last completed step (band list, markers).
+DevState last_geometry(const LbmHandle* h) {
+    DevState d = h->d;
+    use_geo(d, h->geo[d.precision != 0 ? h->last_gset : 0]);
     return d;
 }
 
@@ -285,8 +326,12 @@ int init_state(LbmHandle* h) {
         CK(cudaGetLastError());
     }
     std::vector<int> em(N, BAND_EMPTY);
-    CK(cudaMemcpy(d.band_map, em.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemset(d.band_n, 0, 2 * sizeof(int)));
+    for (int s = 0; s < 2; ++s) {
+        CK(cudaMemcpy(h->geo[s].band_map, em.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemset(h->geo[s].band_n, 0, 2 * sizeof(int)));
+    }
+    h->gset = 0;
+    h->last_gset = 0;
     CK(cudaMemset(d.sum_row, 0, sizeof(double) * h->row_len));
     CK(cudaMemset(d.sample_count, 0, sizeof(int)));
     CK(cudaMemset(d.status, 0, sizeof(int)));
@@ -367,8 +412,19 @@ void collect_phase_times(LbmHandle* h) {
     h->evused = 0;
 }
 
-// One evolution step (solution.f90:272-422) on the current parity.
-void enqueue_step(LbmHandle* h, bool fields, bool diag) {
+// Fused path: the geometry of the coming step (its motion, markers, band list
+// and factorised G) in its own set, before the first step of a call; later
+// steps build the next step's geometry while they run.
+void prime_geometry(LbmHandle* h) {
+    DevState d = current(h);
+    launch_ibm_band(d, h->s_main, nullptr);
+    launch_ibm_factor(d, h->factor_smem, h->s_main);
+}
+
+// One evolution step (solution.f90:272-422) on the current parity.  On the
+// fused path, prefetch builds the geometry of the following step in the
+// other set.
+void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch) {
     DevState d = current(h);
     d.diag = diag ? 1 : 0;
     d.write_fields = fields ? 1 : 0;
@@ -401,24 +457,34 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag) {
         }
         launch_step_advance(d, h->s_main);
     } else {
-        // The immersed boundary (two high-priority streams) and the far field
-        // overlap the bulk kernel: all read only the current planes, and the
+        // The immersed boundary, the far field and the next step's geometry
+        // overlap the bulk kernel.  All read only the current planes, and the
         // writes go to disjoint nodes of the next planes (interior, band,
         // border).  Support boxes keep off the border rows and columns the far
-        // field reads, so it needs nothing from the immersed boundary.
+        // field reads, so it needs nothing from the immersed boundary.  The
+        // geometry of this step was built by the previous step (or the
+        // prime); the next step's goes to the other set, whose last reader
+        // was the previous step.
+        DevState dn = d;
+        use_geo(dn, h->geo[1 - h->gset]);
+        dn.cycle_ahead = 1;
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
         cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
-        {
-            PhaseMark pm(h, 0, h->s_ibm);
-            launch_ibm_band(d, h->s_ibm, h->ev_geom);
+        if (prefetch) {
+            cudaStreamWaitEvent(h->s_aux, h->ev_main, 0);
+            {
+                PhaseMark pm(h, 0, h->s_aux);
+                launch_ibm_band(dn, h->s_aux, h->ev_geom);
+            }
+            cudaEventRecord(h->ev_list, h->s_aux);
+            cudaStreamWaitEvent(h->s_aux2, h->ev_geom, 0);
+            {
+                PhaseMark pm(h, 5, h->s_aux2);
+                launch_ibm_factor(dn, h->factor_smem, h->s_aux2);
+            }
+            cudaEventRecord(h->ev_fact, h->s_aux2);
         }
-        cudaStreamWaitEvent(h->s_aux, h->ev_geom, 0);
-        {
-            PhaseMark pm(h, 5, h->s_aux);
-            launch_ibm_factor(d, h->factor_smem, h->s_aux);
-        }
-        cudaEventRecord(h->ev_fact, h->s_aux);
         {
             PhaseMark pm(h, 3, h->s_bc);
             launch_outer_bc(d, h->s_bc);
@@ -427,7 +493,6 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag) {
         {
             PhaseMark pm(h, 4, h->s_ibm);
             launch_ibm_rhs(d, true, h->s_ibm);
-            cudaStreamWaitEvent(h->s_ibm, h->ev_fact, 0);
             launch_ibm_solve(d, true, h->s_ibm);
         }
         cudaEventRecord(h->ev_ibm, h->s_ibm);
@@ -441,8 +506,14 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag) {
             launch_fused_band(d, fields, h->s_main);
         }
         cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
+        if (prefetch) {
+            cudaStreamWaitEvent(h->s_main, h->ev_list, 0);
+            cudaStreamWaitEvent(h->s_main, h->ev_fact, 0);
+        }
         launch_step_advance(d, h->s_main);
         h->parity = 1 - h->parity;
+        h->last_gset = h->gset;
+        h->gset = 1 - h->gset;
     }
     if (h->timing) h->timed_steps += 1;
 }
@@ -458,14 +529,19 @@ void drop_graphs(LbmHandle* h) {
 // Two steps starting at parity p, captured from both streams (the second
 // stream joins and leaves through events, as in eager launches).
 int build_graph(LbmHandle* h, int p) {
-    const int saved = h->parity;
+    // planes and geometry sets alternate together; their relation changes
+    // only with a lattice shift, which drops the graphs
+    const int saved = h->parity, saved_g = h->gset, saved_last = h->last_gset;
+    h->gset = p ^ (h->parity ^ h->gset);
     h->parity = p;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->s_main, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h, false, false);
-    enqueue_step(h, false, false);
+    enqueue_step(h, false, false, true);
+    enqueue_step(h, false, false, true);
     cudaError_t e = cudaStreamEndCapture(h->s_main, &g);
     h->parity = saved;
+    h->gset = saved_g;
+    h->last_gset = saved_last;
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(&h->gexec[p], g, 0);
     cudaGraphDestroy(g);
@@ -669,6 +745,20 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
         return -1;
+    // the second geometry set (fused path: the next step's geometry)
+    h->geo[0] = geo_of(d);
+    h->geo[1] = h->geo[0];
+    if (c.precision != LBM_PRECISION_FP64) {
+        GeoSet& g = h->geo[1];
+        if (dalloc(h, &g.wm, wz) || dalloc(h, &g.xb1, npz) || dalloc(h, &g.yb1, npz) || dalloc(h, &g.xb2, nsz) ||
+            dalloc(h, &g.yb2, nsz) || dalloc(h, &g.kx, 6 * nsz) || dalloc(h, &g.ky, 6 * nsz) ||
+            dalloc(h, &g.box, 4 * nsz) || dalloc(h, &g.claim_cnt, nsz + 1) || dalloc(h, &g.pb, nsz * BOX_SLOTS) ||
+            dalloc(h, &g.band_claimer, (size_t)cap) || dalloc(h, &g.band_n, 2) ||
+            dalloc(h, &g.band_ij, 2 * (size_t)cap) || dalloc(h, &g.band_wing, cap) || dalloc(h, &g.band_map, N) ||
+            dalloc(h, &g.ibm_flags, 4) || dalloc(h, &g.lband, (size_t)std::max<long long>(1, ltot)) ||
+            dalloc(h, &g.linv, (size_t)std::max<long long>(1, itot)))
+            return -1;
+    }
     if (ensure_rows(h, 1024)) return -1;
     // the immersed-boundary chain is latency-bound and on the critical path:
     // its streams get the highest priority so their blocks are scheduled
@@ -678,8 +768,9 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     CK(cudaStreamCreateWithPriority(&h->s_main, cudaStreamNonBlocking, prio_lo));
     CK(cudaStreamCreateWithPriority(&h->s_ibm, cudaStreamNonBlocking, prio_hi));
     CK(cudaStreamCreateWithPriority(&h->s_aux, cudaStreamNonBlocking, prio_hi));
-    CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, prio_lo));
-    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_geom, &h->ev_fact, &h->ev_bc})
+    CK(cudaStreamCreateWithPriority(&h->s_aux2, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, prio_hi));
+    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_geom, &h->ev_fact, &h->ev_bc, &h->ev_list})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
     h->pinned_n = 4096;
@@ -773,11 +864,13 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     // all but the last two steps replay a two-step CUDA graph; the last two
     // may write fields or diagnostics and are launched directly
     const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
+    if (h->d.precision != 0 && n_steps > 0) prime_geometry(h);
     int64_t n = 0;
     if (graphs) {
         for (; n + 2 < n_steps - 1; n += 2) {
             if (!h->gexec[h->parity] && build_graph(h, h->parity)) return -1;
             CK(cudaGraphLaunch(h->gexec[h->parity], h->s_main));
+            h->last_gset = 1 - h->gset;
         }
     }
     for (; n < n_steps; ++n) {
@@ -797,7 +890,7 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
             }
             fields = true;
         }
-        enqueue_step(h, fields, last);
+        enqueue_step(h, fields, last, !last);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->s_main));
@@ -930,14 +1023,15 @@ int lbm_get_band(LbmHandle* h, int32_t* n, int32_t* ij_wing, int32_t cap) {
     if (!h || !n) return -1;
     CK(cudaSetDevice(h->cfg.device));
     int nb = 0;
-    CK(cudaMemcpy(&nb, h->d.band_n, sizeof(int), cudaMemcpyDeviceToHost));
+    const DevState g = last_geometry(h);
+    CK(cudaMemcpy(&nb, g.band_n, sizeof(int), cudaMemcpyDeviceToHost));
     *n = nb;
     if (!ij_wing) return 0;
     const int m = std::min(nb, cap);
     std::vector<int> ij(2 * (size_t)std::max(m, 1)), w(std::max(m, 1));
     if (m > 0) {
-        CK(cudaMemcpy(ij.data(), h->d.band_ij, 2 * m * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(w.data(), h->d.band_wing, m * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(ij.data(), g.band_ij, 2 * m * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.data(), g.band_wing, m * sizeof(int), cudaMemcpyDeviceToHost));
     }
     for (int b = 0; b < m; ++b) {
         ij_wing[3 * b] = ij[2 * b] + 1;
@@ -950,7 +1044,7 @@ int lbm_get_band(LbmHandle* h, int32_t* n, int32_t* ij_wing, int32_t cap) {
 int lbm_get_markers(LbmHandle* h, double* xb1, double* yb1, double* xb2, double* yb2) {
     if (!h) return -1;
     CK(cudaSetDevice(h->cfg.device));
-    const DevState& d = h->d;
+    const DevState d = last_geometry(h);
     if (xb1 && d.npts) CK(cudaMemcpy(xb1, d.xb1, d.npts * sizeof(double), cudaMemcpyDeviceToHost));
     if (yb1 && d.npts) CK(cudaMemcpy(yb1, d.yb1, d.npts * sizeof(double), cudaMemcpyDeviceToHost));
     if (xb2 && d.nseg) CK(cudaMemcpy(xb2, d.xb2, d.nseg * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1024,18 +1118,14 @@ void lbm_destroy(LbmHandle* h) {
     if (!h) return;
     cudaSetDevice(h->cfg.device);
     cudaDeviceSynchronize();
+    drop_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->pinned) cudaFreeHost(h->pinned);
-    if (h->s_main) cudaStreamDestroy(h->s_main);
-    if (h->s_ibm) cudaStreamDestroy(h->s_ibm);
-    if (h->s_aux) cudaStreamDestroy(h->s_aux);
-    if (h->s_bc) cudaStreamDestroy(h->s_bc);
-    for (cudaEvent_t e : {h->ev_geom, h->ev_fact, h->ev_bc})
+    for (cudaStream_t s : {h->s_main, h->s_ibm, h->s_aux, h->s_aux2, h->s_bc})
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : {h->ev_geom, h->ev_fact, h->ev_bc, h->ev_ibm, h->ev_main, h->ev_list})
         if (e) cudaEventDestroy(e);
-    if (h->ev_ibm) cudaEventDestroy(h->ev_ibm);
-    if (h->ev_main) cudaEventDestroy(h->ev_main);
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
-    drop_graphs(h);
     delete h;
 }
 
