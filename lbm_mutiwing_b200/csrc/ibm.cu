@@ -512,15 +512,22 @@ __global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) 
 // Per-wing force and moment from the block partials (in block order), the
 // no-slip residual when diagnostics are on, and the force row.
 __global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks) {
+    constexpr int CHUNK = 64;   // block partials staged per pass
     __shared__ double fm[MAX_WINGS][3];
     __shared__ double red[8][2];
+    __shared__ double part[CHUNK * MAX_WINGS * 3];
     const int tid = threadIdx.x, W = d.wing_count;
-    if (tid < 3 * W) {
-        const int w = tid / 3, c = tid % 3;
-        double v = 0.0;
-        for (int k = 0; k < nblocks; ++k) v += d.force_part[((long long)k * W + w) * 3 + c];
-        fm[w][c] = v;
+    // partials are loaded in parallel, then added in block order
+    double v = 0.0;
+    for (int k0 = 0; k0 < nblocks; k0 += CHUNK) {
+        const int nk = min(CHUNK, nblocks - k0);
+        for (int t = tid; t < nk * 3 * W; t += blockDim.x) part[t] = d.force_part[(long long)k0 * W * 3 + t];
+        __syncthreads();
+        if (tid < 3 * W)
+            for (int k = 0; k < nk; ++k) v += part[k * 3 * W + tid];
+        __syncthreads();
     }
+    if (tid < 3 * W) fm[tid / 3][tid % 3] = v;
     if (d.diag) {
         double e2 = 0.0, r2 = 0.0;
         for (int s = tid; s < d.nseg; s += blockDim.x) {
@@ -542,6 +549,11 @@ __global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks
         if ((tid & 31) == 0) { red[tid >> 5][0] = e2; red[tid >> 5][1] = r2; }
     }
     __syncthreads();
+    // force normalisation and force row (solution.f90:330-385): thread 0
+    // assembles the row in shared memory, then one thread per column writes
+    // it and adds it to the running sums
+    __shared__ double rowv[4 + 12 * MAX_WINGS];
+    const int rl = 4 + 12 * W;
     if (tid == 0) {
         if (d.diag) {
             double a = 0.0, b = 0.0;
@@ -549,44 +561,39 @@ __global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks
             d.ibm_resid[0] = a;
             d.ibm_resid[1] = b;
         }
-        // force normalisation and force row (solution.f90:330-385)
         const double uu = d.uu, sc = d.scale;
-        const double time = step_time(d);
-        const long long ri = *d.row_index;
-        const int rl = 4 + 12 * W;
-        double* row = (d.force_rows && ri < d.force_rows_cap) ? d.force_rows + ri * rl : nullptr;
         double fx = 0.0, fy = 0.0, mt = 0.0;
-        double rowv[4 + 12 * MAX_WINGS];
-        rowv[0] = time;
+        rowv[0] = step_time(d);
         int col = 1;
         for (int w = 0; w < W; ++w) {
             const double Fx = 2.0 * fm[w][0] / (uu * uu * (1.0 / sc));
             const double Fy = 2.0 * fm[w][1] / (uu * uu * (1.0 / sc));
             const double Mz = -(2.0 * fm[w][2] / (uu * uu * (1.0 / (sc * sc))));
-            d.wing_fm[3 * w] = fm[w][0];
-            d.wing_fm[3 * w + 1] = fm[w][1];
-            d.wing_fm[3 * w + 2] = fm[w][2];
             rowv[col] = Fx; rowv[col + 1] = Fy; rowv[col + 2] = Mz;
             col += 3;
         }
         for (int w = 0; w < W; ++w) { fx = fx + rowv[1 + 3 * w]; fy = fy + rowv[2 + 3 * w]; }
         for (int w = 0; w < W; ++w) mt = mt + rowv[3 + 3 * w];
         rowv[col] = fx; rowv[col + 1] = fy; rowv[col + 2] = mt;
-        col += 3;
-        for (int w = 0; w < W; ++w) {
-            const WingMotion m = d.wm[w];
-            rowv[col] = add(add(add(d.wing_x_origin, mul((double)w, d.wing_x_spacing)), m.sa), m.extra_s / (1.0 / sc));
-            rowv[col + 1] = m.sau; rowv[col + 2] = m.saac;
-            rowv[col + 3] = add(d.wing_y_origin, m.sb);
-            rowv[col + 4] = m.sbv; rowv[col + 5] = m.sbac;
-            rowv[col + 6] = m.angle; rowv[col + 7] = m.omega; rowv[col + 8] = m.omgac;
-            col += 9;
-        }
-        for (int c = 0; c < rl; ++c) {
-            if (row) row[c] = rowv[c];
-            d.sum_row[c] = d.sum_row[c] + rowv[c];
-        }
         *d.sample_count += 1;
+    }
+    if (tid < W) {   // one thread per wing: its motion columns
+        const int w = tid, col = 4 + 3 * W + 9 * w;
+        const WingMotion m = d.wm[w];
+        const double sc = d.scale;
+        rowv[col] = add(add(add(d.wing_x_origin, mul((double)w, d.wing_x_spacing)), m.sa), m.extra_s / (1.0 / sc));
+        rowv[col + 1] = m.sau; rowv[col + 2] = m.saac;
+        rowv[col + 3] = add(d.wing_y_origin, m.sb);
+        rowv[col + 4] = m.sbv; rowv[col + 5] = m.sbac;
+        rowv[col + 6] = m.angle; rowv[col + 7] = m.omega; rowv[col + 8] = m.omgac;
+    }
+    if (tid < 3 * W) d.wing_fm[tid] = fm[tid / 3][tid % 3];
+    __syncthreads();
+    const long long ri = *d.row_index;
+    double* row = (d.force_rows && ri < d.force_rows_cap) ? d.force_rows + ri * rl : nullptr;
+    for (int c = tid; c < rl; c += blockDim.x) {
+        if (row) row[c] = rowv[c];
+        d.sum_row[c] = d.sum_row[c] + rowv[c];
     }
 }
 

@@ -105,7 +105,9 @@ __device__ inline bool factor_diagonal_block(const double* A, int ld, int k0, in
 // block and the reciprocal pivots in d.linv (the diagonal blocks of the
 // storage are left as scratch).  Pivots below 1e-15 of the largest diagonal
 // are clamped (numerically singular systems made by marker clusters finer
-// than the lattice).
+// than the lattice).  SMEM: the storage is worked on in shared memory (the
+// template parameter lets every access compile to a shared-memory access).
+template <bool SMEM>
 __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) {
     extern __shared__ __align__(16) double smem[];
     const int w = blockIdx.x;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) 
     const long long wsize = ibm_wing_storage(nw, bw);
     double* gS = d.lband + d.wing_lofs[w];
     double* S = gS;
-    const bool in_smem = d.factor_in_smem != 0;
+    constexpr bool in_smem = SMEM;
     if (in_smem) {
         S = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + d.factor_smem_off);
         if (tid == 0) {
@@ -287,6 +289,8 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) 
 // the right-hand sides.  Shared memory: [2 right-hand sides with zero tails]
 // [permutation][per-panel inverse blocks and pivots][factor].  Each lane
 // updates rows lane and lane + 32 below or above a panel (bw <= 64) or loops.
+// SMEM: the factor is copied to shared memory.
+template <bool SMEM>
 __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
     extern __shared__ __align__(16) double sm[];
     __shared__ uint64_t bar;
@@ -301,7 +305,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
     double* Sm = Lsh + ibm_linv_storage(d.nw_max);
     const double* gS = d.lband + d.wing_lofs[w];
     const long long lbytes = (long long)npan * IBM_PANEL_AUX * 8;
-    const long long sbytes = d.solve_in_smem ? ibm_wing_storage(nw, bw) * 8 : 0;
+    const long long sbytes = SMEM ? ibm_wing_storage(nw, bw) * 8 : 0;
     if (tid == 0) {
         mbar_init(&bar, 1);
         mbar_arrive_expect_tx(&bar, (uint32_t)(lbytes + sbytes));
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
         mbar_wait(&bar, 0);
         return;
     }
-    const double* A = (d.solve_in_smem ? Sm : gS) + ld;   // row 0
+    const double* A = (SMEM ? Sm : gS) + ld;   // row 0
     const int li = lane & (PANEL - 1);
     // L' D v = r: per panel w_p = Li_p z_p, v_p = w_p / d, rows below -= L' w_p
     for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {
@@ -436,17 +440,31 @@ size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool f
 }
 
 cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
-    cudaError_t e = cudaFuncSetAttribute(ibm_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(ibm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem);
+    const int fs = (int)factor_smem, ss = (int)solve_smem;
+    cudaError_t e = cudaFuncSetAttribute(ibm_factor_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ibm_factor_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ibm_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ibm_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    return e;
 }
 
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st) {
-    if (d.wing_count > 0) ibm_factor_kernel<<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
+    if (d.wing_count <= 0) return;
+    if (d.factor_in_smem)
+        ibm_factor_kernel<true><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
+    else
+        ibm_factor_kernel<false><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
 }
 
 void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st) {
-    if (d.wing_count > 0) ibm_solve_kernel<<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+    if (d.wing_count <= 0) return;
+    if (d.solve_in_smem)
+        ibm_solve_kernel<true><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+    else
+        ibm_solve_kernel<false><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
 }
 
 }  // namespace lbm
