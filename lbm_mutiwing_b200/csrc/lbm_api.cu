@@ -108,9 +108,13 @@ using namespace lbm;
 constexpr int NPHASE = 6;
 
 // Immersed-boundary geometry of one step: motion, markers, support boxes,
-// kernel values, band list and map, and the factorised G.  The fused path
-// keeps two sets so that the geometry of step n + 1 (which depends only on
-// the motion) is built while step n still reads its own.
+// kernel values, band list and map, and the factorised G.  It depends only
+// on the motion, so the fused path builds it GEO_AHEAD steps in advance, on
+// side streams, into one of GEO_SETS sets while earlier steps read theirs.
+constexpr int GEO_SETS = 2, GEO_AHEAD = 1;
+// steps per CUDA graph: a multiple of 2 (plane parity) and of GEO_SETS, so
+// a graph ends in the state it started from
+constexpr int GRAPH_STEPS = 2;
 struct GeoSet {
     WingMotion* wm = nullptr;
     double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
@@ -142,16 +146,18 @@ struct LbmHandle {
     FusedConsts fc{};
     int parity = 0;                 // fused path: 0 -> current planes in gA
     float* planes[2] = {nullptr, nullptr};
-    GeoSet geo[2];                  // geometry sets (the plain path uses set 0)
+    GeoSet geo[GEO_SETS];           // geometry sets (the plain path uses set 0)
     int gset = 0;                   // fused path: set of the next step
     int last_gset = 0;              // set of the last completed step
+    bool pending[GEO_SETS] = {};    // set built on the side streams, not yet waited for
     // streams of one fused step: main (bulk kernel, band re-collision),
-    // ibm (right-hand side, solve, spread, forces), aux (the next step's
-    // motion, markers and band list), aux2 (its assembly and factorisation
-    // of G), bc (far field)
-    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_aux = nullptr, s_aux2 = nullptr, s_bc = nullptr;
-    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_geom = nullptr, ev_fact = nullptr, ev_bc = nullptr,
-                ev_list = nullptr;
+    // ibm (right-hand side, solve, spread, forces), bc (far field), and two
+    // pairs of geometry streams used by alternate steps, so that the
+    // geometry builds of consecutive steps run side by side: aux (motion,
+    // markers, band list), aux2 (assembly and factorisation of G)
+    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_bc = nullptr, s_aux[2] = {}, s_aux2[2] = {};
+    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_bc = nullptr, ev_geom[2] = {};
+    cudaEvent_t ev_list[GEO_SETS] = {}, ev_fact[GEO_SETS] = {};   // a set's band list / factor done
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
     int row_len = 4;
@@ -182,7 +188,7 @@ struct LbmHandle {
     long long timed_steps = 0;
     // CUDA graphs of two consecutive steps, one per starting parity; any
     // change of a pointer or value baked into DevState drops them
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2][GEO_SETS] = {};   // by starting plane parity and geometry set
 };
 
 namespace {
@@ -326,9 +332,10 @@ int init_state(LbmHandle* h) {
         CK(cudaGetLastError());
     }
     std::vector<int> em(N, BAND_EMPTY);
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < GEO_SETS; ++s) {
         CK(cudaMemcpy(h->geo[s].band_map, em.data(), N * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemset(h->geo[s].band_n, 0, 2 * sizeof(int)));
+        h->pending[s] = false;
     }
     h->gset = 0;
     h->last_gset = 0;
@@ -412,19 +419,24 @@ void collect_phase_times(LbmHandle* h) {
     h->evused = 0;
 }
 
-// Fused path: the geometry of the coming step (its motion, markers, band list
-// and factorised G) in its own set, before the first step of a call; later
-// steps build the next step's geometry while they run.
-void prime_geometry(LbmHandle* h) {
-    DevState d = current(h);
-    launch_ibm_band(d, h->s_main, nullptr);
-    launch_ibm_factor(d, h->factor_smem, h->s_main);
+// Fused path: the geometry (motion, markers, band list and factorised G) of
+// the first GEO_AHEAD steps of a call, each in its own set; every later
+// step's geometry is built GEO_AHEAD steps ahead while earlier steps run.
+void prime_geometry(LbmHandle* h, int64_t n_steps) {
+    for (int a = 0; a < GEO_AHEAD && a < n_steps; ++a) {
+        DevState d = current(h);
+        use_geo(d, h->geo[(h->gset + a) % GEO_SETS]);
+        d.cycle_ahead = a;
+        launch_ibm_band(d, h->s_main, nullptr);
+        launch_ibm_factor(d, h->factor_smem, h->s_main);
+    }
+    for (bool& p : h->pending) p = false;
 }
 
 // One evolution step (solution.f90:272-422) on the current parity.  On the
-// fused path, prefetch builds the geometry of the following step in the
-// other set.
-void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch) {
+// fused path, prefetch builds the geometry of the step GEO_AHEAD ahead, and
+// drain makes this step wait for it as well (graph boundaries).
+void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drain) {
     DevState d = current(h);
     d.diag = diag ? 1 : 0;
     d.write_fields = fields ? 1 : 0;
@@ -457,33 +469,36 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch) {
         }
         launch_step_advance(d, h->s_main);
     } else {
-        // The immersed boundary, the far field and the next step's geometry
+        // The immersed boundary, the far field and a later step's geometry
         // overlap the bulk kernel.  All read only the current planes, and the
         // writes go to disjoint nodes of the next planes (interior, band,
         // border).  Support boxes keep off the border rows and columns the far
         // field reads, so it needs nothing from the immersed boundary.  The
-        // geometry of this step was built by the previous step (or the
-        // prime); the next step's goes to the other set, whose last reader
-        // was the previous step.
+        // geometry of this step was built GEO_AHEAD steps ago (or by the
+        // prime); the one built now goes to the set whose last reader was
+        // the previous step.
+        const int sn = (h->gset + GEO_AHEAD) % GEO_SETS, s1 = (h->gset + 1) % GEO_SETS;
         DevState dn = d;
-        use_geo(dn, h->geo[1 - h->gset]);
-        dn.cycle_ahead = 1;
+        use_geo(dn, h->geo[sn]);
+        dn.cycle_ahead = GEO_AHEAD;
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
         cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
         if (prefetch) {
-            cudaStreamWaitEvent(h->s_aux, h->ev_main, 0);
+            cudaStream_t sa = h->s_aux[h->parity], sb = h->s_aux2[h->parity];
+            cudaStreamWaitEvent(sa, h->ev_main, 0);
             {
-                PhaseMark pm(h, 0, h->s_aux);
-                launch_ibm_band(dn, h->s_aux, h->ev_geom);
+                PhaseMark pm(h, 0, sa);
+                launch_ibm_band(dn, sa, h->ev_geom[h->parity]);
             }
-            cudaEventRecord(h->ev_list, h->s_aux);
-            cudaStreamWaitEvent(h->s_aux2, h->ev_geom, 0);
+            cudaEventRecord(h->ev_list[sn], sa);
+            cudaStreamWaitEvent(sb, h->ev_geom[h->parity], 0);
             {
-                PhaseMark pm(h, 5, h->s_aux2);
-                launch_ibm_factor(dn, h->factor_smem, h->s_aux2);
+                PhaseMark pm(h, 5, sb);
+                launch_ibm_factor(dn, h->factor_smem, sb);
             }
-            cudaEventRecord(h->ev_fact, h->s_aux2);
+            cudaEventRecord(h->ev_fact[sn], sb);
+            h->pending[sn] = true;
         }
         {
             PhaseMark pm(h, 3, h->s_bc);
@@ -506,44 +521,56 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch) {
             launch_fused_band(d, fields, h->s_main);
         }
         cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
-        if (prefetch) {
-            cudaStreamWaitEvent(h->s_main, h->ev_list, 0);
-            cudaStreamWaitEvent(h->s_main, h->ev_fact, 0);
+        // the geometry kernel of the set built now reads the cycle counter
+        // that the advance below increments
+        if (prefetch) cudaStreamWaitEvent(h->s_main, h->ev_geom[h->parity], 0);
+        // the next step starts once its geometry is complete
+        for (int s : {s1, sn}) {
+            if (!h->pending[s] || (s != s1 && !drain)) continue;
+            cudaStreamWaitEvent(h->s_main, h->ev_list[s], 0);
+            cudaStreamWaitEvent(h->s_main, h->ev_fact[s], 0);
+            h->pending[s] = false;
         }
         launch_step_advance(d, h->s_main);
         h->parity = 1 - h->parity;
         h->last_gset = h->gset;
-        h->gset = 1 - h->gset;
+        h->gset = s1;
     }
     if (h->timing) h->timed_steps += 1;
 }
 
 void drop_graphs(LbmHandle* h) {
-    for (auto& g : h->gexec)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    for (auto& row : h->gexec)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
 }
 
 // Two steps starting at parity p, captured from both streams (the second
 // stream joins and leaves through events, as in eager launches).
-int build_graph(LbmHandle* h, int p) {
-    // planes and geometry sets alternate together; their relation changes
-    // only with a lattice shift, which drops the graphs
+// GRAPH_STEPS steps from plane parity p and geometry set gs.  The graph is
+// self-contained: it starts with the geometry of its first GEO_AHEAD steps
+// complete and its last step waits for the geometry it built for the steps
+// after the graph.
+int build_graph(LbmHandle* h, int p, int gs) {
     const int saved = h->parity, saved_g = h->gset, saved_last = h->last_gset;
-    h->gset = p ^ (h->parity ^ h->gset);
+    bool saved_pending[GEO_SETS];
+    std::copy(h->pending, h->pending + GEO_SETS, saved_pending);
     h->parity = p;
+    h->gset = gs;
+    for (bool& q : h->pending) q = false;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->s_main, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h, false, false, true);
-    enqueue_step(h, false, false, true);
+    for (int k = 0; k < GRAPH_STEPS; ++k) enqueue_step(h, false, false, true, k == GRAPH_STEPS - 1);
     cudaError_t e = cudaStreamEndCapture(h->s_main, &g);
     h->parity = saved;
     h->gset = saved_g;
     h->last_gset = saved_last;
+    std::copy(saved_pending, saved_pending + GEO_SETS, h->pending);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&h->gexec[p], g, 0);
+    e = cudaGraphInstantiate(&h->gexec[p][gs], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
     return 0;
@@ -747,9 +774,9 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         return -1;
     // the second geometry set (fused path: the next step's geometry)
     h->geo[0] = geo_of(d);
-    h->geo[1] = h->geo[0];
-    if (c.precision != LBM_PRECISION_FP64) {
-        GeoSet& g = h->geo[1];
+    for (int s = 1; s < GEO_SETS; ++s) h->geo[s] = h->geo[0];
+    for (int s = 1; s < GEO_SETS && c.precision != LBM_PRECISION_FP64; ++s) {
+        GeoSet& g = h->geo[s];
         if (dalloc(h, &g.wm, wz) || dalloc(h, &g.xb1, npz) || dalloc(h, &g.yb1, npz) || dalloc(h, &g.xb2, nsz) ||
             dalloc(h, &g.yb2, nsz) || dalloc(h, &g.kx, 6 * nsz) || dalloc(h, &g.ky, 6 * nsz) ||
             dalloc(h, &g.box, 4 * nsz) || dalloc(h, &g.claim_cnt, nsz + 1) || dalloc(h, &g.pb, nsz * BOX_SLOTS) ||
@@ -767,11 +794,18 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CK(cudaStreamCreateWithPriority(&h->s_main, cudaStreamNonBlocking, prio_lo));
     CK(cudaStreamCreateWithPriority(&h->s_ibm, cudaStreamNonBlocking, prio_hi));
-    CK(cudaStreamCreateWithPriority(&h->s_aux, cudaStreamNonBlocking, prio_hi));
-    CK(cudaStreamCreateWithPriority(&h->s_aux2, cudaStreamNonBlocking, prio_hi));
+    for (int k = 0; k < 2; ++k) {
+        CK(cudaStreamCreateWithPriority(&h->s_aux[k], cudaStreamNonBlocking, prio_hi));
+        CK(cudaStreamCreateWithPriority(&h->s_aux2[k], cudaStreamNonBlocking, prio_hi));
+        CK(cudaEventCreateWithFlags(&h->ev_geom[k], cudaEventDisableTiming));
+    }
     CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, prio_hi));
-    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_geom, &h->ev_fact, &h->ev_bc, &h->ev_list})
+    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_bc})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (int s = 0; s < GEO_SETS; ++s) {
+        CK(cudaEventCreateWithFlags(&h->ev_list[s], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->ev_fact[s], cudaEventDisableTiming));
+    }
     CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
     h->pinned_n = 4096;
     if (c.precision != LBM_PRECISION_FP64) h->fc = fused_consts(d);
@@ -864,13 +898,17 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     // all but the last two steps replay a two-step CUDA graph; the last two
     // may write fields or diagnostics and are launched directly
     const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
-    if (h->d.precision != 0 && n_steps > 0) prime_geometry(h);
+    const bool fused = h->d.precision != 0;
+    if (fused && n_steps > 0) prime_geometry(h, n_steps);
     int64_t n = 0;
-    if (graphs) {
-        for (; n + 2 < n_steps - 1; n += 2) {
-            if (!h->gexec[h->parity] && build_graph(h, h->parity)) return -1;
-            CK(cudaGraphLaunch(h->gexec[h->parity], h->s_main));
-            h->last_gset = 1 - h->gset;
+    if (graphs && fused) {
+        // whole graphs while the last two steps and the geometry they need
+        // stay outside
+        for (; n + GRAPH_STEPS <= n_steps - 2; n += GRAPH_STEPS) {
+            cudaGraphExec_t& ge = h->gexec[h->parity][h->gset];
+            if (!ge && build_graph(h, h->parity, h->gset)) return -1;
+            CK(cudaGraphLaunch(ge, h->s_main));
+            h->last_gset = (h->gset + GEO_SETS - 1) % GEO_SETS;
         }
     }
     for (; n < n_steps; ++n) {
@@ -890,7 +928,7 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
             }
             fields = true;
         }
-        enqueue_step(h, fields, last, !last);
+        enqueue_step(h, fields, last, n + GEO_AHEAD <= n_steps - 1, false);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->s_main));
@@ -1121,10 +1159,14 @@ void lbm_destroy(LbmHandle* h) {
     drop_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->pinned) cudaFreeHost(h->pinned);
-    for (cudaStream_t s : {h->s_main, h->s_ibm, h->s_aux, h->s_aux2, h->s_bc})
+    for (cudaStream_t s : {h->s_main, h->s_ibm, h->s_aux[0], h->s_aux[1], h->s_aux2[0], h->s_aux2[1], h->s_bc})
         if (s) cudaStreamDestroy(s);
-    for (cudaEvent_t e : {h->ev_geom, h->ev_fact, h->ev_bc, h->ev_ibm, h->ev_main, h->ev_list})
+    for (cudaEvent_t e : {h->ev_geom[0], h->ev_geom[1], h->ev_bc, h->ev_ibm, h->ev_main})
         if (e) cudaEventDestroy(e);
+    for (int s = 0; s < GEO_SETS; ++s) {
+        if (h->ev_list[s]) cudaEventDestroy(h->ev_list[s]);
+        if (h->ev_fact[s]) cudaEventDestroy(h->ev_fact[s]);
+    }
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
     delete h;
 }

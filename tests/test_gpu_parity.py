@@ -198,13 +198,20 @@ def test_fused_move_mesh(gpu_lib):
 
 
 def test_graph_replay_matches_direct_launches(gpu_lib):
-    ep = episode_b(13)
+    """Graph replay (whole multi-step graphs plus a direct tail), direct
+    launches, and the same steps split over two calls give identical bits:
+    the geometry built ahead of time on side streams is the same geometry."""
+    ep = episode_b(31)
     out = []
-    for graphs in (True, False):
+    for graphs, split in ((True, False), (False, False), (True, True)):
         for prec in (api.PRECISION_FP64, api.PRECISION_FP32):
             with api.Simulation(ep, prec, graphs=graphs) as s:
-                rows = s.step(13)
+                if split:
+                    rows = np.concatenate([s.step(17), s.step(13)])
+                else:
+                    rows = s.step(30)
                 out.append((prec, rows, s.f()))
     for k in range(2):
-        assert np.array_equal(out[k][1], out[k + 2][1])
-        assert np.array_equal(out[k][2], out[k + 2][2])
+        for other in (k + 2, k + 4):
+            assert np.array_equal(out[k][1], out[other][1])
+            assert np.array_equal(out[k][2], out[other][2])
