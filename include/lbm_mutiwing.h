@@ -116,6 +116,15 @@ int lbm_reset_sums(LbmHandle* h);
  * on that step. */
 int lbm_get_fields(LbmHandle* h, double* rho, double* u, double* v, double* pre);
 
+/* output (solution.f90:132-241): every stride_x-th node of every
+ * stride_y-th row, row by row, of u/UU, v/UU, the pressure and the vorticity
+ * dv/dx - du/dy (centred inside, second-order one-sided on the border),
+ * computed on the device; ((nx-1)/stride_x+1) x ((ny-1)/stride_y+1) values
+ * each (any pointer may be NULL).  Needs the fields of the last step
+ * (LBM_STEP_FIELDS on the FP32 path). */
+int lbm_get_output(LbmHandle* h, int32_t stride_x, int32_t stride_y, double* u, double* v, double* pre,
+                   double* vort);
+
 /* erranalysis (solution.f90:77-130) on the fields of the last two steps. */
 int lbm_err(LbmHandle* h, double* err);
 

@@ -58,6 +58,7 @@ SIGNATURES = [
     ("lbm_get_sums", C.c_int, [C.c_void_p, D, I32, I32]),
     ("lbm_reset_sums", C.c_int, [C.c_void_p]),
     ("lbm_get_fields", C.c_int, [C.c_void_p, D, D, D, D]),
+    ("lbm_get_output", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, D, D, D, D]),
     ("lbm_err", C.c_int, [C.c_void_p, D]),
     ("lbm_err_fields_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                          C.c_int64, C.c_int32, C.c_void_p, D, C.c_char_p, C.c_int32]),
@@ -226,6 +227,14 @@ class Simulation:
         """rho, u, v, pre as (ny, nx) arrays."""
         arrs = [np.zeros((self.ny, self.nx)) for _ in range(4)]
         self._check(self.L.lbm_get_fields(self.h, *[_dp(a) for a in arrs]))
+        return tuple(arrs)
+
+    def output(self, stride_x: int = 2, stride_y: int = 2):
+        """u/UU, v/UU, pre, vorticity at the output nodes as (ony, onx) arrays
+        (output, solution.f90:132-241)."""
+        onx, ony = (self.nx - 1) // stride_x + 1, (self.ny - 1) // stride_y + 1
+        arrs = [np.zeros((ony, onx)) for _ in range(4)]
+        self._check(self.L.lbm_get_output(self.h, stride_x, stride_y, *[_dp(a) for a in arrs]))
         return tuple(arrs)
 
     def err(self) -> float:

@@ -21,6 +21,8 @@
 // The zero zones of the banded storage (entries past the bandwidth, rows past
 // the last segment) make every panel-shaped read in bounds and zero where it
 // falls outside the matrix, so the inner loops load without conditions.
+#include <mutex>
+
 #include "bulk_copy.cuh"
 #include "lbm_kernels.h"
 
@@ -439,15 +441,34 @@ size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool f
     return z + perm + inv + (factor_in_smem ? (size_t)wing_storage_max * sizeof(double) : 0);
 }
 
+// The dynamic shared-memory limit is a per-device property of each kernel,
+// shared by every handle: it is raised once to the device's opt-in maximum
+// (minus the kernel's static shared memory), never lowered, so handles of
+// different sizes created in any order, from any thread, all launch.
+static std::mutex g_prepare_mutex;
+static unsigned long long g_prepared_devices = 0;
+
+template <class K>
+static cudaError_t raise_smem_limit(K kernel, int optin) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
-    const int fs = (int)factor_smem, ss = (int)solve_smem;
-    cudaError_t e = cudaFuncSetAttribute(ibm_factor_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ibm_factor_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ibm_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ibm_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    if (factor_smem + 16 * 1024 > (size_t)optin || solve_smem + 1024 > (size_t)optin) return cudaErrorInvalidValue;
+    std::lock_guard<std::mutex> lock(g_prepare_mutex);
+    if (dev < 64 && (g_prepared_devices >> dev) & 1ULL) return cudaSuccess;
+    e = raise_smem_limit(ibm_factor_kernel<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel<false>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<false>, optin);
+    if (e == cudaSuccess && dev < 64) g_prepared_devices |= 1ULL << dev;
     return e;
 }
 

@@ -266,4 +266,60 @@ void launch_plain_shift(const DevState& d, int dr, cudaStream_t st) {
     plain_shift_kernel<<<(d.ny + 127) / 128, 128, 0, st>>>(d, dr);
 }
 
+// output (solution.f90:132-241): at every sx-th node of every sy-th row,
+// u/UU, v/UU, the pressure and the vorticity dv/dx - du/dy with centred
+// differences inside and second-order one-sided ones on the border rows and
+// columns (:197-211), in the reference's operation order.  The fused path's
+// pressure is rho/3 of the streamed populations inside and the border
+// store's sum / 3 on the border, as its field export gives it.
+__global__ void output_fields_kernel(DevState d, int sx, int sy, int onx, int ony, double* out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long per = (long long)onx * ony;
+    if (t >= per) return;
+    const int oi = (int)(t % onx), oj = (int)(t / onx);
+    const int i = oi * sx, j = oj * sy;
+    const bool fused = d.precision != 0;
+    const double* U = fused ? d.fo_u : d.u;
+    const double* V = fused ? d.fo_v : d.v;
+    auto u = [&](int a, int b) { return U[pidx(d, a, b)]; };
+    auto v = [&](int a, int b) { return V[pidx(d, a, b)]; };
+    const double uu = d.uu, sc = d.scale;
+    double dvx, duy;
+    if (i == d.nx - 1)
+        dvx = (1.5 * v(i, j) - 2.0 * v(i - 1, j) + 0.5 * v(i - 2, j)) / (uu * sc);
+    else if (i == 0)
+        dvx = (-1.5 * v(i, j) + 2.0 * v(i + 1, j) - 0.5 * v(i + 2, j)) / (uu * sc);
+    else
+        dvx = (v(i + 1, j) - v(i - 1, j)) / (uu * 2.0 * sc);
+    if (j == d.ny - 1)
+        duy = (1.5 * u(i, j) - 2.0 * u(i, j - 1) + 0.5 * u(i, j - 2)) / (uu * sc);
+    else if (j == 0)
+        duy = (-1.5 * u(i, j) + 2.0 * u(i, j + 1) - 0.5 * u(i, j + 2)) / (uu * sc);
+    else
+        duy = (u(i, j + 1) - u(i, j - 1)) / (uu * 2.0 * sc);
+    double pre;
+    if (!fused) {
+        pre = d.pre[pidx(d, i, j)];
+    } else if (i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1) {
+        const long long eper = 2LL * d.ny + 2LL * d.nx;
+        const long long e = (i == 0) ? j : (i == d.nx - 1) ? d.ny + j : (j == 0) ? 2LL * d.ny + i
+                                                                               : 2LL * d.ny + d.nx + i;
+        double s = 0.0;
+        for (int k = 0; k < 9; ++k) s = s + d.edge_f0[k * eper + e];
+        pre = s / 3.0;
+    } else {
+        pre = d.fo_rho[pidx(d, i, j)] / 3.0;
+    }
+    out[t] = u(i, j) / uu;
+    out[per + t] = v(i, j) / uu;
+    out[2 * per + t] = pre;
+    out[3 * per + t] = dvx - duy;
+}
+
+void launch_output_fields(const DevState& d, int sx, int sy, double* out, cudaStream_t st) {
+    const int onx = (d.nx - 1) / sx + 1, ony = (d.ny - 1) / sy + 1;
+    const long long n = (long long)onx * ony;
+    output_fields_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(d, sx, sy, onx, ony, out);
+}
+
 }  // namespace lbm

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <queue>
 #include <string>
 #include <vector>
@@ -188,10 +189,20 @@ struct LbmHandle {
     long long timed_steps = 0;
     // CUDA graphs of two consecutive steps, one per starting parity; any
     // change of a pointer or value baked into DevState drops them
-    cudaGraphExec_t gexec[2][GEO_SETS] = {};   // by starting plane parity and geometry set
+    cudaGraphExec_t gexec[2][GEO_SETS] = {};
+    double* d_out = nullptr;        // strided output fields (SAVE)
+    size_t out_cap = 0;   // by starting plane parity and geometry set
 };
 
 namespace {
+
+// Graph capture and device-wide operations of different handles must not
+// interleave: an allocation, a free or a device synchronisation issued by
+// one thread while another thread captures a step graph invalidates that
+// capture.  Every entry point that allocates, frees, synchronises the device
+// or captures holds this lock (handles are otherwise independent).
+std::recursive_mutex g_device_mutex;
+using DeviceLock = std::lock_guard<std::recursive_mutex>;
 
 void drop_graphs(LbmHandle* h);
 
@@ -212,6 +223,7 @@ int cuda_fail(LbmHandle* h, cudaError_t e, const char* where) {
 
 template <class T>
 int dalloc(LbmHandle* h, T** p, size_t count) {
+    DeviceLock lock(g_device_mutex);
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     cudaError_t e = cudaMalloc((void**)p, bytes);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
@@ -353,6 +365,7 @@ int init_state(LbmHandle* h) {
 }
 
 int ensure_rows(LbmHandle* h, int64_t n) {
+    DeviceLock lock(g_device_mutex);
     if (n <= h->rows_cap) return 0;
     if (h->d_rowbuf) {
         cudaFree(h->d_rowbuf);
@@ -555,6 +568,7 @@ void drop_graphs(LbmHandle* h) {
 // complete and its last step waits for the geometry it built for the steps
 // after the graph.
 int build_graph(LbmHandle* h, int p, int gs) {
+    DeviceLock lock(g_device_mutex);
     const int saved = h->parity, saved_g = h->gset, saved_last = h->last_gset;
     bool saved_pending[GEO_SETS];
     std::copy(h->pending, h->pending + GEO_SETS, saved_pending);
@@ -600,6 +614,7 @@ void lbm_config_default(LbmConfig* c) {
 }
 
 int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* points_per_wing, LbmHandle** out) {
+    DeviceLock lock(g_device_mutex);
     if (!out) return -1;
     *out = nullptr;
     LbmHandle* h = new LbmHandle();
@@ -814,6 +829,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
 }
 
 int lbm_reset(LbmHandle* h) {
+    DeviceLock lock(g_device_mutex);
     if (!h) return -1;
     CK(cudaSetDevice(h->cfg.device));
     CK(cudaDeviceSynchronize());
@@ -821,6 +837,7 @@ int lbm_reset(LbmHandle* h) {
 }
 
 int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_t ncols) {
+    DeviceLock lock(g_device_mutex);
     if (!h) return -1;
     const int nc = 1 + 9 * h->cfg.wing_count;
     if (ncols != nc) return fail(h, "motion table needs 1 + 9*wing_count columns");
@@ -1001,6 +1018,36 @@ int lbm_get_fields(LbmHandle* h, double* rho, double* u, double* v, double* pre)
     return 0;
 }
 
+int lbm_get_output(LbmHandle* h, int32_t stride_x, int32_t stride_y, double* u, double* v, double* pre,
+                   double* vort) {
+    if (!h) return -1;
+    if (stride_x < 1 || stride_y < 1) return fail(h, "output strides must be >= 1");
+    if (!h->fields_valid) return fail(h, "fields are not available: step with LBM_STEP_FIELDS first");
+    CK(cudaSetDevice(h->cfg.device));
+    const DevState d = current(h);
+    const int onx = (d.nx - 1) / stride_x + 1, ony = (d.ny - 1) / stride_y + 1;
+    const size_t per = (size_t)onx * ony;
+    if (h->out_cap < 4 * per) {
+        DeviceLock lock(g_device_mutex);
+        if (h->d_out) {
+            cudaFree(h->d_out);
+            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_out), h->allocs.end());
+            h->dev_bytes -= (int64_t)h->out_cap * sizeof(double);
+            h->d_out = nullptr;
+            h->out_cap = 0;
+        }
+        if (dalloc(h, &h->d_out, 4 * per)) return -1;
+        h->out_cap = 4 * per;
+    }
+    launch_output_fields(d, stride_x, stride_y, h->d_out, h->s_main);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s_main));
+    double* dst[4] = {u, v, pre, vort};
+    for (int k = 0; k < 4; ++k)
+        if (dst[k]) CK(cudaMemcpy(dst[k], h->d_out + k * per, per * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
 int lbm_err(LbmHandle* h, double* err) {
     if (!h || !err) return -1;
     if (!h->err_valid) return fail(h, "err is not available: step at least twice with LBM_STEP_ERR first");
@@ -1013,6 +1060,7 @@ int lbm_err(LbmHandle* h, double* err) {
 }
 
 int lbm_get_f(LbmHandle* h, double* f) {
+    DeviceLock lock(g_device_mutex);
     if (!h || !f) return -1;
     CK(cudaSetDevice(h->cfg.device));
     const DevState d = current(h);
@@ -1035,6 +1083,7 @@ int lbm_get_f(LbmHandle* h, double* f) {
 }
 
 int lbm_set_f(LbmHandle* h, const double* f) {
+    DeviceLock lock(g_device_mutex);
     if (!h || !f) return -1;
     CK(cudaSetDevice(h->cfg.device));
     const DevState d = current(h);
@@ -1091,6 +1140,7 @@ int lbm_get_markers(LbmHandle* h, double* xb1, double* yb1, double* xb2, double*
 }
 
 int lbm_move_mesh(LbmHandle* h, int32_t dr) {
+    DeviceLock lock(g_device_mutex);
     if (!h) return -1;
     if (dr != 1 && dr != -1) return fail(h, "dr must be +1 or -1");
     CK(cudaSetDevice(h->cfg.device));
@@ -1154,6 +1204,7 @@ const char* lbm_last_error(const LbmHandle* h) { return h ? h->err.c_str() : "nu
 
 void lbm_destroy(LbmHandle* h) {
     if (!h) return;
+    DeviceLock lock(g_device_mutex);
     cudaSetDevice(h->cfg.device);
     cudaDeviceSynchronize();
     drop_graphs(h);

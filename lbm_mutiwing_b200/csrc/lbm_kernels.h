@@ -9,6 +9,8 @@ void launch_plain_stream(const DevState& d, cudaStream_t st);
 void launch_plain_moments(const DevState& d, cudaStream_t st);
 void launch_plain_collide(const DevState& d, cudaStream_t st);
 void launch_plain_shift(const DevState& d, int dr, cudaStream_t st);
+// strided output fields u/UU, v/UU, pre, vorticity (4 planes of onx x ony)
+void launch_output_fields(const DevState& d, int sx, int sy, double* out, cudaStream_t st);
 // both paths
 void launch_outer_bc(const DevState& d, cudaStream_t st);
 void launch_err(const DevState& d, double* partial, double* out, cudaStream_t st);

@@ -238,3 +238,25 @@ def read_motion_file(path: str, wing_count: int) -> np.ndarray:
     if not rows:
         raise ValueError("motion table is empty")
     return np.asarray(rows, dtype=np.float64)
+
+
+_MIX_CACHE: dict = {}
+
+
+def by_name(name: str, steps: int = 8) -> Episode:
+    """Episode of a named workload for an online server: ``800x400``,
+    ``4000x2000``, ``16000x8000``, or ``mix:<k>`` (episode k of the seeded
+    64-episode mixed batch).  Online episodes take their motion from the
+    clients, so the motion table is kept short."""
+    if name == "800x400":
+        return tandem_800x400(steps=steps)
+    if name == "4000x2000":
+        return tandem_4000x2000(steps=steps)
+    if name == "16000x8000":
+        return formation_16000x8000(steps=steps)
+    if name.startswith("mix:"):
+        k = int(name[4:])
+        if "mix" not in _MIX_CACHE:
+            _MIX_CACHE["mix"] = mixed_batch(64, steps=steps)
+        return _MIX_CACHE["mix"][k]
+    raise ValueError(f"unknown workload {name!r}")
