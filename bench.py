@@ -38,6 +38,9 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# many episodes' streams in flight (the batched and served measurements)
+# need more hardware work queues than the default 8; read at context creation
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS (lattice node updates per second / 1e6)"
@@ -54,6 +57,7 @@ def parse():
     p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     p.add_argument("--workload", default="4000x2000", choices=["800x400", "4000x2000"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-serving", action="store_true", help="skip the batched and served measurements")
     return p.parse_args()
 
 
@@ -181,6 +185,67 @@ def config_of(ep, storage, world):
             "parallelism": f"{world} independent episodes (one per GPU)"}
 
 
+def serving_metrics(steps=200, requests=3, rate_hz=20.0):
+    """The seeded 64-episode mixed batch (grids 401x201 .. 2001x1001, 1-4
+    wings): (1) every episode advanced `steps` steps, all resident and in
+    flight at once (FP32), against the same episodes served one at a time
+    through the plain FP64 path; (2) 64 online clients (one per episode) on
+    the ZeroMQ server with Poisson arrivals, segments of 100-2000 steps, SAVE
+    with p = 0.05: STEP latency percentiles at the client; (3) the FP32
+    path's segment-averaged forces against FP64 for one client's segments."""
+    import threading
+    from lbm_mutiwing_b200 import api, batch, loadgen
+    from lbm_mutiwing_b200 import protocol as P
+    from lbm_mutiwing_b200 import workloads as wl
+    from lbm_mutiwing_b200.serve import Server
+    eps = wl.mixed_batch(64, steps=steps + 8)
+    nodes = sum(e.nx * e.ny for e in eps)
+    sims = batch.create(eps, api.PRECISION_FP32)
+    batch.advance_together(sims, 4, first_cycle=1)
+    wall = batch.advance_together(sims, steps, first_cycle=5)
+    for s in sims:
+        s.close()
+    batched = nodes * steps / wall / 1e6
+    plain_s, plain_nu = batch.advance_one_at_a_time(eps, max(8, steps // 4))
+    plain = plain_nu / plain_s / 1e6
+    srv = Server("tcp://127.0.0.1:0", wl.by_name, "mix:0", precision=api.PRECISION_FP32, workers=64)
+    th = threading.Thread(target=srv.serve, kwargs={"idle_timeout_s": 600}, daemon=True)
+    th.start()
+    names = [f"mix:{k}" for k in range(64)]
+    res = loadgen.poisson_load(f"tcp://127.0.0.1:{srv.port}", names, wl.by_name, requests_per_client=requests,
+                               rate_hz=rate_hz)
+    srv.stop()
+    th.join(60)
+    srv.close()
+    # FP32 vs FP64 segment-averaged forces of one client's segments
+    ep = wl.by_name("mix:1")
+    rng = np.random.default_rng(7)
+    dt = ep.scale * ep.uu
+    lines, cyc = ["RESET 0.0"], 1
+    for n in (150, 400, 250):
+        cyc += n
+        lines.append(loadgen.step_line((cyc - 1) * dt, rng.normal(0, 0.05, 3 * ep.wing_count)))
+    from lbm_mutiwing_b200.session import EpisodeSession
+    rows = {}
+    for prec in (api.PRECISION_FP64, api.PRECISION_FP32):
+        with api.Simulation(ep, prec, motion_source=api.MOTION_STREAM) as sim:
+            se = EpisodeSession(sim, ep)
+            rows[prec] = [np.array(P.parse_force_reply(se.handle(P.parse(l, ep.wing_count)))) for l in lines]
+    W = ep.wing_count
+    err = 0.0
+    for a, b in zip(rows[api.PRECISION_FP32], rows[api.PRECISION_FP64]):
+        fa, fb = a[1:1 + 3 * W], b[1:1 + 3 * W]
+        err = max(err, float(np.max(np.abs(fa - fb)) / max(float(np.max(np.abs(fb))), 1e-30)))
+    return {"episodes": len(eps), "nodes": nodes, "wings": sum(e.wing_count for e in eps),
+            "batched_fp32_mlups": batched, "one_at_a_time_fp64_mlups": plain,
+            "batched_over_one_at_a_time": batched / plain,
+            "served_clients": len(names), "served_steps": len(res.step_latency_s),
+            "served_step_p50_ms": res.percentile(50) * 1e3, "served_step_p99_ms": res.percentile(99) * 1e3,
+            "served_mlups": res.mlups(), "served_errors": len(res.errors),
+            "fp32_vs_fp64_force_max_rel_err": err,
+            "force_err_sample": "segment-averaged per-wing Fx, Fy, M of mix episode 1, 3 STEP segments"}
+
+
 def run_ours(args):
     from lbm_mutiwing_b200 import ranks
     rank, world, local = ranks.init("nccl")
@@ -284,6 +349,8 @@ def run_ours(args):
         mlups, steps, dt = oracle_steps(workload(args.workload, 200), threads, budget_s=15.0)
         line["cpu_baseline"] = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{steps} full steps of {ep.name} after 1 untimed step ({dt:.1f} s)"}
+    if rank == 0 and world == 1 and not args.no_serving:
+        line["serving"] = serving_metrics()
     if rank == 0:
         print(json.dumps(line))
     ranks.finish()

@@ -190,15 +190,23 @@ def formation_16000x8000(steps: int = 20000) -> Episode:
 def mixed_batch(count: int = 64, seed: int = 20261203, steps: int = 1000) -> List[Episode]:
     """Mixed batch: grids from {400x200, 800x400, 1200x600, 2000x1000}
     nodes at dx = 0.01, 1-4 NACA00xx wings (thickness 8-18 %, 100-300
-    markers), pitch 5-25 deg, heave 0.1-0.6 chord, f 0.2-1.0."""
+    markers), pitch 5-25 deg, heave 0.1-0.6 chord, f 0.2-1.0, seeded.
+
+    Wings sit 1.5 chords apart, leading edge at least 0.75 chord from the
+    inflow border and trailing edge 1.25 chords from the outflow border, so
+    the draw of 1-4 wings is capped by what the domain holds (two wings in
+    a 4-chord domain); the heave amplitude is capped at 0.3 h - 0.5 so the
+    wings stay clear of the top and bottom borders in the 2-chord-high grids."""
     rng = np.random.default_rng(seed)
     sizes = [(4.0, 2.0), (8.0, 4.0), (12.0, 6.0), (20.0, 10.0)]
     eps = []
     for e in range(count):
         w, h = sizes[int(rng.integers(0, 4))]
-        nw = int(rng.integers(1, 5))
-        spacing_x = 1.5 if w >= 8.0 else 0.9
-        x0 = -0.25 * w + 0.5
+        nw_draw = int(rng.integers(1, 5))
+        spacing_x = 1.5
+        lo, hi = -0.5 * w + 1.0, 0.5 * w - 2.0        # quarter-chord positions that fit
+        nw = max(1, min(nw_draw, int((hi - lo) / spacing_x) + 1))
+        x0 = lo
         nx, ny, ox, oy = lattice(w, h, 0.01)
         ep = Episode(name=f"mix{e:02d}", nx=nx, ny=ny, scale=0.01, re=float(rng.uniform(200, 1000)),
                      ox=ox, oy=oy, wing_x_origin=x0, wing_x_spacing=spacing_x, wing_y_origin=0.0,
@@ -210,7 +218,7 @@ def mixed_batch(count: int = 64, seed: int = 20261203, steps: int = 1000) -> Lis
         for k in range(nw):
             wings.append(WingMotion(x=x0 + k * spacing_x, y=0.0,
                                     pitch_amp=float(rng.uniform(5, 25)) * math.pi / 180.0,
-                                    heave_amp=float(rng.uniform(0.1, 0.6)) * min(1.0, h / 8.0),
+                                    heave_amp=min(float(rng.uniform(0.1, 0.6)), 0.3 * h - 0.5),
                                     freq=float(rng.uniform(0.2, 1.0)),
                                     phase=float(rng.uniform(0, 2 * math.pi))))
         ep.motion = motion_table(wings, (steps + 1) * 0.01 * ep.uu, 0.01 * ep.uu)
