@@ -236,6 +236,11 @@ __global__ void fused_import_kernel(DevState d, const double* f, float* g) {
     }
 }
 
+bool is_bulk_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(fused_bulk_kernel<false>) ||
+           func == reinterpret_cast<const void*>(fused_bulk_kernel<true>);
+}
+
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st) {
     dim3 b(BULK_TX), g((d.nx - 2 + BULK_TX - 1) / BULK_TX, (d.ny - 2 + BULK_ROWS - 1) / BULK_ROWS);
     if (fields)

@@ -149,6 +149,7 @@ struct LbmHandle {
     float* planes[2] = {nullptr, nullptr};
     GeoSet geo[GEO_SETS];           // geometry sets (the plain path uses set 0)
     int gset = 0;                   // fused path: set of the next step
+    int prio_lo = 0, prio_hi = 0;   // stream priority range of the device
     int last_gset = 0;              // set of the last completed step
     bool pending[GEO_SETS] = {};    // set built on the side streams, not yet waited for
     // streams of one fused step: main (bulk kernel, band re-collision),
@@ -584,7 +585,28 @@ int build_graph(LbmHandle* h, int p, int gs) {
     h->last_gset = saved_last;
     std::copy(saved_pending, saved_pending + GEO_SETS, h->pending);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&h->gexec[p][gs], g, 0);
+    // Graph launches run every node at the priority of the launch stream
+    // unless nodes carry their own: the bulk kernel gets the low priority
+    // and every other kernel the high one, so the immersed-boundary, far
+    // field and geometry kernels are dispatched ahead of pending bulk blocks
+    // instead of after the bulk grid.
+    size_t nn = 0;
+    e = cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+    for (size_t k = 0; e == cudaSuccess && k < nn; ++k) {
+        cudaGraphNodeType ty;
+        e = cudaGraphNodeGetType(nodes[k], &ty);
+        if (e != cudaSuccess || ty != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        e = cudaGraphKernelNodeGetParams(nodes[k], &kp);
+        if (e != cudaSuccess) break;
+        cudaKernelNodeAttrValue v;
+        std::memset(&v, 0, sizeof(v));
+        v.priority = is_bulk_kernel(kp.func) ? h->prio_lo : h->prio_hi;
+        e = cudaGraphKernelNodeSetAttribute(nodes[k], cudaKernelNodeAttributePriority, &v);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->gexec[p][gs], g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
     return 0;
@@ -807,6 +829,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     // ahead of waiting bulk blocks
     int prio_lo = 0, prio_hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    h->prio_lo = prio_lo;
+    h->prio_hi = prio_hi;
     CK(cudaStreamCreateWithPriority(&h->s_main, cudaStreamNonBlocking, prio_lo));
     CK(cudaStreamCreateWithPriority(&h->s_ibm, cudaStreamNonBlocking, prio_hi));
     for (int k = 0; k < 2; ++k) {
