@@ -248,6 +248,149 @@ void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cud
     else
         fused_bulk_kernel<false><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr);
 }
+// ------------------------------------------------------------ far field
+// boundary_condition1 (boundary_condition.f90:288-858) for the fused path:
+// the same LODI update and edge populations as outer_bc_kernel, with the
+// moment transforms written out (M f and M^-1 m = M^T diag(1/9, 1/36,
+// 1/36, 1/6, 1/12, 1/6, 1/12, 1/4, 1/4) m), one reciprocal per density,
+// and fused multiply-adds -- this path is compared with tolerances, and the
+// kernel runs while the bulk kernel saturates memory, so its dependent
+// arithmetic chain is kept short.
+struct FarMom {
+    double r, u, v;
+};
+
+__device__ __forceinline__ void border_f0(const DevState& d, int i, int j, double* f) {
+    const long long per = 2LL * d.ny + 2LL * d.nx;
+    const long long e = (i == 0) ? j : (i == d.nx - 1) ? d.ny + j : (j == 0) ? 2LL * d.ny + i : 2LL * d.ny + d.nx + i;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = d.edge_f0[k * per + e];
+}
+
+__device__ __forceinline__ void pulled_f0(const DevState& d, int i, int j, double* f) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + pidx(d, i - ex(k), j - ey(k))] + weight(k);
+}
+
+__device__ __forceinline__ FarMom far_moments(const double* f) {
+    const double r = (((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7]))) + f[8];
+    const double jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+    const double jy = (f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8]);
+    const double ir = 1.0 / r;
+    return FarMom{r, jx * ir, jy * ir};
+}
+
+// LODI update of the left (side = 0) or right (side = 1) column at row j
+// (boundary_condition.f90:413-441, 495-521)
+__device__ FarMom far_lodi(const DevState& d, int side, int j, double* fnb) {
+    const double cs = (double)sqrtf(3.0f) / 3.0;
+    const int ib = side == 0 ? 0 : d.nx - 1, i1 = side == 0 ? 1 : d.nx - 2, i2 = side == 0 ? 2 : d.nx - 3;
+    double fb[9], f2[9];
+    border_f0(d, ib, j, fb);
+    pulled_f0(d, i1, j, fnb);
+    pulled_f0(d, i2, j, f2);
+    const FarMom b = far_moments(fb), m1 = far_moments(fnb), m2 = far_moments(f2);
+    const double sg = side == 0 ? -1.0 : 1.0;   // one-sided difference toward the inside
+    const double rhox = sg * (3.0 * b.r - 4.0 * m1.r + m2.r) * 0.5;
+    const double ux = sg * (3.0 * b.u - 4.0 * m1.u + m2.u) * 0.5;
+    const double vx = sg * (3.0 * b.v - 4.0 * m1.v + m2.v) * 0.5;
+    double lx1 = 0.0, lx2 = 0.0, lx3 = 0.0;
+    if (side == 0) {
+        lx1 = (b.u - cs) * (cs * cs * rhox - cs * b.r * ux);
+        lx2 = (b.u < 0.0) ? b.u * vx : 0.0;
+    } else {
+        lx2 = (b.u >= 0.0) ? b.u * vx : 0.0;
+        lx3 = (b.u + cs) * (cs * cs * rhox + cs * b.r * ux);
+    }
+    FarMom o;
+    o.r = b.r - (lx1 + lx3) * 1.5;
+    o.u = b.u + (lx1 - lx3) / (2.0 * cs * o.r);
+    o.v = b.v - lx2;
+    return o;
+}
+
+__device__ __forceinline__ void far_meq(const FarMom& m, double* t) {
+    const double jx = m.r * m.u, jy = m.r * m.v, ir = 1.0 / m.r;
+    const double q = (jx * jx + jy * jy) * ir;
+    t[0] = m.r; t[1] = -2.0 * m.r + 3.0 * q; t[2] = m.r - 3.0 * q;
+    t[3] = jx; t[4] = -jx; t[5] = jy; t[6] = -jy;
+    t[7] = (jx * jx - jy * jy) * ir; t[8] = jx * jy * ir;
+}
+
+// edge populations f = M^-1 [m_eq(edge) + (I - S)(M f0(nbr) - m_eq(nbr))]
+__device__ void far_edge(const DevState& d, int ie, int je, const FarMom& e, const double* fn, const FarMom& nb) {
+    double t1[9], t2[9], m[9];
+    far_meq(e, t1);
+    far_meq(nb, t2);
+    const double s14 = (fn[1] + fn[3]) + (fn[2] + fn[4]), s58 = (fn[5] + fn[7]) + (fn[6] + fn[8]);
+    const double d13 = fn[1] - fn[3], d24 = fn[2] - fn[4], a5 = fn[5] - fn[7], a6 = fn[6] - fn[8];
+    m[0] = (fn[0] + s14) + s58;
+    m[1] = -4.0 * fn[0] - s14 + 2.0 * s58;
+    m[2] = 4.0 * fn[0] - 2.0 * s14 + s58;
+    m[3] = d13 + a5 - a6;
+    m[4] = -2.0 * d13 + a5 - a6;
+    m[5] = d24 + a5 + a6;
+    m[6] = -2.0 * d24 + a5 + a6;
+    m[7] = (fn[1] + fn[3]) - (fn[2] + fn[4]);
+    m[8] = (fn[5] + fn[7]) - (fn[6] + fn[8]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m[k] = t1[k] + (1.0 - d.s[k]) * (m[k] - t2[k]);
+    const double b0 = m[0] * (1.0 / 9.0), b1 = m[1] * (1.0 / 36.0), b2 = m[2] * (1.0 / 36.0);
+    const double b3 = m[3] * (1.0 / 6.0), b4 = m[4] * (1.0 / 12.0), b5 = m[5] * (1.0 / 6.0);
+    const double b6 = m[6] * (1.0 / 12.0), b7 = m[7] * 0.25, b8 = m[8] * 0.25;
+    const double rA = b0 - b1 - 2.0 * b2, rD = b0 + 2.0 * b1 + b2;
+    const double x34 = b3 - 2.0 * b4, y56 = b5 - 2.0 * b6, xd = b3 + b4, yd = b5 + b6;
+    double o[9];
+    o[0] = b0 - 4.0 * b1 + 4.0 * b2;
+    o[1] = rA + x34 + b7; o[2] = rA + y56 - b7; o[3] = rA - x34 + b7; o[4] = rA - y56 - b7;
+    o[5] = rD + xd + yd + b8; o[6] = rD - xd + yd - b8; o[7] = rD - xd - yd + b8; o[8] = rD + xd - yd - b8;
+    const long long p = pidx(d, ie, je);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) d.gB[k * d.plane + p] = (float)(o[k] - weight(k));
+    if (d.write_fields && d.fo_rho) {
+        d.fo_rho[p] = e.r;
+        d.fo_u[p] = e.u;
+        d.fo_v[p] = e.v;
+    }
+}
+
+// One thread per border node: [left j=1..ny-2][right j=1..ny-2][top i][bottom i];
+// the corners of the top and bottom rows take the LODI state of the column
+// node inside them, as the reference's edge order left -> right -> top ->
+// bottom leaves it.
+__global__ void __launch_bounds__(64) fused_bc_kernel(DevState d) {
+    const int nl = d.ny - 2;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double fn[9];
+    if (t < 2 * nl) {
+        const int side = t < nl ? 0 : 1, j = 1 + (side == 0 ? t : t - nl);
+        const FarMom e = far_lodi(d, side, j, fn);
+        far_edge(d, side == 0 ? 0 : d.nx - 1, j, e, fn, far_moments(fn));
+        return;
+    }
+    t -= 2 * nl;
+    if (t < 2 * d.nx) {
+        const bool top = t < d.nx;
+        const int i = top ? t : t - d.nx;
+        const int je = top ? d.ny - 1 : 0, jn = top ? d.ny - 2 : 1;
+        FarMom nb;
+        if (i == 0 || i == d.nx - 1) {
+            double fc[9];
+            nb = far_lodi(d, i == 0 ? 0 : 1, jn, fc);
+            border_f0(d, i, jn, fn);   // the corner column node's own populations
+        } else {
+            pulled_f0(d, i, jn, fn);
+            nb = far_moments(fn);
+        }
+        far_edge(d, i, je, FarMom{nb.r, 0.0, 0.0}, fn, nb);
+    }
+}
+
+void launch_fused_bc(const DevState& d, cudaStream_t st) {
+    const int n = 2 * (d.ny - 2) + 2 * d.nx;
+    fused_bc_kernel<<<(n + 63) / 64, 64, 0, st>>>(d);
+}
+
 void launch_fused_band(const DevState& d, bool fields, cudaStream_t st) {
     const int n = d.band_cap;
     if (fields)

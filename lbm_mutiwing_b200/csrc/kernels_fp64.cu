@@ -4,8 +4,8 @@
 // padded row pitch.  Built with -fmad=false so every multiply and add rounds
 // separately, as in the reference's source order.
 //
-// Also the far-field boundary kernels of both paths, the convergence
-// residual, the lattice shift and the field export.
+// Also the plain path's far-field kernel, the convergence residual, the
+// lattice shift and the output fields of both paths.
 #include "bc.cuh"
 #include "lbm_kernels.h"
 
@@ -29,51 +29,6 @@ struct PlainAcc {
         d.rho[p] = m.r;
         d.u[p] = m.u;
         d.v[p] = m.v;
-    }
-};
-
-// Fused path: f0 is the pull of the previous post-collision planes (gA) for
-// interior nodes and the border store for border nodes.
-struct FusedAcc {
-    DevState d;
-    __device__ bool border(int i, int j) const {
-        return i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1;
-    }
-    __device__ double edge(int i, int j, int k) const {
-        const long long per = 2LL * d.ny + 2LL * d.nx;
-        long long e = (i == 0) ? j : (i == d.nx - 1) ? d.ny + j : (j == 0) ? 2LL * d.ny + i
-                                                                            : 2LL * d.ny + d.nx + i;
-        return d.edge_f0[k * per + e];
-    }
-    __device__ double f0(int i, int j, int k) const {
-        if (border(i, j)) return edge(i, j, k);
-        float g = d.gA[k * d.plane + pidx(d, i - ex(k), j - ey(k))];
-        return (double)g + weight(k);
-    }
-    __device__ Mom moments(int i, int j) const {
-        double trho = 0.0, tu = 0.0, tv = 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            double t = f0(i, j, k);
-            trho = trho + t;
-            tu = tu + (double)ex(k) * t;
-            tv = tv + (double)ey(k) * t;
-        }
-        // support boxes keep three nodes off the border, so no node the far
-        // field reads is an immersed-boundary band node
-        return Mom{trho, tu / trho, tv / trho};
-    }
-    __device__ void write_f(int i, int j, const double* f) const {
-        long long p = pidx(d, i, j);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) d.gB[k * d.plane + p] = (float)(f[k] - weight(k));
-    }
-    __device__ void write_fields(int i, int j, Mom m) const {
-        if (!d.write_fields || !d.fo_rho) return;
-        long long p = pidx(d, i, j);
-        d.fo_rho[p] = m.r;
-        d.fo_u[p] = m.u;
-        d.fo_v[p] = m.v;
     }
 };
 
@@ -252,7 +207,7 @@ void launch_outer_bc(const DevState& d, cudaStream_t st) {
     if (d.precision == 0)
         outer_bc_kernel<PlainAcc><<<(n + 127) / 128, 128, 0, st>>>(PlainAcc{d});
     else
-        outer_bc_kernel<FusedAcc><<<(n + 127) / 128, 128, 0, st>>>(FusedAcc{d});
+        launch_fused_bc(d, st);   // the fused path's own form (kernels_fp32.cu)
 }
 void launch_err(const DevState& d, double* partial, double* out, cudaStream_t st) {
     if (d.precision == 0)

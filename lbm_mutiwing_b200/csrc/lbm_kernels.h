@@ -25,6 +25,7 @@ FusedConsts fused_consts(const DevState& d);
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st);
 bool is_bulk_kernel(const void* func);   // the bulk kernel (low priority in graphs)
 void launch_fused_band(const DevState& d, bool fields, cudaStream_t st);
+void launch_fused_bc(const DevState& d, cudaStream_t st);   // far field of the fused path
 void launch_fused_init(const DevState& d, cudaStream_t st);
 void launch_fused_shift(const DevState& d, int dr, cudaStream_t st);
 void launch_fused_export(const DevState& d, const float* g, double* f, cudaStream_t st);
