@@ -8,7 +8,7 @@
  * in module globals and calls `evolution` once per lattice step.  Each entry
  * point below replaces one reference routine; the citation names it
  * (file:line in the reference project).  A Fortran host binds these with an
- * ISO_C_BINDING interface block.
+ * ISO_C_BINDING interface block, the way zmq_comm.f90:23-81 binds libzmq.
  *
  * Conventions
  *  - Status: 0 on success, negative on error; lbm_last_error() gives the text
@@ -49,6 +49,7 @@ extern "C" {
 #define LBM_STEP_ERR 2         /* last two steps keep u, u0 so lbm_err is available */
 
 typedef struct LbmHandle LbmHandle;
+typedef struct LbmBatch LbmBatch;
 
 /* Runtime form of the reference's compile-time parameters
  * (main.f90:7-152, ini_mesh.f90:15-67). */
@@ -193,6 +194,24 @@ int64_t lbm_device_bytes(const LbmHandle* h);
 
 const char* lbm_last_error(const LbmHandle* h);
 void lbm_destroy(LbmHandle* h);
+
+/* Packed stepping of many resident episodes (the batched form of the
+ * reference's per-episode evolution loop, driver.f90:322-363 once per
+ * client): lbm_batch_step advances handle hs[i] by n_steps[i] steps from
+ * first_cycle[i] exactly as lbm_step(hs[i], first_cycle[i], n_steps[i],
+ * force_rows[i], flags[i]) would, bit for bit, but every kernel of a step is
+ * one launch over all episodes still stepping.  FP32-path handles on the
+ * batch's device only; each handle at most once; force_rows[i] may be NULL
+ * (or force_rows itself), flags NULL means 0.  rcs (may be NULL) receives
+ * each handle's status (nonzero: its lbm_last_error text); the call returns
+ * 0, or -1 with lbm_batch_last_error naming the first failing episode.  The
+ * handles' phase timers are not updated.  A batch object serves one call at
+ * a time; handles must not be used by other threads during the call. */
+int lbm_batch_create(int32_t device, LbmBatch** out);
+int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* first_cycle,
+                   const int64_t* n_steps, double* const* force_rows, const int32_t* flags, int32_t* rcs);
+const char* lbm_batch_last_error(const LbmBatch* b);
+void lbm_batch_destroy(LbmBatch* b);
 int lbm_abi_version(void);
 
 #ifdef __cplusplus

@@ -75,6 +75,11 @@ SIGNATURES = [
     ("lbm_device_bytes", C.c_int64, [C.c_void_p]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_destroy", None, [C.c_void_p]),
+    ("lbm_batch_create", C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    ("lbm_batch_step", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int64), C.POINTER(D), I32, I32]),
+    ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("lbm_batch_destroy", None, [C.c_void_p]),
 ]
 
 _lib = None
@@ -291,6 +296,77 @@ class Simulation:
 
     def device_bytes(self) -> int:
         return int(self.L.lbm_device_bytes(self.h))
+
+
+class BatchStepError(LbmError):
+    """Raised by Batch.step when episodes failed; rcs[i] != 0 marks them and
+    messages[i] holds each failed episode's error text."""
+
+    def __init__(self, msg, rcs, messages):
+        super().__init__(msg)
+        self.rcs = rcs
+        self.messages = messages
+
+
+class Batch:
+    """Packed stepping of many FP32-path episodes on one device
+    (lbm_batch_step): each step is one launch per kernel over every episode
+    still stepping, with results identical to stepping each episode alone."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        h = C.c_void_p()
+        rc = self.L.lbm_batch_create(device, C.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.L.lbm_batch_last_error(h).decode() if h.value else "lbm_batch_create failed"
+            if h.value:
+                self.L.lbm_batch_destroy(h)
+            self.h = None
+            raise LbmError(msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lbm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def step(self, sims: Sequence["Simulation"], n_steps, first_cycles=None, rows: bool = True, flags=0):
+        """Advance sims[i] by n_steps[i] (an int applies to all) from
+        first_cycles[i] (default: each simulation's next cycle); returns the
+        force rows of each (None where rows is False)."""
+        n = len(sims)
+        if n == 0:
+            return []
+        ns = [int(n_steps)] * n if np.isscalar(n_steps) else [int(x) for x in n_steps]
+        fl = [int(flags)] * n if np.isscalar(flags) else [int(x) for x in flags]
+        first = [s.cycle for s in sims] if first_cycles is None else [int(x) for x in first_cycles]
+        outs = [np.zeros((k, s.row_len)) if rows and k else None for s, k in zip(sims, ns)]
+        hs = (C.c_void_p * n)(*[s.h.value for s in sims])
+        fc = (C.c_int64 * n)(*first)
+        nn = (C.c_int64 * n)(*ns)
+        rp = (D * n)(*[_dp(o) if o is not None else D() for o in outs])
+        ff = (C.c_int32 * n)(*fl)
+        rcs = (C.c_int32 * n)()
+        rc = self.L.lbm_batch_step(self.h, n, hs, fc, nn, rp, ff, rcs)
+        if rc != 0:
+            codes = list(rcs)
+            msgs = [sims[i].L.lbm_last_error(sims[i].h).decode() if codes[i] else "" for i in range(n)]
+            raise BatchStepError(self.L.lbm_batch_last_error(self.h).decode(), codes, msgs)
+        for s, f0, k in zip(sims, first, ns):
+            s.cycle = f0 + k
+        return outs
 
 
 def finalize_force_average(sum_row: np.ndarray, count: int, row_len: int, wing_count: int,

@@ -46,6 +46,7 @@
 #include <cstdio>
 
 #include "lbm_kernels.h"
+#include "multi.cuh"
 
 namespace lbm {
 
@@ -159,8 +160,8 @@ __device__ inline void marker(const DevState& d, const WingMotion& m, int w, int
 // of the previous band (airfoil.f90:276-284).  Twelve threads per segment:
 // thread (s, axis, k) scans its axis for the box and evaluates the kernel at
 // the box's k-th node column or row.
-__global__ void ibm_geometry_kernel(DevState d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_geometry_kernel_body(const DevState& d, const int bid_) {
+    const int t = bid_ * blockDim.x + threadIdx.x;
     if (t < d.wing_count) d.wm[t] = wing_motion(d, t);
     if (t < d.npts) {
         const int w = wing_of_point(d, t);
@@ -208,23 +209,33 @@ __global__ void ibm_geometry_kernel(DevState d) {
     }
     if (t == 0 && d.wing_count > 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
 }
+__global__ void ibm_geometry_kernel(DevState d) { ibm_geometry_kernel_body(d, blockIdx.x); }
+__global__ void ibm_geometry_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_geometry_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 __device__ inline bool box_empty(const DevState& d, int s) {
     return d.box[4 * s + 1] < d.box[4 * s] || d.box[4 * s + 3] < d.box[4 * s + 2];
 }
 
 // claims: lowest segment index wins (airfoil.f90:322-333)
-__global__ void ibm_claim_kernel(DevState d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_claim_kernel_body(const DevState& d, const int bid_) {
+    const int t = bid_ * blockDim.x + threadIdx.x;
     if (t >= d.nseg * BOX_SLOTS) return;
     const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
     if (box_empty(d, s)) return;
     const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
     if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
 }
+__global__ void ibm_claim_kernel(DevState d) { ibm_claim_kernel_body(d, blockIdx.x); }
+__global__ void ibm_claim_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_claim_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
-__global__ void ibm_count_kernel(DevState d) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const int bid_) {
+    const int s = bid_ * blockDim.x + threadIdx.x;
     if (s >= d.nseg) return;
     int c = 0;
     if (!box_empty(d, s))
@@ -232,10 +243,15 @@ __global__ void ibm_count_kernel(DevState d) {
             for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) c += (d.band_map[pidx(d, i - 1, j - 1)] == s);
     d.claim_cnt[s] = c;
 }
+__global__ void ibm_count_kernel(DevState d) { ibm_count_kernel_body(d, blockIdx.x); }
+__global__ void ibm_count_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_count_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // Exclusive scan of the claim counts (one block), band size, and the check
 // whether two wings' supports overlap (coupled solve).
-__global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) {
+__device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const int bid_) {
     __shared__ int wsum[32];
     __shared__ int wbox[MAX_WINGS][4];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -283,12 +299,17 @@ __global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) {
         if (coupled) set_status(d, ST_WINGS_COUPLED);
     }
 }
+__global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) { ibm_scan_kernel_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(1024) ibm_scan_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_scan_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // Band list in the reference's order (segment, then i, then j) and the
 // band_map encoding -(b + 2); a node still holding its claimer's index is
 // never confused with another segment's index, so encoding as we go is safe.
-__global__ void ibm_list_kernel(DevState d) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_list_kernel_body(const DevState& d, const int bid_) {
+    const int s = bid_ * blockDim.x + threadIdx.x;
     if (s >= d.nseg || box_empty(d, s)) return;
     const int nb = d.band_n[0];
     const int w = d.seg_wing[s];
@@ -307,14 +328,19 @@ __global__ void ibm_list_kernel(DevState d) {
             ++b;
         }
 }
+__global__ void ibm_list_kernel(DevState d) { ibm_list_kernel_body(d, blockIdx.x); }
+__global__ void ibm_list_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_list_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // u*, rho at band nodes (solution.f90:510-554): the moment fields of the
 // plain path, or the moments of the pulled distributions of the fused path
 // (band nodes are interior nodes: boxes keep off the border).  Also zeroes
 // the spread accumulators.
 template <bool FUSED>
-__global__ void ibm_ustar_kernel(DevState d) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_ustar_kernel_body(const DevState& d, const int bid_) {
+    const int b = bid_ * blockDim.x + threadIdx.x;
     if (b >= d.band_n[0]) return;
     const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
     const long long p = pidx(d, i, j);
@@ -340,12 +366,19 @@ __global__ void ibm_ustar_kernel(DevState d) {
     d.band_us[b] = tu / trho;
     d.band_vs[b] = tv / trho;
 }
+template <bool FUSED>
+__global__ void ibm_ustar_kernel(DevState d) { ibm_ustar_kernel_body<FUSED>(d, blockIdx.x); }
+template <bool FUSED>
+__global__ void ibm_ustar_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_ustar_kernel_body<FUSED>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // r = ub - X u* (boundary_condition.f90:1540-1555, 1609-1629) and the band
 // index of each (segment, slot); one warp per segment, slots 0..35 over the
 // lanes, summed by a fixed butterfly.
-__global__ void ibm_rhs_kernel(DevState d) {
-    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__device__ __forceinline__ void ibm_rhs_kernel_body(const DevState& d, const int bid_) {
+    const int s = (bid_ * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (s >= d.nseg) return;
     const int nb = d.band_n[0];
@@ -388,6 +421,11 @@ __global__ void ibm_rhs_kernel(DevState d) {
         d.qy[s] = vb - bv;
     }
 }
+__global__ void ibm_rhs_kernel(DevState d) { ibm_rhs_kernel_body(d, blockIdx.x); }
+__global__ void ibm_rhs_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_rhs_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // G(a, c) = Sx(a, c) Sy(a, c), the delta kernel being separable.
 __device__ inline double gram(const DevState& d, int a, int c) {
@@ -402,8 +440,9 @@ __device__ inline double gram(const DevState& d, int a, int c) {
 // Banded G per wing in RCM order (layout of ibm_wing_storage): row p of
 // wing w starts at lband[lofs_w + (p + 1) * ld]; entry dd holds G(p, p - dd).
 // Every slot of the storage is written, zero zones included.
-__global__ void ibm_assemble_kernel(DevState d, long long total) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_assemble_kernel_body(const DevState& d, const int bid_) {
+    const long long total = d.lband_total;
+    const long long t = bid_ * (long long)blockDim.x + threadIdx.x;
     if (t >= total) return;
     int w = 0;
     while (w + 1 < d.wing_count && t >= d.wing_lofs[w + 1]) ++w;
@@ -411,6 +450,11 @@ __global__ void ibm_assemble_kernel(DevState d, long long total) {
     const long long r = t - d.wing_lofs[w];
     const int p = (int)(r / ld) - 1, dd = (int)(r % ld), q = p - dd;
     d.lband[t] = (p >= 0 && p < nw && q >= 0 && dd <= bw) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
+}
+__global__ void ibm_assemble_kernel(DevState d) { ibm_assemble_kernel_body(d, blockIdx.x); }
+__global__ void ibm_assemble_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_assemble_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
 // Fixed-point exponent shared by the spread and the finish kernels: every
@@ -426,8 +470,8 @@ __device__ inline int spread_exponent(const DevState& d) {
 
 // du = X^T y: every (segment, slot) contribution is rounded once to a 64-bit
 // fixed-point number and added with an integer atomic.
-__global__ void ibm_spread_kernel(DevState d) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_spread_kernel_body(const DevState& d, const int bid_) {
+    const int t = bid_ * blockDim.x + threadIdx.x;
     if (t >= d.nseg * BOX_SLOTS) return;
     const int bi = d.pb[t];
     if (bi < 0) return;
@@ -439,18 +483,23 @@ __global__ void ibm_spread_kernel(DevState d) {
     atomicAdd(reinterpret_cast<unsigned long long*>(d.band_dv) + bi,
               (unsigned long long)__double2ll_rn(ldexp(wv * d.ry[s], e)));
 }
+__global__ void ibm_spread_kernel(DevState d) { ibm_spread_kernel_body(d, blockIdx.x); }
+__global__ void ibm_spread_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_spread_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // du back to FP64, velocity correction and body force (plain path fields),
 // and per-block partial sums of each wing's force and moment over the
 // block's contiguous slice of the band list (each wing owns a contiguous
 // range: claim order).
 template <bool FUSED>
-__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) {
+__device__ __forceinline__ void ibm_finish_kernel_body(const DevState& d, const int bid_) {
     constexpr int NWARP = FINISH_THREADS / 32;
     __shared__ double red[NWARP][3];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = d.band_n[0];
-    const int b = blockIdx.x * FINISH_THREADS + tid;
+    const int b = bid_ * FINISH_THREADS + tid;
     const int e = spread_exponent(d);
     double t1 = 0.0, t2 = 0.0;
     int myw = -1;
@@ -478,11 +527,11 @@ __global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) 
         x0 = (d.ox + d.scale * (double)i - xw) / d.scale - m.extra_pos;
         y0 = (d.oy + d.scale * (double)j - yw) / d.scale;
     }
-    const int b0 = blockIdx.x * FINISH_THREADS;
+    const int b0 = bid_ * FINISH_THREADS;
     const int b1 = min(nb, b0 + FINISH_THREADS) - 1;
     const int wlo = b0 < nb ? d.band_wing[b0] : 0, whi = b0 < nb ? d.band_wing[b1] : -1;
     for (int w = 0; w < d.wing_count; ++w) {
-        double* out = d.force_part + ((long long)blockIdx.x * d.wing_count + w) * 3;
+        double* out = d.force_part + ((long long)bid_ * d.wing_count + w) * 3;
         if (w < wlo || w > whi) {
             if (tid < 3) out[tid] = 0.0;
             continue;
@@ -508,10 +557,18 @@ __global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) 
         __syncthreads();
     }
 }
+template <bool FUSED>
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) { ibm_finish_kernel_body<FUSED>(d, blockIdx.x); }
+template <bool FUSED>
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_finish_kernel_body<FUSED>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // Per-wing force and moment from the block partials (in block order), the
 // no-slip residual when diagnostics are on, and the force row.
-__global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks) {
+__device__ __forceinline__ void ibm_forces_kernel_body(const DevState& d, const int bid_) {
+    const int nblocks = (int)max(1LL, ((long long)d.band_cap + FINISH_THREADS - 1) / FINISH_THREADS);
     constexpr int CHUNK = 64;   // block partials staged per pass
     __shared__ double fm[MAX_WINGS][3];
     __shared__ double red[8][2];
@@ -596,12 +653,22 @@ __global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d, int nblocks
         d.sum_row[c] = d.sum_row[c] + rowv[c];
     }
 }
+__global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d) { ibm_forces_kernel_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(256) ibm_forces_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_forces_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
-__global__ void step_advance_kernel(DevState d) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
+__device__ __forceinline__ void step_advance_kernel_body(const DevState& d, const int bid_) {
+    if (threadIdx.x == 0 && bid_ == 0) {
         *d.cycle += 1;
         *d.row_index += 1;
     }
+}
+__global__ void step_advance_kernel(DevState d) { step_advance_kernel_body(d, blockIdx.x); }
+__global__ void step_advance_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    step_advance_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
 // ------------------------------------------------------------ host side
@@ -621,7 +688,7 @@ void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_do
 
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
     const long long total = d.lband_total;
-    ibm_assemble_kernel<<<blocks(total, 256), 256, 0, st>>>(d, total);
+    ibm_assemble_kernel<<<blocks(total, 256), 256, 0, st>>>(d);
     launch_ibm_factor_blocks(d, factor_smem, st);
 }
 
@@ -641,9 +708,48 @@ void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st) {
         ibm_finish_kernel<true><<<nbk, FINISH_THREADS, 0, st>>>(d);
     else
         ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
-    ibm_forces_kernel<<<1, 256, 0, st>>>(d, nbk);
+    ibm_forces_kernel<<<1, 256, 0, st>>>(d);
 }
 
 void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kernel<<<1, 32, 0, st>>>(d); }
+
+// ------------------------------------------------------------ packed launches
+// (fused path: u* from the pulled distributions, velocity correction of the
+// band re-collision)
+int multi_blocks_ibm(MultiKernel k, const DevState& d) {
+    switch (k) {
+    case MK_GEOMETRY: return blocks(std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap), 128);
+    case MK_CLAIM: return blocks((long long)d.nseg * BOX_SLOTS, 256);
+    case MK_COUNT: return blocks(d.nseg, 64);
+    case MK_SCAN: return 1;
+    case MK_LIST: return blocks(d.nseg, 64);
+    case MK_ASSEMBLE: return blocks(d.lband_total, 256);
+    case MK_USTAR: return blocks(d.band_cap, 128);
+    case MK_RHS: return blocks(32LL * d.nseg, 128);
+    case MK_SPREAD: return blocks((long long)d.nseg * BOX_SLOTS, 256);
+    case MK_FINISH: return ibm_finish_blocks(d);
+    case MK_FORCES: return 1;
+    case MK_ADVANCE: return 1;
+    default: return -1;
+    }
+}
+
+bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st) {
+    switch (k) {
+    case MK_GEOMETRY: ibm_geometry_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
+    case MK_CLAIM: ibm_claim_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_COUNT: ibm_count_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
+    case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
+    case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
+    case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_USTAR: ibm_ustar_kernel_multi<true><<<nb, 128, 0, st>>>(m); return true;
+    case MK_RHS: ibm_rhs_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
+    case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_FINISH: ibm_finish_kernel_multi<true><<<nb, FINISH_THREADS, 0, st>>>(m); return true;
+    case MK_FORCES: ibm_forces_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_ADVANCE: step_advance_kernel_multi<<<nb, 32, 0, st>>>(m); return true;
+    default: return false;
+    }
+}
 
 }  // namespace lbm

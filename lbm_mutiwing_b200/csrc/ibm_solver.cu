@@ -25,6 +25,7 @@
 
 #include "bulk_copy.cuh"
 #include "lbm_kernels.h"
+#include "multi.cuh"
 
 namespace lbm {
 
@@ -110,9 +111,9 @@ __device__ inline bool factor_diagonal_block(const double* A, int ld, int k0, in
 // than the lattice).  SMEM: the storage is worked on in shared memory (the
 // template parameter lets every access compile to a shared-memory access).
 template <bool SMEM>
-__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) {
+__device__ __forceinline__ void ibm_factor_kernel_body(const DevState& d, const int bid_) {
     extern __shared__ __align__(16) double smem[];
-    const int w = blockIdx.x;
+    const int w = bid_;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
     const int bwr = (d.bw_max + TILE - 1) / TILE * TILE;
@@ -284,6 +285,13 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) 
         if (tid == 0) bulk_store_all(gS, S, wsize * 8);
     }
 }
+template <bool SMEM>
+__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) { ibm_factor_kernel_body<SMEM>(d, blockIdx.x); }
+template <bool SMEM>
+__global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_factor_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 // Forward and backward substitution with the factor of wing w: warp 0 solves
 // for the x component, warp 1 for the y component, on shared-memory copies
@@ -293,10 +301,10 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel(DevState d) 
 // updates rows lane and lane + 32 below or above a panel (bw <= 64) or loops.
 // SMEM: the factor is copied to shared memory.
 template <bool SMEM>
-__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
+__device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const int bid_) {
     extern __shared__ __align__(16) double sm[];
     __shared__ uint64_t bar;
-    const int w = blockIdx.x;
+    const int w = bid_;
     const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
     const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
     const int npan = (nw + PANEL - 1) / PANEL;
@@ -426,6 +434,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
     for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
     if (lane == 0) d.ymax[2 * w + comp] = ym;
 }
+template <bool SMEM>
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) { ibm_solve_kernel_body<SMEM>(d, blockIdx.x); }
+template <bool SMEM>
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_solve_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 size_t ibm_factor_staging_bytes(int bw_max) {
     const int nt = round_tile(bw_max) / TILE;
@@ -468,6 +483,10 @@ cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel<false>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<false>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<false>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<false>, optin);
     if (e == cudaSuccess && dev < 64) g_prepared_devices |= 1ULL << dev;
     return e;
 }
@@ -486,6 +505,29 @@ void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t 
         ibm_solve_kernel<true><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
     else
         ibm_solve_kernel<false><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+}
+
+// Packed launches: one block per wing of every episode; episodes whose
+// factor (or substitution) does not take the kind's shared-memory form get
+// no blocks in it.  The dynamic shared memory is the largest of the batch.
+int multi_blocks_solver(MultiKernel k, const DevState& d) {
+    switch (k) {
+    case MK_FACTOR_SMEM: return d.factor_in_smem ? d.wing_count : 0;
+    case MK_FACTOR_GLOBAL: return d.factor_in_smem ? 0 : d.wing_count;
+    case MK_SOLVE_SMEM: return d.solve_in_smem ? d.wing_count : 0;
+    case MK_SOLVE_GLOBAL: return d.solve_in_smem ? 0 : d.wing_count;
+    default: return -1;
+    }
+}
+
+bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int nb, size_t smem, cudaStream_t st) {
+    switch (k) {
+    case MK_FACTOR_SMEM: ibm_factor_kernel_multi<true><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
+    case MK_FACTOR_GLOBAL: ibm_factor_kernel_multi<false><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
+    case MK_SOLVE_SMEM: ibm_solve_kernel_multi<true><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
+    case MK_SOLVE_GLOBAL: ibm_solve_kernel_multi<false><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
+    default: return false;
+    }
 }
 
 }  // namespace lbm

@@ -17,6 +17,7 @@
 // Band nodes are re-collided afterwards in FP64 by fused_band_kernel with the
 // corrected velocity and the Guo forcing term.
 #include "lbm_kernels.h"
+#include "multi.cuh"
 
 namespace lbm {
 
@@ -38,13 +39,14 @@ FusedConsts fused_consts(const DevState& d) {
 }
 
 template <bool FIELDS>
-__global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __restrict__ gA, float* __restrict__ gB,
-                                                             int nx, int ny, int pitch, long long plane,
-                                                             FusedConsts c, double* __restrict__ fo_rho,
-                                                             double* __restrict__ fo_u, double* __restrict__ fo_v) {
-    const int i = blockIdx.x * BULK_TX + threadIdx.x + 1;
+__device__ __forceinline__ void fused_bulk_body(const float* __restrict__ gA, float* __restrict__ gB,
+                                                int nx, int ny, int pitch, long long plane,
+                                                const FusedConsts& c, double* __restrict__ fo_rho,
+                                                double* __restrict__ fo_u, double* __restrict__ fo_v,
+                                                int bx, int by) {
+    const int i = bx * BULK_TX + threadIdx.x + 1;
     if (i > nx - 2) return;
-    const int j0 = blockIdx.y * BULK_ROWS + 1;
+    const int j0 = by * BULK_ROWS + 1;
 #pragma unroll
     for (int r = 0; r < BULK_ROWS; ++r) {
         const int j = j0 + r;
@@ -106,12 +108,31 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
         }
     }
 }
+template <bool FIELDS>
+__global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __restrict__ gA, float* __restrict__ gB,
+                                                             int nx, int ny, int pitch, long long plane,
+                                                             FusedConsts c, double* __restrict__ fo_rho,
+                                                             double* __restrict__ fo_u, double* __restrict__ fo_v) {
+    fused_bulk_body<FIELDS>(gA, gB, nx, ny, pitch, plane, c, fo_rho, fo_u, fo_v, blockIdx.x, blockIdx.y);
+}
+// Packed form: an episode's blocks are its x chunks row by row.
+__global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    const DevState& d = *m.ds[e];
+    const int l = blockIdx.x - __ldg(m.boff + e);
+    const int nbx = (d.nx - 2 + BULK_TX - 1) / BULK_TX;
+    const FusedConsts c = d.fc;
+    if (d.write_fields && d.fo_rho)
+        fused_bulk_body<true>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, d.fo_rho, d.fo_u, d.fo_v, l % nbx, l / nbx);
+    else
+        fused_bulk_body<false>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr, l % nbx, l / nbx);
+}
 
 // Band nodes: FP64 re-collision with the corrected velocity u* + du and the
 // body force 2 rho du (solution.f90:599-655 with boundary_condition.f90:1645-1659).
 template <bool FIELDS>
-__global__ void fused_band_kernel(DevState d) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void fused_band_kernel_body(const DevState& d, const int bid_) {
+    const int b = bid_ * blockDim.x + threadIdx.x;
     if (b >= d.band_n[0]) return;
     const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
     if (i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1) return;
@@ -162,6 +183,16 @@ __global__ void fused_band_kernel(DevState d) {
         d.fo_u[p] = ut;
         d.fo_v[p] = vt;
     }
+}
+template <bool FIELDS>
+__global__ void fused_band_kernel(DevState d) { fused_band_kernel_body<FIELDS>(d, blockIdx.x); }
+__global__ void fused_band_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    const DevState& d = *m.ds[e];
+    if (d.write_fields)
+        fused_band_kernel_body<true>(d, blockIdx.x - __ldg(m.boff + e));
+    else
+        fused_band_kernel_body<false>(d, blockIdx.x - __ldg(m.boff + e));
 }
 
 // Initial state (solution.f90:44-61): f = f0 = feq(1, UU, 0) on every node,
@@ -358,9 +389,9 @@ __device__ void far_edge(const DevState& d, int ie, int je, const FarMom& e, con
 // the corners of the top and bottom rows take the LODI state of the column
 // node inside them, as the reference's edge order left -> right -> top ->
 // bottom leaves it.
-__global__ void __launch_bounds__(64) fused_bc_kernel(DevState d) {
+__device__ __forceinline__ void fused_bc_kernel_body(const DevState& d, const int bid_) {
     const int nl = d.ny - 2;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int t = bid_ * blockDim.x + threadIdx.x;
     double fn[9];
     if (t < 2 * nl) {
         const int side = t < nl ? 0 : 1, j = 1 + (side == 0 ? t : t - nl);
@@ -385,6 +416,11 @@ __global__ void __launch_bounds__(64) fused_bc_kernel(DevState d) {
         far_edge(d, i, je, FarMom{nb.r, 0.0, 0.0}, fn, nb);
     }
 }
+__global__ void __launch_bounds__(64) fused_bc_kernel(DevState d) { fused_bc_kernel_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(64) fused_bc_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    fused_bc_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
 
 void launch_fused_bc(const DevState& d, cudaStream_t st) {
     const int n = 2 * (d.ny - 2) + 2 * d.nx;
@@ -406,5 +442,26 @@ void launch_fused_export(const DevState& d, const float* g, double* f, cudaStrea
 void launch_fused_import(const DevState& d, const double* f, float* g, cudaStream_t st) {
     fused_import_kernel<<<1184, 256, 0, st>>>(d, f, g);
 }
+
+// ------------------------------------------------------------ packed launches
+int multi_blocks_fused(MultiKernel k, const DevState& d) {
+    switch (k) {
+    case MK_BULK: return ((d.nx - 2 + BULK_TX - 1) / BULK_TX) * ((d.ny - 2 + BULK_ROWS - 1) / BULK_ROWS);
+    case MK_BAND: return (d.band_cap + 127) / 128;
+    case MK_BC: return (2 * (d.ny - 2) + 2 * d.nx + 63) / 64;
+    default: return -1;
+    }
+}
+
+bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st) {
+    switch (k) {
+    case MK_BULK: fused_bulk_kernel_multi<<<blocks, BULK_TX, 0, st>>>(m); return true;
+    case MK_BAND: fused_band_kernel_multi<<<blocks, 128, 0, st>>>(m); return true;
+    case MK_BC: fused_bc_kernel_multi<<<blocks, 64, 0, st>>>(m); return true;
+    default: return false;
+    }
+}
+
+bool is_bulk_multi_kernel(const void* func) { return func == reinterpret_cast<const void*>(fused_bulk_kernel_multi); }
 
 }  // namespace lbm

@@ -195,6 +195,23 @@ struct LbmHandle {
     size_t out_cap = 0;   // by starting plane parity and geometry set
 };
 
+// Packed stepping of many fused-path handles (lbm_batch_step): one launch per
+// kernel of a step covers every episode of the batch.  The streams mirror a
+// handle's: bulk (low priority), and main, immersed boundary, far field and
+// the two geometry streams (high priority).
+struct LbmBatch {
+    int device = 0;
+    std::string err;
+    cudaStream_t s_main = nullptr, s_bulk = nullptr, s_ibm = nullptr, s_bc = nullptr, s_aux = nullptr,
+                 s_aux2 = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_bulk = nullptr, ev_ibm = nullptr, ev_bc = nullptr, ev_geom = nullptr,
+                ev_list = nullptr, ev_fact = nullptr;
+    char* d_buf = nullptr;          // device tables: episode states, block offsets, state pointers
+    size_t d_cap = 0;
+    char* h_buf = nullptr;          // pinned staging of the tables
+    size_t h_cap = 0;
+};
+
 namespace {
 
 // Graph capture and device-wide operations of different handles must not
@@ -612,6 +629,60 @@ int build_graph(LbmHandle* h, int p, int gs) {
     return 0;
 }
 
+int batch_fail(LbmBatch* b, const std::string& msg) {
+    if (b) b->err = msg;
+    return -1;
+}
+
+#define BCK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return batch_fail(b, std::string("CUDA error in ") + #call + ": " +  \
+                                                         cudaGetErrorString(e_));                    \
+    } while (0)
+
+int multi_blocks(MultiKernel k, const DevState& d) {
+    int n = multi_blocks_ibm(k, d);
+    if (n < 0) n = multi_blocks_solver(k, d);
+    if (n < 0) n = multi_blocks_fused(k, d);
+    return std::max(n, 0);
+}
+
+// Per handle of a batch, eight states: the plain step, the second-last and
+// the last step of the call (the field and diagnostic flags of lbm_step),
+// and the geometry built one step ahead, each for the two plane parities /
+// geometry sets a step can start from.
+constexpr int BV_PLAIN = 0, BV_SECOND_LAST = 2, BV_LAST = 4, BV_AHEAD = 6, BV_COUNT = 8;
+
+void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out) {
+    for (int ph = 0; ph < 2; ++ph) {
+        DevState d = h->d;
+        const int p = h->parity ^ ph, g = (h->gset + ph) % GEO_SETS;
+        d.gA = h->planes[p];
+        d.gB = h->planes[1 - p];
+        use_geo(d, h->geo[g]);
+        d.cycle_ahead = 0;
+        d.diag = 0;
+        d.write_fields = 0;
+        out[BV_PLAIN + ph] = d;
+        DevState sl = d;
+        sl.write_fields = want_err ? 1 : 0;
+        out[BV_SECOND_LAST + ph] = sl;
+        DevState l = d;
+        l.write_fields = (want_fields || want_err) ? 1 : 0;
+        l.diag = 1;
+        if (want_err) {   // the previous step's velocity becomes u0
+            std::swap(l.fo_u, l.fo_u0);
+            std::swap(l.fo_v, l.fo_v0);
+        }
+        out[BV_LAST + ph] = l;
+        DevState a = d;
+        use_geo(a, h->geo[(g + GEO_AHEAD) % GEO_SETS]);
+        a.cycle_ahead = GEO_AHEAD;
+        out[BV_AHEAD + ph] = a;
+    }
+}
+
 int copy_pitched_out(LbmHandle* h, const double* src, double* dst) {
     const DevState& d = h->d;
     CK(cudaMemcpy2D(dst, sizeof(double) * d.nx, src, sizeof(double) * d.pitch, sizeof(double) * d.nx, d.ny,
@@ -847,7 +918,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
     h->pinned_n = 4096;
-    if (c.precision != LBM_PRECISION_FP64) h->fc = fused_consts(d);
+    if (c.precision != LBM_PRECISION_FP64) h->fc = h->d.fc = fused_consts(d);
     if (init_state(h)) return -1;
     return 0;
 }
@@ -982,6 +1053,250 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
         h->err_valid = h->d.precision == 0 ? true : (want_err && n_steps >= 2);
     }
     return check_status(h);
+}
+
+int lbm_batch_create(int32_t device, LbmBatch** out) {
+    DeviceLock lock(g_device_mutex);
+    if (!out) return -1;
+    LbmBatch* b = new LbmBatch();
+    *out = b;
+    b->device = device;
+    BCK(cudaSetDevice(device));
+    int lo = 0, hi = 0;
+    BCK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    BCK(cudaStreamCreateWithPriority(&b->s_bulk, cudaStreamNonBlocking, lo));
+    for (cudaStream_t* st : {&b->s_main, &b->s_ibm, &b->s_bc, &b->s_aux, &b->s_aux2})
+        BCK(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi));
+    for (cudaEvent_t* e : {&b->ev_start, &b->ev_bulk, &b->ev_ibm, &b->ev_bc, &b->ev_geom, &b->ev_list, &b->ev_fact})
+        BCK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return 0;
+}
+
+const char* lbm_batch_last_error(const LbmBatch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* first_cycle,
+                   const int64_t* n_steps, double* const* force_rows, const int32_t* flags, int32_t* rcs) {
+    if (!b) return -1;
+    if (n < 0 || (n > 0 && (!hs || !first_cycle || !n_steps))) return batch_fail(b, "bad arguments");
+    if (rcs)
+        for (int i = 0; i < n; ++i) rcs[i] = 0;
+    if (n == 0) return 0;
+    for (int i = 0; i < n; ++i) {
+        LbmHandle* h = hs[i];
+        const std::string who = "episode " + std::to_string(i) + ": ";
+        if (!h) return batch_fail(b, who + "null handle");
+        if (h->d.precision == 0) return batch_fail(b, who + "batched steps need the FP32 path");
+        if (h->cfg.device != b->device) return batch_fail(b, who + "handle on another device");
+        if (n_steps[i] < 0) return batch_fail(b, who + "n_steps must be >= 0");
+        if (n_steps[i] > (int64_t)1 << 30) return batch_fail(b, who + "n_steps too large");
+        if (first_cycle[i] < 1) return batch_fail(b, who + "cycles start at 1");
+        if (h->d.motion_source == LBM_MOTION_FILE && h->d.step_rows <= 0 && h->cfg.wing_count > 0)
+            return batch_fail(b, who + "no motion table loaded");
+        for (int j = 0; j < i; ++j)
+            if (hs[j] == h) return batch_fail(b, who + "handle given twice");
+    }
+    BCK(cudaSetDevice(b->device));
+    const int nh = n;
+    std::vector<DevState> var((size_t)nh * BV_COUNT);
+    for (int i = 0; i < nh; ++i) {
+        LbmHandle* h = hs[i];
+        const int32_t fl = flags ? flags[i] : 0;
+        const bool want_fields = (fl & LBM_STEP_FIELDS) != 0, want_err = (fl & LBM_STEP_ERR) != 0;
+        if (ensure_rows(h, n_steps[i])) return batch_fail(b, "episode " + std::to_string(i) + ": " + h->err);
+        if ((want_fields || want_err) && n_steps[i] > 0 && !h->d.fo_rho) {
+            const size_t N = (size_t)h->d.plane;
+            if (dalloc(h, &h->d.fo_rho, N) || dalloc(h, &h->d.fo_u, N) || dalloc(h, &h->d.fo_v, N) ||
+                dalloc(h, &h->d.fo_u0, N) || dalloc(h, &h->d.fo_v0, N))
+                return batch_fail(b, "episode " + std::to_string(i) + ": " + h->err);
+        }
+        // the batch's streams start after the handle's own work
+        BCK(cudaStreamSynchronize(h->s_main));
+        batch_variants(h, want_fields, want_err, &var[(size_t)i * BV_COUNT]);
+    }
+    // episodes by decreasing step count: the episodes still stepping at any
+    // step are a prefix of this order
+    std::vector<int> order(nh);
+    for (int i = 0; i < nh; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n_steps[x] > n_steps[y]; });
+    const int64_t K = n_steps[order[0]];
+    auto active = [&](int64_t k) {   // episodes stepping at step k
+        int a = 0;
+        while (a < nh && n_steps[order[a]] > k) ++a;
+        return a;
+    };
+    // block offsets of every packed kernel, in episode order
+    std::vector<int> boff((size_t)MK_KINDS * (nh + 1), 0);
+    size_t factor_smem = 0, solve_smem = 0;
+    for (int k = 0; k < MK_KINDS; ++k)
+        for (int e = 0; e < nh; ++e) {
+            const long long nb = (long long)boff[(size_t)k * (nh + 1) + e] + multi_blocks((MultiKernel)k, hs[order[e]]->d);
+            if (nb > INT32_MAX) return batch_fail(b, "batch too large for one launch");
+            boff[(size_t)k * (nh + 1) + e + 1] = (int)nb;
+        }
+    for (int e = 0; e < nh; ++e) {
+        factor_smem = std::max(factor_smem, hs[order[e]]->factor_smem);
+        solve_smem = std::max(solve_smem, (size_t)hs[order[e]]->d.solve_smem);
+    }
+    // state-pointer tables of every step (variant indices, reused from two
+    // steps earlier while the episode set and flags are unchanged)
+    struct StepTab { size_t cur, ahead; int a_cur, a_ahead; };
+    std::vector<StepTab> steps((size_t)K);
+    std::vector<int> pool;                 // variant indices of all tables
+    std::vector<int> sig, last_cur[2], last_ahead[2];
+    size_t last_cur_at[2] = {0, 0}, last_ahead_at[2] = {0, 0};
+    auto intern = [&](const std::vector<int>& v, std::vector<int>* last, size_t* last_at, int ph) {
+        if (!v.empty() && last[ph] == v) return last_at[ph];
+        const size_t at = pool.size();
+        pool.insert(pool.end(), v.begin(), v.end());
+        last[ph] = v;
+        last_at[ph] = at;
+        return at;
+    };
+    for (int64_t k = 0, a = active(0); k < K; ++k) {
+        const int ph = (int)(k & 1);
+        const int an = (k + GEO_AHEAD < K) ? active(k + GEO_AHEAD) : 0;
+        sig.assign((size_t)a, 0);
+        for (int e = 0; e < a; ++e) {
+            const int i = order[e];
+            const int64_t left = n_steps[i] - 1 - k;
+            const int v = left == 0 ? BV_LAST : left == 1 ? BV_SECOND_LAST : BV_PLAIN;
+            sig[e] = i * BV_COUNT + v + ph;
+        }
+        steps[k].cur = intern(sig, last_cur, last_cur_at, ph);
+        steps[k].a_cur = (int)a;
+        sig.assign((size_t)an, 0);
+        for (int e = 0; e < an; ++e) sig[e] = order[e] * BV_COUNT + BV_AHEAD + ph;
+        steps[k].ahead = an ? intern(sig, last_ahead, last_ahead_at, ph) : 0;
+        steps[k].a_ahead = an;
+        a = an ? an : active(k + 1);
+    }
+    // one upload: states, block offsets, first cycles, pointer tables
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t off_var = 0, off_boff = up16(var.size() * sizeof(DevState));
+    const size_t off_cyc = up16(off_boff + boff.size() * sizeof(int));
+    const size_t off_ptr = up16(off_cyc + (size_t)nh * sizeof(long long));
+    const size_t total = up16(off_ptr + pool.size() * sizeof(DevState*));
+    if (total > b->d_cap || total > b->h_cap) {
+        DeviceLock lock(g_device_mutex);
+        const size_t cap = std::max(total, (size_t)1 << 20) * 2;
+        if (b->d_buf) cudaFree(b->d_buf);
+        if (b->h_buf) cudaFreeHost(b->h_buf);
+        b->d_buf = nullptr;
+        b->h_buf = nullptr;
+        b->d_cap = b->h_cap = 0;
+        BCK(cudaMalloc((void**)&b->d_buf, cap));
+        BCK(cudaMallocHost((void**)&b->h_buf, cap));
+        b->d_cap = b->h_cap = cap;
+    }
+    std::memcpy(b->h_buf + off_var, var.data(), var.size() * sizeof(DevState));
+    std::memcpy(b->h_buf + off_boff, boff.data(), boff.size() * sizeof(int));
+    long long* cyc = reinterpret_cast<long long*>(b->h_buf + off_cyc);
+    for (int i = 0; i < nh; ++i) cyc[i] = (long long)first_cycle[i];
+    const DevState** ptrs = reinterpret_cast<const DevState**>(b->h_buf + off_ptr);
+    const DevState* dvar = reinterpret_cast<const DevState*>(b->d_buf + off_var);
+    for (size_t q = 0; q < pool.size(); ++q) ptrs[q] = dvar + pool[q];
+    cudaStream_t sm = b->s_main;
+    BCK(cudaMemcpyAsync(b->d_buf, b->h_buf, total, cudaMemcpyHostToDevice, sm));
+    for (int i = 0; i < nh; ++i) {
+        BCK(cudaMemcpyAsync(hs[i]->d.cycle, b->d_buf + off_cyc + (size_t)i * sizeof(long long), sizeof(long long),
+                            cudaMemcpyDeviceToDevice, sm));
+        BCK(cudaMemsetAsync(hs[i]->d.row_index, 0, sizeof(long long), sm));
+    }
+    auto launch = [&](MultiKernel k, size_t at, int ne, cudaStream_t st) {
+        if (ne <= 0) return;
+        const int* bo = reinterpret_cast<const int*>(b->d_buf + off_boff) + (size_t)k * (nh + 1);
+        const int nb = boff[(size_t)k * (nh + 1) + ne];
+        if (nb <= 0) return;
+        MultiArgs m{reinterpret_cast<const DevState* const*>(b->d_buf + off_ptr) + at, bo, ne};
+        const size_t smem = (k == MK_FACTOR_SMEM || k == MK_FACTOR_GLOBAL) ? factor_smem : solve_smem;
+        if (!launch_multi_ibm(k, m, nb, st) && !launch_multi_solver(k, m, nb, smem, st)) launch_multi_fused(k, m, nb, st);
+    };
+    auto geometry = [&](size_t at, int ne, cudaStream_t sa, cudaStream_t sb, bool events) {
+        launch(MK_GEOMETRY, at, ne, sa);
+        if (events) cudaEventRecord(b->ev_geom, sa);
+        for (MultiKernel k : {MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST}) launch(k, at, ne, sa);
+        if (events) {
+            cudaEventRecord(b->ev_list, sa);
+            cudaStreamWaitEvent(sb, b->ev_geom, 0);
+        }
+        for (MultiKernel k : {MK_ASSEMBLE, MK_FACTOR_SMEM, MK_FACTOR_GLOBAL}) launch(k, at, ne, sb);
+        if (events) cudaEventRecord(b->ev_fact, sb);
+    };
+    // the geometry of the first step (prime_geometry), then the steps as
+    // enqueue_step orders them, every kernel packed over the batch
+    if (K > 0) geometry(steps[0].cur, steps[0].a_cur, sm, sm, false);
+    for (int64_t k = 0; k < K; ++k) {
+        const StepTab& t = steps[k];
+        cudaEventRecord(b->ev_start, sm);
+        for (cudaStream_t st : {b->s_bulk, b->s_ibm, b->s_bc}) cudaStreamWaitEvent(st, b->ev_start, 0);
+        if (t.a_ahead) {
+            cudaStreamWaitEvent(b->s_aux, b->ev_start, 0);
+            geometry(t.ahead, t.a_ahead, b->s_aux, b->s_aux2, true);
+        }
+        launch(MK_BC, t.cur, t.a_cur, b->s_bc);
+        cudaEventRecord(b->ev_bc, b->s_bc);
+        for (MultiKernel k2 : {MK_USTAR, MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH, MK_FORCES})
+            launch(k2, t.cur, t.a_cur, b->s_ibm);
+        cudaEventRecord(b->ev_ibm, b->s_ibm);
+        launch(MK_BULK, t.cur, t.a_cur, b->s_bulk);
+        cudaEventRecord(b->ev_bulk, b->s_bulk);
+        cudaStreamWaitEvent(sm, b->ev_bulk, 0);
+        cudaStreamWaitEvent(sm, b->ev_ibm, 0);
+        launch(MK_BAND, t.cur, t.a_cur, sm);
+        cudaStreamWaitEvent(sm, b->ev_bc, 0);
+        if (t.a_ahead) {   // the next step's geometry, which also reads the cycle advanced below
+            cudaStreamWaitEvent(sm, b->ev_list, 0);
+            cudaStreamWaitEvent(sm, b->ev_fact, 0);
+        }
+        launch(MK_ADVANCE, t.cur, t.a_cur, sm);
+    }
+    BCK(cudaStreamSynchronize(sm));
+    BCK(cudaGetLastError());
+    int failed = -1;
+    for (int i = 0; i < nh; ++i) {
+        LbmHandle* h = hs[i];
+        const int64_t ns = n_steps[i];
+        const int32_t fl = flags ? flags[i] : 0;
+        const bool want_fields = (fl & LBM_STEP_FIELDS) != 0, want_err = (fl & LBM_STEP_ERR) != 0;
+        for (bool& q : h->pending) q = false;
+        int rc = 0;
+        if (ns > 0) {
+            h->parity ^= (int)(ns & 1);
+            h->last_gset = (int)((h->gset + ns - 1) % GEO_SETS);
+            h->gset = (int)((h->gset + ns) % GEO_SETS);
+            if (want_err) {
+                std::swap(h->d.fo_u, h->d.fo_u0);
+                std::swap(h->d.fo_v, h->d.fo_v0);
+            }
+            h->fields_valid = want_fields || want_err;
+            h->err_valid = want_err && ns >= 2;
+            if (force_rows && force_rows[i]) {
+                cudaError_t e = cudaMemcpy(force_rows[i], h->d_rowbuf, sizeof(double) * h->row_len * ns,
+                                           cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) rc = cuda_fail(h, e, "cudaMemcpy");
+            }
+        }
+        if (!rc) rc = check_status(h);
+        if (rcs) rcs[i] = rc;
+        if (rc && failed < 0) failed = i;
+    }
+    if (failed >= 0) return batch_fail(b, "episode " + std::to_string(failed) + ": " + hs[failed]->err);
+    return 0;
+}
+
+void lbm_batch_destroy(LbmBatch* b) {
+    if (!b) return;
+    DeviceLock lock(g_device_mutex);
+    cudaSetDevice(b->device);
+    for (cudaStream_t s : {b->s_main, b->s_bulk, b->s_ibm, b->s_bc, b->s_aux, b->s_aux2})
+        if (s) cudaStreamSynchronize(s);
+    if (b->d_buf) cudaFree(b->d_buf);
+    if (b->h_buf) cudaFreeHost(b->h_buf);
+    for (cudaStream_t s : {b->s_main, b->s_bulk, b->s_ibm, b->s_bc, b->s_aux, b->s_aux2})
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : {b->ev_start, b->ev_bulk, b->ev_ibm, b->ev_bc, b->ev_geom, b->ev_list, b->ev_fact})
+        if (e) cudaEventDestroy(e);
+    delete b;
 }
 
 int lbm_get_sums(LbmHandle* h, double* sum_row, int32_t* sample_count, int32_t* row_len) {

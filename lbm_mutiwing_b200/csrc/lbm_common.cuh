@@ -78,6 +78,12 @@ struct WingMotion {
     double extra_v, extra_s, extra_pos;
 };
 
+// Constants of the fused FP32 collision (deviation storage).
+struct FusedConsts {
+    float s1, s2, s4, s6, s7, s8;   // MRT rates of the non-conserved moments
+    float k1, k2, wm1;              // deviation constants (rest-state moments)
+};
+
 // Everything a step kernel needs, passed by value.
 struct DevState {
     // lattice
@@ -165,6 +171,7 @@ struct DevState {
     int movenum;                 // lattice shifts so far (move_mesh)
     double* wing_fm;             // 3 W raw per-wing Fx, Fy, M of the last step
     double* ibm_resid;           // [0] |X du - r|^2, [1] |r|^2
+    FusedConsts fc;              // fused path: collision constants
 };
 
 __host__ __device__ inline long long pidx(const DevState& d, int i, int j) {

@@ -17,10 +17,6 @@ void launch_err(const DevState& d, double* partial, double* out, cudaStream_t st
 int err_partial_count();
 
 // fused FP32 path (kernels_fp32.cu)
-struct FusedConsts {
-    float s1, s2, s4, s6, s7, s8;   // MRT rates of the non-conserved moments
-    float k1, k2, wm1;              // deviation constants (rest-state moments)
-};
 FusedConsts fused_consts(const DevState& d);
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st);
 bool is_bulk_kernel(const void* func);   // the bulk kernel (low priority in graphs)
@@ -72,5 +68,31 @@ inline __host__ __device__ long long ibm_linv_storage(int nw) {
     return (long long)((nw + IBM_PANEL - 1) / IBM_PANEL) * IBM_PANEL_AUX;
 }
 void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle += 1
+
+// Packed launches: one grid covers the blocks of several episodes, block b
+// running the kernel of episode e = max{e : boff[e] <= b} with local block
+// index b - boff[e] (multi.cuh).  The fused path's kernels only; the bulk
+// and band kernels take the field flag from each episode's state.
+enum MultiKernel : int {
+    MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
+    MK_USTAR, MK_RHS, MK_SPREAD, MK_FINISH, MK_FORCES, MK_ADVANCE,     // immersed boundary
+    MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
+    MK_BULK, MK_BAND, MK_BC,                                            // lattice
+    MK_KINDS
+};
+struct MultiArgs {
+    const DevState* const* ds;   // ne episode states (device memory)
+    const int* boff;             // ne + 1 block offsets (device memory)
+    int ne;
+};
+// blocks of one episode in the packed launch of k (0: none); -1 if k is not
+// handled by that file
+int multi_blocks_ibm(MultiKernel k, const DevState& d);
+int multi_blocks_solver(MultiKernel k, const DevState& d);
+int multi_blocks_fused(MultiKernel k, const DevState& d);
+bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st);
+bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int blocks, size_t smem, cudaStream_t st);
+bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st);
+bool is_bulk_multi_kernel(const void* func);
 
 }  // namespace lbm
