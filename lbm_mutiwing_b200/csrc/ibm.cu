@@ -205,6 +205,7 @@ __device__ __forceinline__ void ibm_geometry_kernel_body(const DevState& d, cons
     if (t < d.band_n[0]) {
         const long long p = pidx(d, d.band_ij[2 * t], d.band_ij[2 * t + 1]);
         d.band_map[p] = BAND_EMPTY;
+        if (d.band_bits) atomicAnd(d.band_bits + (p >> 5), ~(1u << (p & 31)));
         if (d.precision == 0) { d.gfx[p] = 0.0; d.gfy[p] = 0.0; }
     }
     if (t == 0 && d.wing_count > 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
@@ -324,6 +325,7 @@ __device__ __forceinline__ void ibm_list_kernel_body(const DevState& d, const in
                 d.band_wing[b] = w;
                 d.band_claimer[b] = s;
                 d.band_map[p] = -(b + 2);
+                if (d.band_bits) atomicOr(d.band_bits + (p >> 5), 1u << (p & 31));
             }
             ++b;
         }

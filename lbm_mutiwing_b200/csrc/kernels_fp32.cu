@@ -38,20 +38,16 @@ FusedConsts fused_consts(const DevState& d) {
     return c;
 }
 
+// One interior node (i, j); nodes of the band list are left to the band
+// re-collision, which runs concurrently and writes them.
 template <bool FIELDS>
-__device__ __forceinline__ void fused_bulk_body(const float* __restrict__ gA, float* __restrict__ gB,
-                                                int nx, int ny, int pitch, long long plane,
-                                                const FusedConsts& c, double* __restrict__ fo_rho,
+__device__ __forceinline__ void fused_bulk_node(const float* __restrict__ gA, float* __restrict__ gB, int pitch,
+                                                long long plane, const FusedConsts& c, double* __restrict__ fo_rho,
                                                 double* __restrict__ fo_u, double* __restrict__ fo_v,
-                                                int bx, int by) {
-    const int i = bx * BULK_TX + threadIdx.x + 1;
-    if (i > nx - 2) return;
-    const int j0 = by * BULK_ROWS + 1;
-#pragma unroll
-    for (int r = 0; r < BULK_ROWS; ++r) {
-        const int j = j0 + r;
-        if (j > ny - 2) break;
+                                                const unsigned* __restrict__ bits, int i, int j) {
+    {
         const long long p = (long long)j * pitch + i;
+        if ((__ldg(bits + (p >> 5)) >> (p & 31)) & 1u) return;
         float g[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) g[k] = __ldg(gA + k * plane + p - ex(k) - (long long)ey(k) * pitch);
@@ -112,20 +108,72 @@ template <bool FIELDS>
 __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __restrict__ gA, float* __restrict__ gB,
                                                              int nx, int ny, int pitch, long long plane,
                                                              FusedConsts c, double* __restrict__ fo_rho,
-                                                             double* __restrict__ fo_u, double* __restrict__ fo_v) {
-    fused_bulk_body<FIELDS>(gA, gB, nx, ny, pitch, plane, c, fo_rho, fo_u, fo_v, blockIdx.x, blockIdx.y);
+                                                             double* __restrict__ fo_u, double* __restrict__ fo_v,
+                                                             const unsigned* __restrict__ bits) {
+    const int i = blockIdx.x * BULK_TX + threadIdx.x + 1;
+    if (i > nx - 2) return;
+    const int j0 = blockIdx.y * BULK_ROWS + 1;
+#pragma unroll
+    for (int r = 0; r < BULK_ROWS; ++r) {
+        const int j = j0 + r;
+        if (j > ny - 2) break;
+        fused_bulk_node<FIELDS>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
+    }
 }
-// Packed form: an episode's blocks are its x chunks row by row.
-__global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    const DevState& d = *m.ds[e];
-    const int l = blockIdx.x - __ldg(m.boff + e);
-    const int nbx = (d.nx - 2 + BULK_TX - 1) / BULK_TX;
-    const FusedConsts c = d.fc;
-    if (d.write_fields && d.fo_rho)
-        fused_bulk_body<true>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, d.fo_rho, d.fo_u, d.fo_v, l % nbx, l / nbx);
+// Packed form: an episode's interior nodes, row by row without the border
+// columns, in runs of BULK_TX consecutive nodes (a warp may straddle two
+// rows), so narrow lattices leave no thread idle; a block takes
+// BULK_MULTI_RUNS runs.
+#ifndef BULK_MULTI_RUNS
+#define BULK_MULTI_RUNS 1
+#endif
+// The episode's parameters are staged in shared memory by one thread, so
+// the kernel fits the single-episode kernel's register budget (eight
+// 256-thread blocks per SM).
+struct BulkArgs {
+    const float* gA;
+    float* gB;
+    double *fo_rho, *fo_u, *fo_v;
+    const unsigned* bits;
+    long long plane;
+    int pitch, w, n, l, fields;
+    FusedConsts c;
+};
+template <bool FIELDS>
+__device__ __forceinline__ void fused_bulk_runs(const BulkArgs& a) {
+#pragma unroll
+    for (int r = 0; r < BULK_MULTI_RUNS; ++r) {
+        const int t = (a.l * BULK_MULTI_RUNS + r) * BULK_TX + threadIdx.x;
+        if (t >= a.n) break;
+        const int jj = t / a.w;
+        fused_bulk_node<FIELDS>(a.gA, a.gB, a.pitch, a.plane, a.c, a.fo_rho, a.fo_u, a.fo_v, a.bits, t - jj * a.w + 1,
+                                jj + 1);
+    }
+}
+__global__ void __launch_bounds__(BULK_TX, 8) fused_bulk_kernel_multi(MultiArgs m) {
+    __shared__ BulkArgs a;
+    if (threadIdx.x == 0) {
+        const int e = multi_episode(m, blockIdx.x);
+        const DevState& d = *m.ds[e];
+        a.gA = d.gA;
+        a.gB = d.gB;
+        a.fo_rho = d.fo_rho;
+        a.fo_u = d.fo_u;
+        a.fo_v = d.fo_v;
+        a.bits = d.band_bits;
+        a.plane = d.plane;
+        a.pitch = d.pitch;
+        a.w = d.nx - 2;
+        a.n = (d.nx - 2) * (d.ny - 2);
+        a.l = blockIdx.x - m.boff[e];
+        a.fields = d.write_fields && d.fo_rho;
+        a.c = d.fc;
+    }
+    __syncthreads();
+    if (a.fields)
+        fused_bulk_runs<true>(a);
     else
-        fused_bulk_body<false>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr, l % nbx, l / nbx);
+        fused_bulk_runs<false>(a);
 }
 
 // Band nodes: FP64 re-collision with the corrected velocity u* + du and the
@@ -275,9 +323,11 @@ bool is_bulk_kernel(const void* func) {
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st) {
     dim3 b(BULK_TX), g((d.nx - 2 + BULK_TX - 1) / BULK_TX, (d.ny - 2 + BULK_ROWS - 1) / BULK_ROWS);
     if (fields)
-        fused_bulk_kernel<true><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, d.fo_rho, d.fo_u, d.fo_v);
+        fused_bulk_kernel<true><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, d.fo_rho, d.fo_u, d.fo_v,
+                                                 d.band_bits);
     else
-        fused_bulk_kernel<false><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr);
+        fused_bulk_kernel<false><<<g, b, 0, st>>>(d.gA, d.gB, d.nx, d.ny, d.pitch, d.plane, c, nullptr, nullptr, nullptr,
+                                                  d.band_bits);
 }
 // ------------------------------------------------------------ far field
 // boundary_condition1 (boundary_condition.f90:288-858) for the fused path:
@@ -446,7 +496,10 @@ void launch_fused_import(const DevState& d, const double* f, float* g, cudaStrea
 // ------------------------------------------------------------ packed launches
 int multi_blocks_fused(MultiKernel k, const DevState& d) {
     switch (k) {
-    case MK_BULK: return ((d.nx - 2 + BULK_TX - 1) / BULK_TX) * ((d.ny - 2 + BULK_ROWS - 1) / BULK_ROWS);
+    case MK_BULK: {
+        const long long runs = ((long long)(d.nx - 2) * (d.ny - 2) + BULK_TX - 1) / BULK_TX;
+        return (int)((runs + BULK_MULTI_RUNS - 1) / BULK_MULTI_RUNS);
+    }
     case MK_BAND: return (d.band_cap + 127) / 128;
     case MK_BC: return (2 * (d.ny - 2) + 2 * d.nx + 63) / 64;
     default: return -1;

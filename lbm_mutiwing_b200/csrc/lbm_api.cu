@@ -121,6 +121,7 @@ struct GeoSet {
     double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
     int *box = nullptr, *claim_cnt = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
     int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
+    unsigned* band_bits = nullptr;
     double *lband = nullptr, *linv = nullptr;
 };
 
@@ -129,6 +130,7 @@ static GeoSet geo_of(const DevState& d) {
     g.wm = d.wm; g.xb1 = d.xb1; g.yb1 = d.yb1; g.xb2 = d.xb2; g.yb2 = d.yb2; g.kx = d.kx; g.ky = d.ky;
     g.box = d.box; g.claim_cnt = d.claim_cnt; g.pb = d.pb; g.band_claimer = d.band_claimer;
     g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
+    g.band_bits = d.band_bits;
     g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv;
     return g;
 }
@@ -137,6 +139,7 @@ static void use_geo(DevState& d, const GeoSet& g) {
     d.wm = g.wm; d.xb1 = g.xb1; d.yb1 = g.yb1; d.xb2 = g.xb2; d.yb2 = g.yb2; d.kx = g.kx; d.ky = g.ky;
     d.box = g.box; d.claim_cnt = g.claim_cnt; d.pb = g.pb; d.band_claimer = g.band_claimer;
     d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
+    d.band_bits = g.band_bits;
     d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv;
 }
 
@@ -238,6 +241,9 @@ int cuda_fail(LbmHandle* h, cudaError_t e, const char* where) {
         cudaError_t e_ = (call);                                   \
         if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);     \
     } while (0)
+
+// words of a band bit plane (one bit per pitched node index)
+size_t band_bits_words(const DevState& d) { return (size_t)((d.plane + 31) / 32); }
 
 template <class T>
 int dalloc(LbmHandle* h, T** p, size_t count) {
@@ -364,6 +370,7 @@ int init_state(LbmHandle* h) {
     std::vector<int> em(N, BAND_EMPTY);
     for (int s = 0; s < GEO_SETS; ++s) {
         CK(cudaMemcpy(h->geo[s].band_map, em.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        if (h->geo[s].band_bits) CK(cudaMemset(h->geo[s].band_bits, 0, band_bits_words(d) * sizeof(unsigned)));
         CK(cudaMemset(h->geo[s].band_n, 0, 2 * sizeof(int)));
         h->pending[s] = false;
     }
@@ -541,20 +548,24 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
             launch_ibm_rhs(d, true, h->s_ibm);
             launch_ibm_solve(d, true, h->s_ibm);
         }
+        {
+            // band nodes: the bulk kernel leaves them out, so their
+            // re-collision runs beside it
+            PhaseMark pm(h, 2, h->s_ibm);
+            launch_fused_band(d, fields, h->s_ibm);
+        }
+        // the cycle counter advances once the force row is written and the
+        // geometry kernel of the set built now has read it, off the bulk
+        // kernel's critical path
+        if (prefetch) cudaStreamWaitEvent(h->s_ibm, h->ev_geom[h->parity], 0);
+        launch_step_advance(d, h->s_ibm);
         cudaEventRecord(h->ev_ibm, h->s_ibm);
         {
             PhaseMark pm(h, 1, h->s_main);
             launch_fused_bulk(d, h->fc, fields, h->s_main);
         }
         cudaStreamWaitEvent(h->s_main, h->ev_ibm, 0);
-        {
-            PhaseMark pm(h, 2, h->s_main);
-            launch_fused_band(d, fields, h->s_main);
-        }
         cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
-        // the geometry kernel of the set built now reads the cycle counter
-        // that the advance below increments
-        if (prefetch) cudaStreamWaitEvent(h->s_main, h->ev_geom[h->parity], 0);
         // the next step starts once its geometry is complete
         for (int s : {s1, sn}) {
             if (!h->pending[s] || (s != s1 && !drain)) continue;
@@ -562,7 +573,6 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
             cudaStreamWaitEvent(h->s_main, h->ev_fact[s], 0);
             h->pending[s] = false;
         }
-        launch_step_advance(d, h->s_main);
         h->parity = 1 - h->parity;
         h->last_gset = h->gset;
         h->gset = s1;
@@ -804,6 +814,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             return -1;
     }
     if (dalloc(h, &d.band_map, N)) return -1;
+    if (c.precision != LBM_PRECISION_FP64 && dalloc(h, &d.band_bits, band_bits_words(d))) return -1;
     d.band_cap = std::max(64, BOX_SLOTS * ns);
     const int cap = d.band_cap;
     int* band_n = nullptr;
@@ -890,6 +901,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             dalloc(h, &g.box, 4 * nsz) || dalloc(h, &g.claim_cnt, nsz + 1) || dalloc(h, &g.pb, nsz * BOX_SLOTS) ||
             dalloc(h, &g.band_claimer, (size_t)cap) || dalloc(h, &g.band_n, 2) ||
             dalloc(h, &g.band_ij, 2 * (size_t)cap) || dalloc(h, &g.band_wing, cap) || dalloc(h, &g.band_map, N) ||
+            dalloc(h, &g.band_bits, band_bits_words(d)) ||
             dalloc(h, &g.ibm_flags, 4) || dalloc(h, &g.lband, (size_t)std::max<long long>(1, ltot)) ||
             dalloc(h, &g.linv, (size_t)std::max<long long>(1, itot)))
             return -1;
@@ -1235,20 +1247,23 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         }
         launch(MK_BC, t.cur, t.a_cur, b->s_bc);
         cudaEventRecord(b->ev_bc, b->s_bc);
-        for (MultiKernel k2 : {MK_USTAR, MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH, MK_FORCES})
+        for (MultiKernel k2 :
+             {MK_USTAR, MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH, MK_BAND, MK_FORCES})
             launch(k2, t.cur, t.a_cur, b->s_ibm);
+        // the cycle counters advance after the force rows and after the
+        // geometry kernel of the next step has read them
+        if (t.a_ahead) cudaStreamWaitEvent(b->s_ibm, b->ev_geom, 0);
+        launch(MK_ADVANCE, t.cur, t.a_cur, b->s_ibm);
         cudaEventRecord(b->ev_ibm, b->s_ibm);
         launch(MK_BULK, t.cur, t.a_cur, b->s_bulk);
         cudaEventRecord(b->ev_bulk, b->s_bulk);
         cudaStreamWaitEvent(sm, b->ev_bulk, 0);
         cudaStreamWaitEvent(sm, b->ev_ibm, 0);
-        launch(MK_BAND, t.cur, t.a_cur, sm);
         cudaStreamWaitEvent(sm, b->ev_bc, 0);
-        if (t.a_ahead) {   // the next step's geometry, which also reads the cycle advanced below
+        if (t.a_ahead) {   // the next step's geometry
             cudaStreamWaitEvent(sm, b->ev_list, 0);
             cudaStreamWaitEvent(sm, b->ev_fact, 0);
         }
-        launch(MK_ADVANCE, t.cur, t.a_cur, sm);
     }
     BCK(cudaStreamSynchronize(sm));
     BCK(cudaGetLastError());

@@ -105,6 +105,7 @@ struct DevState {
     double *fo_u0, *fo_v0;               // previous-step velocity (err)
     // band bookkeeping
     int* band_map;               // ny * pitch: BAND_EMPTY, claiming segment, or -(b + 2)
+    unsigned* band_bits;         // fused path: one bit per node (pitched index) set for listed band nodes
     int band_cap;
     int* band_n;                 // [0] current band size, [1] previous band size
     int* band_ij;                // 2 * cap (i, j) 0-based
