@@ -188,7 +188,8 @@ def config_of(ep, storage, world):
 def serving_metrics(steps=200, requests=3, rate_hz=20.0):
     """The seeded 64-episode mixed batch (grids 401x201 .. 2001x1001, 1-4
     wings): (1) every episode advanced `steps` steps, all resident and in
-    flight at once (FP32), against the same episodes served one at a time
+    flight at once (FP32; packed launches over all episodes, and each episode
+    on its own streams), against the same episodes served one at a time
     through the plain FP64 path; (2) 64 online clients (one per episode) on
     the ZeroMQ server with Poisson arrivals, segments of 100-2000 steps, SAVE
     with p = 0.05: STEP latency percentiles at the client; (3) the FP32
@@ -198,14 +199,19 @@ def serving_metrics(steps=200, requests=3, rate_hz=20.0):
     from lbm_mutiwing_b200 import protocol as P
     from lbm_mutiwing_b200 import workloads as wl
     from lbm_mutiwing_b200.serve import Server
-    eps = wl.mixed_batch(64, steps=steps + 8)
+    eps = wl.mixed_batch(64, steps=2 * steps + 16)
     nodes = sum(e.nx * e.ny for e in eps)
     sims = batch.create(eps, api.PRECISION_FP32)
-    batch.advance_together(sims, 4, first_cycle=1)
-    wall = batch.advance_together(sims, steps, first_cycle=5)
+    packed = api.Batch(0)
+    batch.advance_packed(sims, 4, first_cycle=1, packed=packed)
+    wall = batch.advance_packed(sims, steps, first_cycle=5, packed=packed)
+    packed.close()
+    batched = nodes * steps / wall / 1e6
+    batch.advance_together(sims, 4, first_cycle=steps + 5)
+    wall_streams = batch.advance_together(sims, steps, first_cycle=steps + 9)
     for s in sims:
         s.close()
-    batched = nodes * steps / wall / 1e6
+    batched_streams = nodes * steps / wall_streams / 1e6
     plain_s, plain_nu = batch.advance_one_at_a_time(eps, max(8, steps // 4))
     plain = plain_nu / plain_s / 1e6
     srv = Server("tcp://127.0.0.1:0", wl.by_name, "mix:0", precision=api.PRECISION_FP32, workers=64)
@@ -237,7 +243,8 @@ def serving_metrics(steps=200, requests=3, rate_hz=20.0):
         fa, fb = a[1:1 + 3 * W], b[1:1 + 3 * W]
         err = max(err, float(np.max(np.abs(fa - fb)) / max(float(np.max(np.abs(fb))), 1e-30)))
     return {"episodes": len(eps), "nodes": nodes, "wings": sum(e.wing_count for e in eps),
-            "batched_fp32_mlups": batched, "one_at_a_time_fp64_mlups": plain,
+            "batched_fp32_mlups": batched, "batched_streams_fp32_mlups": batched_streams,
+            "one_at_a_time_fp64_mlups": plain,
             "batched_over_one_at_a_time": batched / plain,
             "served_clients": len(names), "served_steps": len(res.step_latency_s),
             "served_step_p50_ms": res.percentile(50) * 1e3, "served_step_p99_ms": res.percentile(99) * 1e3,

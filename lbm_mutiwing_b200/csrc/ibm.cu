@@ -678,6 +678,14 @@ static inline int blocks(long long n, int t) { return (int)std::max<long long>(1
 
 int ibm_finish_blocks(const DevState& d) { return blocks(d.band_cap, FINISH_THREADS); }
 
+bool is_geometry_kernel(const void* func) {
+    for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel), reinterpret_cast<const void*>(ibm_claim_kernel),
+                          reinterpret_cast<const void*>(ibm_count_kernel), reinterpret_cast<const void*>(ibm_scan_kernel),
+                          reinterpret_cast<const void*>(ibm_list_kernel), reinterpret_cast<const void*>(ibm_assemble_kernel)})
+        if (func == k) return true;
+    return is_factor_kernel(func);
+}
+
 void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done) {
     const long long n1 = std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap);
     ibm_geometry_kernel<<<blocks(n1, 128), 128, 0, st>>>(d);

@@ -491,6 +491,11 @@ cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     return e;
 }
 
+bool is_factor_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(ibm_factor_kernel<true>) ||
+           func == reinterpret_cast<const void*>(ibm_factor_kernel<false>);
+}
+
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st) {
     if (d.wing_count <= 0) return;
     if (d.factor_in_smem)

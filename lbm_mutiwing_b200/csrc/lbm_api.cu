@@ -153,6 +153,7 @@ struct LbmHandle {
     GeoSet geo[GEO_SETS];           // geometry sets (the plain path uses set 0)
     int gset = 0;                   // fused path: set of the next step
     int prio_lo = 0, prio_hi = 0;   // stream priority range of the device
+    int prio_mid = 0;               // between them: geometry built ahead, far field
     int last_gset = 0;              // set of the last completed step
     bool pending[GEO_SETS] = {};    // set built on the side streams, not yet waited for
     // streams of one fused step: main (bulk kernel, band re-collision),
@@ -200,8 +201,8 @@ struct LbmHandle {
 
 // Packed stepping of many fused-path handles (lbm_batch_step): one launch per
 // kernel of a step covers every episode of the batch.  The streams mirror a
-// handle's: bulk (low priority), and main, immersed boundary, far field and
-// the two geometry streams (high priority).
+// handle's: bulk (low priority), far field and the two geometry streams
+// (middle), main and immersed boundary (high).
 struct LbmBatch {
     int device = 0;
     std::string err;
@@ -613,10 +614,10 @@ int build_graph(LbmHandle* h, int p, int gs) {
     std::copy(saved_pending, saved_pending + GEO_SETS, h->pending);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
     // Graph launches run every node at the priority of the launch stream
-    // unless nodes carry their own: the bulk kernel gets the low priority
-    // and every other kernel the high one, so the immersed-boundary, far
-    // field and geometry kernels are dispatched ahead of pending bulk blocks
-    // instead of after the bulk grid.
+    // unless nodes carry their own: the bulk kernel gets the low priority,
+    // the far field and the geometry kernels the middle one and the
+    // immersed-boundary chain the high one, so all are dispatched ahead of
+    // pending bulk blocks instead of after the bulk grid, the chain first.
     size_t nn = 0;
     e = cudaGraphGetNodes(g, nullptr, &nn);
     std::vector<cudaGraphNode_t> nodes(nn);
@@ -630,7 +631,9 @@ int build_graph(LbmHandle* h, int p, int gs) {
         if (e != cudaSuccess) break;
         cudaKernelNodeAttrValue v;
         std::memset(&v, 0, sizeof(v));
-        v.priority = is_bulk_kernel(kp.func) ? h->prio_lo : h->prio_hi;
+        v.priority = is_bulk_kernel(kp.func)                                      ? h->prio_lo
+                     : (is_geometry_kernel(kp.func) || is_far_field_kernel(kp.func)) ? h->prio_mid
+                                                                                      : h->prio_hi;
         e = cudaGraphKernelNodeSetAttribute(nodes[k], cudaKernelNodeAttributePriority, &v);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&h->gexec[p][gs], g, cudaGraphInstantiateFlagUseNodePriority);
@@ -908,20 +911,23 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     if (ensure_rows(h, 1024)) return -1;
     // the immersed-boundary chain is latency-bound and on the critical path:
-    // its streams get the highest priority so their blocks are scheduled
-    // ahead of waiting bulk blocks
+    // its stream gets the highest priority so its blocks are scheduled ahead
+    // of waiting bulk blocks; the far field and the geometry built a step
+    // ahead have slack until the step ends and take the middle priority, so
+    // they never delay the chain
     int prio_lo = 0, prio_hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     h->prio_lo = prio_lo;
     h->prio_hi = prio_hi;
+    h->prio_mid = (prio_lo + prio_hi) / 2;
     CK(cudaStreamCreateWithPriority(&h->s_main, cudaStreamNonBlocking, prio_lo));
     CK(cudaStreamCreateWithPriority(&h->s_ibm, cudaStreamNonBlocking, prio_hi));
     for (int k = 0; k < 2; ++k) {
-        CK(cudaStreamCreateWithPriority(&h->s_aux[k], cudaStreamNonBlocking, prio_hi));
-        CK(cudaStreamCreateWithPriority(&h->s_aux2[k], cudaStreamNonBlocking, prio_hi));
+        CK(cudaStreamCreateWithPriority(&h->s_aux[k], cudaStreamNonBlocking, h->prio_mid));
+        CK(cudaStreamCreateWithPriority(&h->s_aux2[k], cudaStreamNonBlocking, h->prio_mid));
         CK(cudaEventCreateWithFlags(&h->ev_geom[k], cudaEventDisableTiming));
     }
-    CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, h->prio_mid));
     for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_bc})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     for (int s = 0; s < GEO_SETS; ++s) {
@@ -1076,9 +1082,12 @@ int lbm_batch_create(int32_t device, LbmBatch** out) {
     BCK(cudaSetDevice(device));
     int lo = 0, hi = 0;
     BCK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    const int mid = (lo + hi) / 2;
     BCK(cudaStreamCreateWithPriority(&b->s_bulk, cudaStreamNonBlocking, lo));
-    for (cudaStream_t* st : {&b->s_main, &b->s_ibm, &b->s_bc, &b->s_aux, &b->s_aux2})
+    for (cudaStream_t* st : {&b->s_main, &b->s_ibm})
         BCK(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi));
+    for (cudaStream_t* st : {&b->s_bc, &b->s_aux, &b->s_aux2})
+        BCK(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, mid));
     for (cudaEvent_t* e : {&b->ev_start, &b->ev_bulk, &b->ev_ibm, &b->ev_bc, &b->ev_geom, &b->ev_list, &b->ev_fact})
         BCK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return 0;

@@ -20,6 +20,7 @@ int err_partial_count();
 FusedConsts fused_consts(const DevState& d);
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st);
 bool is_bulk_kernel(const void* func);   // the bulk kernel (low priority in graphs)
+bool is_far_field_kernel(const void* func);
 void launch_fused_band(const DevState& d, bool fields, cudaStream_t st);
 void launch_fused_bc(const DevState& d, cudaStream_t st);   // far field of the fused path
 void launch_fused_init(const DevState& d, cudaStream_t st);
@@ -38,6 +39,9 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st);
 // substitution, spread, velocity correction, forces (needs rhs and factor)
 void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st);
 int ibm_finish_blocks(const DevState& d);
+// kernels of a step's geometry (motion through factorisation)
+bool is_geometry_kernel(const void* func);
+bool is_factor_kernel(const void* func);
 // banded L' D L'^T factorisation and substitution (ibm_solver.cu)
 cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem);
 // dynamic shared memory of the substitution kernel

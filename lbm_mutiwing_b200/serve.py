@@ -4,11 +4,12 @@ batching.
 
 * One ROUTER socket; every client (ZeroMQ identity) owns one episode, kept
   resident in HBM between its requests.
-* Requests are executed by a pool of worker threads; each episode's work runs
-  on its own CUDA streams (CUDA-graph segments), so the segments of all
-  clients in flight overlap on the device.  A request that arrives while
-  others are on the GPU starts as soon as a worker is free -- it does not
-  wait for a batch boundary.
+* Requests are executed by a pool of worker threads.  The lattice steps of
+  FP32 episodes go to one continuous batcher (``batch.PackedStepper``): every
+  step is one packed launch per kernel over all clients' episodes in flight,
+  in rounds of at most ``chunk`` steps, and a request that arrives meanwhile
+  joins at the next round -- it does not wait for the others' segments to
+  end.  FP64 episodes (and ``packed=False``) step on their own CUDA streams.
 * Admission by device memory: a RESET that would exceed the memory budget
   waits until running episodes end (STOP) and free their memory.
 * Replies are the reference's text replies (``protocol``); per-request
@@ -68,7 +69,7 @@ class Server:
     def __init__(self, endpoint: str, make_episode: Callable, default_workload: str, precision: int = 1,
                  device: int = 0, workers: int = 64, out_dir: Optional[str] = None,
                  budget_bytes: Optional[int] = None, single: bool = False, write_force_files: bool = False,
-                 sim_factory: Optional[Callable] = None):
+                 sim_factory: Optional[Callable] = None, packed: bool = True, chunk: int = 200):
         import zmq
         self.zmq = zmq
         self.endpoint = endpoint
@@ -81,6 +82,10 @@ class Server:
         self.single = single
         self.write_force_files = write_force_files
         self.sim_factory = sim_factory or _default_sim_factory
+        # packed stepping needs the library's simulations on the FP32 path
+        self.packed = packed and sim_factory is None and precision != 0 and not single
+        self.chunk = chunk
+        self._stepper = None
         self.ctx = zmq.Context.instance()
         self.sock = self.ctx.socket(zmq.REP if single else zmq.ROUTER)
         self.sock.setsockopt(zmq.LINGER, 0)
@@ -155,7 +160,7 @@ class Server:
             out = self.out_dir
             if out is not None and not self.single:
                 out = os.path.join(out, f"client_{idx}")
-            c.session = EpisodeSession(sim, ep, out, 0, self.write_force_files)
+            c.session = EpisodeSession(sim, ep, out, 0, self.write_force_files, stepper=self._get_stepper())
             c.workload = name
             c.nodes = ep.nx * ep.ny
             nb = int(sim.device_bytes()) if hasattr(sim, "device_bytes") else 0
@@ -163,6 +168,15 @@ class Server:
                 self.resident_bytes += nb - c.bytes
             c.bytes = nb
         return c.session.handle(cmd)
+
+    def _get_stepper(self):
+        if not self.packed:
+            return None
+        with self.lock:
+            if self._stepper is None:
+                from .batch import PackedStepper
+                self._stepper = PackedStepper(self.device, self.chunk)
+            return self._stepper.step
 
     def _release(self, c: _Client):
         if c.session is not None:
@@ -270,6 +284,9 @@ class Server:
         self.pool.shutdown(wait=True)
         for c in list(self.clients.values()):
             self._release(c)
+        if self._stepper is not None:
+            self._stepper.close()
+            self._stepper = None
         self.sock.close(0)
         self.wake_pull.close(0)
 

@@ -28,8 +28,12 @@ class EpisodeSession:
     """State of one client's episode between requests."""
 
     def __init__(self, sim, ep, out_dir: Optional[str] = None, episode_index: int = 0,
-                 write_force_files: bool = False, output_stride=(2, 2)):
+                 write_force_files: bool = False, output_stride=(2, 2), stepper=None):
         self.sim = sim
+        # stepper(sim, n_steps, first_cycle=, rows=, flags=) advances the
+        # simulation: by default its own step; the server passes its
+        # continuous batcher
+        self.stepper = stepper
         self.ep = ep
         self.W = ep.wing_count
         self.ncol = 1 + 9 * self.W
@@ -135,7 +139,10 @@ class EpisodeSession:
         nsteps = target_cycle - self.n + 1
         self.sim.set_stream_rows(self.start_row, self.target_row)
         self.sim.reset_sums()
-        rows = self.sim.step(nsteps, first_cycle=self.n, rows=True, flags=STEP_FIELDS)
+        if self.stepper is not None:
+            rows = self.stepper(self.sim, nsteps, first_cycle=self.n, rows=True, flags=STEP_FIELDS)
+        else:
+            rows = self.sim.step(nsteps, first_cycle=self.n, rows=True, flags=STEP_FIELDS)
         self.last_rows = rows
         self.n = target_cycle + 1
         self.steps_run += nsteps

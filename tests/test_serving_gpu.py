@@ -7,7 +7,8 @@
 * served FORCE replies equal the segment averages of a direct run through
   the C ABI with the same motion rows;
 * a client's replies are identical alone and in a mix of concurrent clients
-  (episodes are independent and deterministic).
+  (episodes are independent and deterministic), and the same whether the
+  server steps episodes in packed rounds or each on its own streams.
 """
 import threading
 
@@ -83,9 +84,9 @@ def test_plain_output_matches_oracle(gpu_lib, oracle_lib):
         assert np.abs(g - w).max() <= 1e-9 * max(1.0, np.abs(w).max())
 
 
-def _server():
+def _server(**kw):
     from lbm_mutiwing_b200.serve import Server
-    srv = Server("tcp://127.0.0.1:0", make_episode, "a", precision=api.PRECISION_FP32, workers=8)
+    srv = Server("tcp://127.0.0.1:0", make_episode, "a", precision=api.PRECISION_FP32, workers=8, **kw)
     th = threading.Thread(target=srv.serve, kwargs={"idle_timeout_s": 120}, daemon=True)
     th.start()
     return srv, th, f"tcp://127.0.0.1:{srv.port}"
@@ -161,3 +162,32 @@ def test_served_replies_same_alone_and_in_mix(gpu_lib):
     assert all(r.startswith("FORCE") for r in alone[:-1])
     assert out[0] == alone and out[3] == alone
     assert out[1] == out[4]
+
+
+def _mix(**kw):
+    srv, th, addr = _server(**kw)
+    out = {}
+    try:
+        def run(k, name):
+            out[k] = loadgen.run_script(addr, _script(name), identity=b"mix%d" % k)
+        ths = [threading.Thread(target=run, args=(k, n)) for k, n in enumerate("abcab")]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+    finally:
+        srv.stop()
+        th.join(30)
+        srv.close()
+    return out
+
+
+def test_packed_rounds_equal_own_streams(gpu_lib):
+    """Continuous batching in rounds of 5 steps (segments of 7, 30 and 12
+    steps split across rounds, clients joining mid-segment) gives the same
+    replies as every episode stepping alone on its own streams."""
+    ref = _mix(packed=False)
+    got = _mix(chunk=5)
+    assert all(r.startswith("FORCE") for r in ref[0][:-1])
+    for k in range(5):
+        assert got[k] == ref[k], k
