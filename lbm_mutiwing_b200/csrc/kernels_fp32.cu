@@ -39,15 +39,21 @@ FusedConsts fused_consts(const DevState& d) {
 }
 
 // One interior node (i, j); nodes of the band list are left to the band
-// re-collision, which runs concurrently and writes them.
-template <bool FIELDS>
+// re-collision, which runs concurrently and writes them.  EARLY: the band
+// bit is tested before the nine pulls (one memory round trip ahead of
+// them); otherwise it is loaded beside them and only gates the stores.  In
+// the single-episode step the early test is faster overall: the bulk kernel
+// then draws a little less bandwidth from the concurrent immersed-boundary
+// chain, which is as long as the bulk kernel at 4001 x 2001.
+template <bool FIELDS, bool EARLY>
 __device__ __forceinline__ void fused_bulk_node(const float* __restrict__ gA, float* __restrict__ gB, int pitch,
                                                 long long plane, const FusedConsts& c, double* __restrict__ fo_rho,
                                                 double* __restrict__ fo_u, double* __restrict__ fo_v,
                                                 const unsigned* __restrict__ bits, int i, int j) {
     {
         const long long p = (long long)j * pitch + i;
-        if ((__ldg(bits + (p >> 5)) >> (p & 31)) & 1u) return;
+        const unsigned word = __ldg(bits + (p >> 5));
+        if (EARLY && ((word >> (p & 31)) & 1u)) return;
         float g[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) g[k] = __ldg(gA + k * plane + p - ex(k) - (long long)ey(k) * pitch);
@@ -94,6 +100,7 @@ __device__ __forceinline__ void fused_bulk_node(const float* __restrict__ gA, fl
         o[6] = rD - xd + yd - b8;
         o[7] = rD - xd - yd + b8;
         o[8] = rD + xd - yd - b8;
+        if (!EARLY && ((word >> (p & 31)) & 1u)) return;
 #pragma unroll
         for (int k = 0; k < 9; ++k) gB[k * plane + p] = o[k];
         if (FIELDS) {
@@ -117,15 +124,16 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
     for (int r = 0; r < BULK_ROWS; ++r) {
         const int j = j0 + r;
         if (j > ny - 2) break;
-        fused_bulk_node<FIELDS>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
+        fused_bulk_node<FIELDS, true>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
     }
 }
 // Packed form: an episode's interior nodes, row by row without the border
 // columns, in runs of BULK_TX consecutive nodes (a warp may straddle two
 // rows), so narrow lattices leave no thread idle; a block takes
-// BULK_MULTI_RUNS runs.
+// BULK_MULTI_RUNS runs (2: 8% faster steps than 1 on the 64-episode mixed
+// batch; 4 no better, 8 worse).
 #ifndef BULK_MULTI_RUNS
-#define BULK_MULTI_RUNS 1
+#define BULK_MULTI_RUNS 2
 #endif
 // The episode's parameters are staged in shared memory by one thread, so
 // the kernel fits the single-episode kernel's register budget (eight
@@ -146,8 +154,8 @@ __device__ __forceinline__ void fused_bulk_runs(const BulkArgs& a) {
         const int t = (a.l * BULK_MULTI_RUNS + r) * BULK_TX + threadIdx.x;
         if (t >= a.n) break;
         const int jj = t / a.w;
-        fused_bulk_node<FIELDS>(a.gA, a.gB, a.pitch, a.plane, a.c, a.fo_rho, a.fo_u, a.fo_v, a.bits, t - jj * a.w + 1,
-                                jj + 1);
+        fused_bulk_node<FIELDS, false>(a.gA, a.gB, a.pitch, a.plane, a.c, a.fo_rho, a.fo_u, a.fo_v, a.bits,
+                                       t - jj * a.w + 1, jj + 1);
     }
 }
 __global__ void __launch_bounds__(BULK_TX, 8) fused_bulk_kernel_multi(MultiArgs m) {
