@@ -177,8 +177,10 @@ int lbm_status(LbmHandle* h, int32_t* bits);
  * CUDA events around its kernels; lbm_get_phase_times returns, in ms summed
  * over the timed steps: [0] move_boundary (markers and band), [1]
  * collide-stream (bulk kernel, or stream + moments + collide), [2] band
- * re-collision, [3] far-field boundary, [4] immersed-boundary right-hand
- * side, substitution, spread and forces, [5] assembly and factorisation of
+ * re-collision (FP64 path: none, the collide pass covers it; FP32 path: 0,
+ * it is part of [4]), [3] far-field boundary, [4] immersed-boundary
+ * right-hand side, substitution, spread and forces (FP32 path: with the band
+ * re-collision and the cycle advance), [5] assembly and factorisation of
  * the immersed-boundary system, and [6] the number of steps timed.  On the
  * FP32 path phases 0, 3, 4 and 5 overlap phase 1.  Enabling (or disabling)
  * clears the totals.  n is the length of out (at most 7 values are written). */

@@ -94,15 +94,21 @@ __device__ inline void triplet(double s0, double v0, double v1, double dt, doubl
     a = dv / dt * smooth_d(x);
 }
 
+// time of the current step (force rows) and of the geometry being built
+// (solution.f90:292); the geometry runs one step ahead of the flow on its
+// own counter, which the band list kernel advances
 __device__ inline double step_time(const DevState& d) {
-    return mul((double)(*d.cycle + d.cycle_ahead - 1), mul(d.scale, d.uu));   // solution.f90:292
+    return mul((double)(*d.cycle - 1), mul(d.scale, d.uu));
+}
+__device__ inline double geometry_time(const DevState& d) {
+    return mul((double)(*d.gcycle - 1), mul(d.scale, d.uu));
 }
 
 // mode + apply_motion_row for wing w at the current cycle (mode.f90:451-471,
 // 180-218, 414-449) and update_body_extra_from_rel (mode.f90:473-495),
 // whose relative motion is zero unless rigid-body dynamics are enabled.
 __device__ WingMotion wing_motion(const DevState& d, int w) {
-    const double time = step_time(d);
+    const double time = geometry_time(d);
     double v[9];
     if (d.motion_source == 2) {
         const double t1 = d.stream_start[0], t2 = d.stream_target[0], dt = t2 - t1;
@@ -309,8 +315,10 @@ __global__ void __launch_bounds__(1024) ibm_scan_kernel_multi(MultiArgs m) {
 // Band list in the reference's order (segment, then i, then j) and the
 // band_map encoding -(b + 2); a node still holding its claimer's index is
 // never confused with another segment's index, so encoding as we go is safe.
+// The geometry's cycle counter moves on (the motion kernel read it before).
 __device__ __forceinline__ void ibm_list_kernel_body(const DevState& d, const int bid_) {
     const int s = bid_ * blockDim.x + threadIdx.x;
+    if (s == 0) *d.gcycle += 1;
     if (s >= d.nseg || box_empty(d, s)) return;
     const int nb = d.band_n[0];
     const int w = d.seg_wing[s];
@@ -370,11 +378,6 @@ __device__ __forceinline__ void ibm_ustar_kernel_body(const DevState& d, const i
 }
 template <bool FUSED>
 __global__ void ibm_ustar_kernel(DevState d) { ibm_ustar_kernel_body<FUSED>(d, blockIdx.x); }
-template <bool FUSED>
-__global__ void ibm_ustar_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    ibm_ustar_kernel_body<FUSED>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
-}
 
 // r = ub - X u* (boundary_condition.f90:1540-1555, 1609-1629) and the band
 // index of each (segment, slot); one warp per segment, slots 0..35 over the
@@ -424,9 +427,82 @@ __device__ __forceinline__ void ibm_rhs_kernel_body(const DevState& d, const int
     }
 }
 __global__ void ibm_rhs_kernel(DevState d) { ibm_rhs_kernel_body(d, blockIdx.x); }
-__global__ void ibm_rhs_kernel_multi(MultiArgs m) {
+
+// rho and u* of a band node from its pulled distributions (fused path;
+// band nodes are interior nodes: boxes keep off the border), as the
+// moments of solution.f90:510-554.
+__device__ __forceinline__ void pulled_moments(const DevState& d, long long p, double f[9], double& rho, double& us,
+                                               double& vs) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
+    double trho = 0.0, tu = 0.0, tv = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        trho = trho + f[k];
+        tu = tu + (double)ex(k) * f[k];
+        tv = tv + (double)ey(k) * f[k];
+    }
+    rho = trho;
+    us = tu / trho;
+    vs = tv / trho;
+}
+
+// Fused path: the rhs with u* evaluated at each box node from the pulled
+// distributions (no separate u* pass), clearing the spread accumulators of
+// the band nodes it meets (every listed node lies in its claimer's box).
+__device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int bid_) {
+    const int s = (bid_ * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= d.nseg) return;
+    const int nb = d.band_n[0];
+    const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
+    double bu = 0.0, bv = 0.0;
+    for (int slot = lane; slot < BOX_SLOTS; slot += 32) {
+        const int a = slot / 6, c = slot % 6;
+        const int i = i1 + a, j = j1 + c;
+        int bi = -1;
+        if (i <= i2 && j <= j2) {
+            const long long p = pidx(d, i - 1, j - 1);
+            const int bm = d.band_map[p];
+            bi = (bm <= -2) ? -(bm + 2) : -1;
+            if (bi >= nb) bi = -1;
+            if (bi < 0) {
+                set_status(d, ST_BAND_OVERFLOW);
+            } else {
+                double f[9], rho, us, vs;
+                pulled_moments(d, p, f, rho, us, vs);
+                reinterpret_cast<unsigned long long*>(d.band_du)[bi] = 0ull;
+                reinterpret_cast<unsigned long long*>(d.band_dv)[bi] = 0ull;
+                const double wv = d.kx[6 * s + a] * d.ky[6 * s + c];
+                bu = bu + wv * us;
+                bv = bv + wv * vs;
+            }
+        }
+        d.pb[s * BOX_SLOTS + slot] = bi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bu += __shfl_xor_sync(0xffffffffu, bu, o);
+        bv += __shfl_xor_sync(0xffffffffu, bv, o);
+    }
+    if (lane == 0) {
+        const int w = d.seg_wing[s];
+        const WingMotion m = d.wm[w];
+        const int p = d.wing_pstart[w] + (s - d.wing_sstart[w]);
+        double sn, cs;
+        sincos(m.angle, &sn, &cs);
+        const double xs = d.xb0[p + 1] + d.xb0[p], ys = d.yb0[p + 1] + d.yb0[p];
+        const double ub = d.uu * (-(m.omega * sn * 0.5 * xs) + m.omega * cs * 0.5 * ys + m.sau) + m.extra_v;
+        const double vb = d.uu * (-(m.omega * cs * 0.5 * xs) - m.omega * sn * 0.5 * ys + m.sbv);
+        d.rx[s] = ub - bu;
+        d.ry[s] = vb - bv;
+        d.qx[s] = ub - bu;   // kept for the residual diagnostic
+        d.qy[s] = vb - bv;
+    }
+}
+__global__ void ibm_rhs_fused_kernel(DevState d) { ibm_rhs_fused_body(d, blockIdx.x); }
+__global__ void ibm_rhs_fused_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
-    ibm_rhs_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+    ibm_rhs_fused_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
 // G(a, c) = Sx(a, c) Sy(a, c), the delta kernel being separable.
@@ -457,6 +533,11 @@ __global__ void ibm_assemble_kernel(DevState d) { ibm_assemble_kernel_body(d, bl
 __global__ void ibm_assemble_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     ibm_assemble_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
+
+// blocks of the finish and closing kernels (as ibm_finish_blocks)
+__device__ __forceinline__ int ibm_finish_blocks_dev(const DevState& d) {
+    return (int)max(1LL, ((long long)d.band_cap + FINISH_THREADS - 1) / FINISH_THREADS);
 }
 
 // Fixed-point exponent shared by the spread and the finish kernels: every
@@ -561,17 +642,14 @@ __device__ __forceinline__ void ibm_finish_kernel_body(const DevState& d, const 
 }
 template <bool FUSED>
 __global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) { ibm_finish_kernel_body<FUSED>(d, blockIdx.x); }
-template <bool FUSED>
-__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    ibm_finish_kernel_body<FUSED>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
-}
 
 // Per-wing force and moment from the block partials (in block order), the
-// no-slip residual when diagnostics are on, and the force row.
-__device__ __forceinline__ void ibm_forces_kernel_body(const DevState& d, const int bid_) {
+// no-slip residual when diagnostics are on, and the force row; run by one
+// block of 256 threads.  The partials come from other blocks: they are read
+// through L2.
+__device__ __forceinline__ void force_row_body(const DevState& d) {
     const int nblocks = (int)max(1LL, ((long long)d.band_cap + FINISH_THREADS - 1) / FINISH_THREADS);
-    constexpr int CHUNK = 64;   // block partials staged per pass
+    constexpr int CHUNK = 16;   // block partials staged per pass
     __shared__ double fm[MAX_WINGS][3];
     __shared__ double red[8][2];
     __shared__ double part[CHUNK * MAX_WINGS * 3];
@@ -580,7 +658,7 @@ __device__ __forceinline__ void ibm_forces_kernel_body(const DevState& d, const 
     double v = 0.0;
     for (int k0 = 0; k0 < nblocks; k0 += CHUNK) {
         const int nk = min(CHUNK, nblocks - k0);
-        for (int t = tid; t < nk * 3 * W; t += blockDim.x) part[t] = d.force_part[(long long)k0 * W * 3 + t];
+        for (int t = tid; t < nk * 3 * W; t += blockDim.x) part[t] = __ldcg(d.force_part + (long long)k0 * W * 3 + t);
         __syncthreads();
         if (tid < 3 * W)
             for (int k = 0; k < nk; ++k) v += part[k * 3 * W + tid];
@@ -655,22 +733,155 @@ __device__ __forceinline__ void ibm_forces_kernel_body(const DevState& d, const 
         d.sum_row[c] = d.sum_row[c] + rowv[c];
     }
 }
-__global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d) { ibm_forces_kernel_body(d, blockIdx.x); }
-__global__ void __launch_bounds__(256) ibm_forces_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    ibm_forces_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
-}
+__global__ void __launch_bounds__(256) ibm_forces_kernel(DevState d) { force_row_body(d); }
 
-__device__ __forceinline__ void step_advance_kernel_body(const DevState& d, const int bid_) {
-    if (threadIdx.x == 0 && bid_ == 0) {
+__global__ void step_advance_kernel(DevState d) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
         *d.cycle += 1;
         *d.row_index += 1;
     }
 }
-__global__ void step_advance_kernel(DevState d) { step_advance_kernel_body(d, blockIdx.x); }
-__global__ void step_advance_kernel_multi(MultiArgs m) {
+
+// Band node re-collision in FP64 with the corrected velocity (ut, vt) and the
+// body force (gx, gy) = 2 rho du (solution.f90:599-655 with
+// boundary_condition.f90:1645-1659); f holds the pulled distributions.
+template <bool FIELDS>
+__device__ __forceinline__ void band_recollide(const DevState& d, long long p, const double f[9], double rt, double ut,
+                                               double vt, double gx, double gy) {
+    double temp[9], temp1[9], fp[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sum = sum + (double)mrt_m(r, q) * f[q];
+        temp1[r] = sum;
+    }
+    const double* s = d.s;
+    temp[0] = 0.0;
+    temp[1] = -(2.0 * rt) + 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[2] = rt - 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[3] = 0.0;
+    temp[4] = -(rt * ut);
+    temp[5] = 0.0;
+    temp[6] = -(rt * vt);
+    temp[7] = (rt * ut * rt * ut - rt * vt * rt * vt);
+    temp[8] = (rt * ut * rt * vt);
+    fp[0] = 0.0;
+    fp[1] = 6.0 * (1.0 - 0.5 * s[1]) * (ut * gx + vt * gy);
+    fp[2] = -(6.0 * (1.0 - 0.5 * s[2]) * (ut * gx + vt * gy));
+    fp[3] = gx;
+    fp[4] = -((1.0 - 0.5 * s[4]) * gx);
+    fp[5] = gy;
+    fp[6] = -((1.0 - 0.5 * s[6]) * gy);
+    fp[7] = 2.0 * (1.0 - 0.5 * s[7]) * (ut * gx - vt * gy);
+    fp[8] = (1.0 - 0.5 * s[8]) * (ut * gy + vt * gx);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) temp[k] = temp1[k] + (temp[k] - temp1[k]) * s[k] + fp[k];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) sum = sum + d.minv[r * 9 + q] * temp[q];
+        d.gB[r * d.plane + p] = (float)(sum - weight(r));
+    }
+    if (FIELDS && d.fo_rho) {
+        d.fo_rho[p] = rt;
+        d.fo_u[p] = ut;
+        d.fo_v[p] = vt;
+    }
+}
+
+// Fused path, after the spread, one thread per band node: du back to FP64,
+// rho and u* from the pulled distributions (the values the rhs used), the
+// node's re-collision, and the block's partial force and moment sums per
+// wing (as ibm_finish_kernel).  The last block to finish (a device-wide
+// counter per episode) reduces the partials in block order, writes the
+// force row and sums (force_row_body) and advances the cycle counter, so
+// the chain ends in this one kernel.
+template <bool FIELDS>
+__device__ __forceinline__ void ibm_close_body(const DevState& d, const int bid_) {
+    constexpr int NWARP = FINISH_THREADS / 32;
+    __shared__ double red[NWARP][3];
+    __shared__ int last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nb = d.band_n[0];
+    const int b = bid_ * FINISH_THREADS + tid;
+    const int e = spread_exponent(d);
+    double t1 = 0.0, t2 = 0.0;
+    int myw = -1;
+    double x0 = 0.0, y0 = 0.0;
+    if (b < nb) {
+        const double du = ldexp((double)reinterpret_cast<long long*>(d.band_du)[b], -e);
+        const double dv = ldexp((double)reinterpret_cast<long long*>(d.band_dv)[b], -e);
+        d.band_du[b] = du;
+        d.band_dv[b] = dv;
+        const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
+        const long long p = pidx(d, i, j);
+        double f[9], rh, us, vs;
+        pulled_moments(d, p, f, rh, us, vs);
+        t1 = 2.0 * rh * du;
+        t2 = 2.0 * rh * dv;
+        if (i != 0 && j != 0 && i != d.nx - 1 && j != d.ny - 1) band_recollide<FIELDS>(d, p, f, rh, us + du, vs + dv, t1, t2);
+        myw = d.band_wing[b];
+        const WingMotion m = d.wm[myw];
+        const double xw = d.xc + d.wing_x_origin + (double)myw * d.wing_x_spacing + m.sa;
+        const double yw = d.yc + d.wing_y_origin + m.sb;
+        x0 = (d.ox + d.scale * (double)i - xw) / d.scale - m.extra_pos;
+        y0 = (d.oy + d.scale * (double)j - yw) / d.scale;
+    }
+    const int b0 = bid_ * FINISH_THREADS;
+    const int b1 = min(nb, b0 + FINISH_THREADS) - 1;
+    const int wlo = b0 < nb ? d.band_wing[b0] : 0, whi = b0 < nb ? d.band_wing[b1] : -1;
+    for (int w = 0; w < d.wing_count; ++w) {
+        double* out = d.force_part + ((long long)bid_ * d.wing_count + w) * 3;
+        if (w < wlo || w > whi) {
+            if (tid < 3) out[tid] = 0.0;
+            continue;
+        }
+        double fx = 0.0, fy = 0.0, mz = 0.0;
+        if (myw == w) {
+            fx = -t1;
+            fy = -t2;
+            mz = -x0 * t2 + y0 * t1;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            fx += __shfl_down_sync(0xffffffffu, fx, o);
+            fy += __shfl_down_sync(0xffffffffu, fy, o);
+            mz += __shfl_down_sync(0xffffffffu, mz, o);
+        }
+        if (lane == 0) { red[warp][0] = fx; red[warp][1] = fy; red[warp][2] = mz; }
+        __syncthreads();
+        if (tid < 3) {
+            double v = 0.0;
+            for (int k = 0; k < NWARP; ++k) v += red[k][tid];
+            out[tid] = v;
+        }
+        __syncthreads();
+    }
+    // the last block of the episode closes the step
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(d.fin_count, 1) == ibm_finish_blocks_dev(d) - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    force_row_body(d);
+    __syncthreads();
+    if (tid == 0) {
+        *d.fin_count = 0;
+        *d.cycle += 1;
+        *d.row_index += 1;
+    }
+}
+template <bool FIELDS>
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_close_kernel(DevState d) { ibm_close_body<FIELDS>(d, blockIdx.x); }
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_close_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
-    step_advance_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+    const DevState& d = *m.ds[e];
+    if (d.write_fields)
+        ibm_close_body<true>(d, blockIdx.x - __ldg(m.boff + e));
+    else
+        ibm_close_body<false>(d, blockIdx.x - __ldg(m.boff + e));
 }
 
 // ------------------------------------------------------------ host side
@@ -703,29 +914,35 @@ void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
 }
 
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
-    if (fused)
-        ibm_ustar_kernel<true><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
-    else
-        ibm_ustar_kernel<false><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
+    if (fused) {
+        ibm_rhs_fused_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
+        return;
+    }
+    ibm_ustar_kernel<false><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
     ibm_rhs_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
 }
 
-void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st) {
+void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st) {
     launch_ibm_substitution(d, (size_t)d.solve_smem, st);
     ibm_spread_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
     const int nbk = ibm_finish_blocks(d);
-    if (fused)
-        ibm_finish_kernel<true><<<nbk, FINISH_THREADS, 0, st>>>(d);
-    else
-        ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
+    if (fused) {
+        if (fields)
+            ibm_close_kernel<true><<<nbk, FINISH_THREADS, 0, st>>>(d);
+        else
+            ibm_close_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
+        return;
+    }
+    ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
     ibm_forces_kernel<<<1, 256, 0, st>>>(d);
 }
 
 void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kernel<<<1, 32, 0, st>>>(d); }
 
 // ------------------------------------------------------------ packed launches
-// (fused path: u* from the pulled distributions, velocity correction of the
-// band re-collision)
+// (fused path: u* in the rhs from the pulled distributions; the closing
+// kernel re-collides the band nodes, writes the force row and advances the
+// cycle)
 int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_GEOMETRY: return blocks(std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap), 128);
@@ -734,12 +951,9 @@ int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     case MK_SCAN: return 1;
     case MK_LIST: return blocks(d.nseg, 64);
     case MK_ASSEMBLE: return blocks(d.lband_total, 256);
-    case MK_USTAR: return blocks(d.band_cap, 128);
     case MK_RHS: return blocks(32LL * d.nseg, 128);
     case MK_SPREAD: return blocks((long long)d.nseg * BOX_SLOTS, 256);
     case MK_FINISH: return ibm_finish_blocks(d);
-    case MK_FORCES: return 1;
-    case MK_ADVANCE: return 1;
     default: return -1;
     }
 }
@@ -752,12 +966,9 @@ bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st
     case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
     case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
     case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_USTAR: ibm_ustar_kernel_multi<true><<<nb, 128, 0, st>>>(m); return true;
-    case MK_RHS: ibm_rhs_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
+    case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_FINISH: ibm_finish_kernel_multi<true><<<nb, FINISH_THREADS, 0, st>>>(m); return true;
-    case MK_FORCES: ibm_forces_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_ADVANCE: step_advance_kernel_multi<<<nb, 32, 0, st>>>(m); return true;
+    case MK_FINISH: ibm_close_kernel_multi<<<nb, FINISH_THREADS, 0, st>>>(m); return true;
     default: return false;
     }
 }

@@ -184,73 +184,6 @@ __global__ void __launch_bounds__(BULK_TX, 8) fused_bulk_kernel_multi(MultiArgs 
         fused_bulk_runs<false>(a);
 }
 
-// Band nodes: FP64 re-collision with the corrected velocity u* + du and the
-// body force 2 rho du (solution.f90:599-655 with boundary_condition.f90:1645-1659).
-template <bool FIELDS>
-__device__ __forceinline__ void fused_band_kernel_body(const DevState& d, const int bid_) {
-    const int b = bid_ * blockDim.x + threadIdx.x;
-    if (b >= d.band_n[0]) return;
-    const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
-    if (i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1) return;
-    const long long p = pidx(d, i, j);
-    double f[9], temp[9], temp1[9], fp[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
-#pragma unroll
-    for (int r = 0; r < 9; ++r) {
-        double sum = 0.0;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) sum = sum + (double)mrt_m(r, q) * f[q];
-        temp1[r] = sum;
-    }
-    const double rt = d.band_rho[b];
-    const double ut = d.band_us[b] + d.band_du[b], vt = d.band_vs[b] + d.band_dv[b];
-    const double gx = 2.0 * rt * d.band_du[b], gy = 2.0 * rt * d.band_dv[b];
-    const double* s = d.s;
-    temp[0] = 0.0;
-    temp[1] = -(2.0 * rt) + 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
-    temp[2] = rt - 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
-    temp[3] = 0.0;
-    temp[4] = -(rt * ut);
-    temp[5] = 0.0;
-    temp[6] = -(rt * vt);
-    temp[7] = (rt * ut * rt * ut - rt * vt * rt * vt);
-    temp[8] = (rt * ut * rt * vt);
-    fp[0] = 0.0;
-    fp[1] = 6.0 * (1.0 - 0.5 * s[1]) * (ut * gx + vt * gy);
-    fp[2] = -(6.0 * (1.0 - 0.5 * s[2]) * (ut * gx + vt * gy));
-    fp[3] = gx;
-    fp[4] = -((1.0 - 0.5 * s[4]) * gx);
-    fp[5] = gy;
-    fp[6] = -((1.0 - 0.5 * s[6]) * gy);
-    fp[7] = 2.0 * (1.0 - 0.5 * s[7]) * (ut * gx - vt * gy);
-    fp[8] = (1.0 - 0.5 * s[8]) * (ut * gy + vt * gx);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) temp[k] = temp1[k] + (temp[k] - temp1[k]) * s[k] + fp[k];
-#pragma unroll
-    for (int r = 0; r < 9; ++r) {
-        double sum = 0.0;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) sum = sum + d.minv[r * 9 + q] * temp[q];
-        d.gB[r * d.plane + p] = (float)(sum - weight(r));
-    }
-    if (FIELDS && d.fo_rho) {
-        d.fo_rho[p] = rt;
-        d.fo_u[p] = ut;
-        d.fo_v[p] = vt;
-    }
-}
-template <bool FIELDS>
-__global__ void fused_band_kernel(DevState d) { fused_band_kernel_body<FIELDS>(d, blockIdx.x); }
-__global__ void fused_band_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    const DevState& d = *m.ds[e];
-    if (d.write_fields)
-        fused_band_kernel_body<true>(d, blockIdx.x - __ldg(m.boff + e));
-    else
-        fused_band_kernel_body<false>(d, blockIdx.x - __ldg(m.boff + e));
-}
-
 // Initial state (solution.f90:44-61): f = f0 = feq(1, UU, 0) on every node,
 // both copies of the planes and the border f0 store.
 __global__ void fused_init_kernel(DevState d) {
@@ -485,13 +418,6 @@ void launch_fused_bc(const DevState& d, cudaStream_t st) {
     fused_bc_kernel<<<(n + 63) / 64, 64, 0, st>>>(d);
 }
 
-void launch_fused_band(const DevState& d, bool fields, cudaStream_t st) {
-    const int n = d.band_cap;
-    if (fields)
-        fused_band_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(d);
-    else
-        fused_band_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(d);
-}
 void launch_fused_init(const DevState& d, cudaStream_t st) { fused_init_kernel<<<1184, 256, 0, st>>>(d); }
 void launch_fused_shift(const DevState& d, int dr, cudaStream_t st) { fused_shift_kernel<<<1184, 256, 0, st>>>(d, dr); }
 void launch_fused_export(const DevState& d, const float* g, double* f, cudaStream_t st) {
@@ -508,7 +434,6 @@ int multi_blocks_fused(MultiKernel k, const DevState& d) {
         const long long runs = ((long long)(d.nx - 2) * (d.ny - 2) + BULK_TX - 1) / BULK_TX;
         return (int)((runs + BULK_MULTI_RUNS - 1) / BULK_MULTI_RUNS);
     }
-    case MK_BAND: return (d.band_cap + 127) / 128;
     case MK_BC: return (2 * (d.ny - 2) + 2 * d.nx + 63) / 64;
     default: return -1;
     }
@@ -517,7 +442,6 @@ int multi_blocks_fused(MultiKernel k, const DevState& d) {
 bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st) {
     switch (k) {
     case MK_BULK: fused_bulk_kernel_multi<<<blocks, BULK_TX, 0, st>>>(m); return true;
-    case MK_BAND: fused_band_kernel_multi<<<blocks, 128, 0, st>>>(m); return true;
     case MK_BC: fused_bc_kernel_multi<<<blocks, 64, 0, st>>>(m); return true;
     default: return false;
     }

@@ -383,6 +383,8 @@ int init_state(LbmHandle* h) {
     CK(cudaMemset(d.rel_pos, 0, sizeof(double) * std::max(1, d.wing_count)));
     long long one = 1;
     CK(cudaMemcpy(d.cycle, &one, sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.gcycle, &one, sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.fin_count, 0, sizeof(int)));
     h->d.movenum = 0;
     h->fields_valid = false;
     h->err_valid = false;
@@ -465,7 +467,6 @@ void prime_geometry(LbmHandle* h, int64_t n_steps) {
     for (int a = 0; a < GEO_AHEAD && a < n_steps; ++a) {
         DevState d = current(h);
         use_geo(d, h->geo[(h->gset + a) % GEO_SETS]);
-        d.cycle_ahead = a;
         launch_ibm_band(d, h->s_main, nullptr);
         launch_ibm_factor(d, h->factor_smem, h->s_main);
     }
@@ -496,7 +497,7 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         {
             PhaseMark pm(h, 4, h->s_main);
             launch_ibm_rhs(d, false, h->s_main);
-            launch_ibm_solve(d, false, h->s_main);
+            launch_ibm_solve(d, false, false, h->s_main);
         }
         {
             PhaseMark pm(h, 1, h->s_main);
@@ -519,7 +520,6 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         const int sn = (h->gset + GEO_AHEAD) % GEO_SETS, s1 = (h->gset + 1) % GEO_SETS;
         DevState dn = d;
         use_geo(dn, h->geo[sn]);
-        dn.cycle_ahead = GEO_AHEAD;
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
         cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
@@ -545,21 +545,13 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         }
         cudaEventRecord(h->ev_bc, h->s_bc);
         {
+            // rhs, substitution, spread, then one closing kernel: band nodes
+            // re-collided (the bulk kernel leaves them out), force row, cycle
+            // advance
             PhaseMark pm(h, 4, h->s_ibm);
             launch_ibm_rhs(d, true, h->s_ibm);
-            launch_ibm_solve(d, true, h->s_ibm);
+            launch_ibm_solve(d, true, fields, h->s_ibm);
         }
-        {
-            // band nodes: the bulk kernel leaves them out, so their
-            // re-collision runs beside it
-            PhaseMark pm(h, 2, h->s_ibm);
-            launch_fused_band(d, fields, h->s_ibm);
-        }
-        // the cycle counter advances once the force row is written and the
-        // geometry kernel of the set built now has read it, off the bulk
-        // kernel's critical path
-        if (prefetch) cudaStreamWaitEvent(h->s_ibm, h->ev_geom[h->parity], 0);
-        launch_step_advance(d, h->s_ibm);
         cudaEventRecord(h->ev_ibm, h->s_ibm);
         {
             PhaseMark pm(h, 1, h->s_main);
@@ -674,7 +666,6 @@ void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out
         d.gA = h->planes[p];
         d.gB = h->planes[1 - p];
         use_geo(d, h->geo[g]);
-        d.cycle_ahead = 0;
         d.diag = 0;
         d.write_fields = 0;
         out[BV_PLAIN + ph] = d;
@@ -691,7 +682,6 @@ void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out
         out[BV_LAST + ph] = l;
         DevState a = d;
         use_geo(a, h->geo[(g + GEO_AHEAD) % GEO_SETS]);
-        a.cycle_ahead = GEO_AHEAD;
         out[BV_AHEAD + ph] = a;
     }
 }
@@ -842,6 +832,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &diofs, wz) ||
         dalloc(h, &d.linv, (size_t)std::max<long long>(1, itot)) || dalloc(h, &d.wm, wz) ||
         dalloc(h, &d.rel_pos, wz) || dalloc(h, &d.cycle, 1) || dalloc(h, &d.row_index, 1) ||
+        dalloc(h, &d.gcycle, 1) || dalloc(h, &d.fin_count, 1) ||
         dalloc(h, &d.sum_row, (size_t)h->row_len) || dalloc(h, &d.sample_count, 1) || dalloc(h, &d.status, 1) ||
         dalloc(h, &d.wing_fm, 3 * wz) || dalloc(h, &d.ibm_resid, 2) || dalloc(h, &d.stream_start, (size_t)d.ncol) ||
         dalloc(h, &d.stream_target, (size_t)d.ncol))
@@ -1021,6 +1012,7 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     if (ensure_rows(h, n_steps)) return -1;
     long long init[2] = {(long long)first_cycle, 0};
     CK(cudaMemcpyAsync(h->d.cycle, &init[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
+    CK(cudaMemcpyAsync(h->d.gcycle, &init[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
     CK(cudaMemcpyAsync(h->d.row_index, &init[1], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
     CK(cudaStreamSynchronize(h->s_main));
     const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
@@ -1219,8 +1211,9 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     cudaStream_t sm = b->s_main;
     BCK(cudaMemcpyAsync(b->d_buf, b->h_buf, total, cudaMemcpyHostToDevice, sm));
     for (int i = 0; i < nh; ++i) {
-        BCK(cudaMemcpyAsync(hs[i]->d.cycle, b->d_buf + off_cyc + (size_t)i * sizeof(long long), sizeof(long long),
-                            cudaMemcpyDeviceToDevice, sm));
+        for (long long* c : {hs[i]->d.cycle, hs[i]->d.gcycle})
+            BCK(cudaMemcpyAsync(c, b->d_buf + off_cyc + (size_t)i * sizeof(long long), sizeof(long long),
+                                cudaMemcpyDeviceToDevice, sm));
         BCK(cudaMemsetAsync(hs[i]->d.row_index, 0, sizeof(long long), sm));
     }
     auto launch = [&](MultiKernel k, size_t at, int ne, cudaStream_t st) {
@@ -1256,13 +1249,8 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         }
         launch(MK_BC, t.cur, t.a_cur, b->s_bc);
         cudaEventRecord(b->ev_bc, b->s_bc);
-        for (MultiKernel k2 :
-             {MK_USTAR, MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH, MK_BAND, MK_FORCES})
+        for (MultiKernel k2 : {MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
             launch(k2, t.cur, t.a_cur, b->s_ibm);
-        // the cycle counters advance after the force rows and after the
-        // geometry kernel of the next step has read them
-        if (t.a_ahead) cudaStreamWaitEvent(b->s_ibm, b->ev_geom, 0);
-        launch(MK_ADVANCE, t.cur, t.a_cur, b->s_ibm);
         cudaEventRecord(b->ev_ibm, b->s_ibm);
         launch(MK_BULK, t.cur, t.a_cur, b->s_bulk);
         cudaEventRecord(b->ev_bulk, b->s_bulk);

@@ -162,7 +162,8 @@ struct DevState {
     double *rel_pos;             // W
     // step bookkeeping
     long long* cycle;            // device copy of the current cycle number
-    int cycle_ahead;             // the geometry kernels work for cycle + cycle_ahead
+    long long* gcycle;           // cycle of the next geometry to build (advanced by the band list kernel)
+    int* fin_count;              // fused path: blocks of the closing kernel done this step
     double* force_rows;          // rows of 4 + 12 W, indexed by step within segment
     long long* row_index;        // step within segment
     int force_rows_cap;

@@ -21,7 +21,6 @@ FusedConsts fused_consts(const DevState& d);
 void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st);
 bool is_bulk_kernel(const void* func);   // the bulk kernel (low priority in graphs)
 bool is_far_field_kernel(const void* func);
-void launch_fused_band(const DevState& d, bool fields, cudaStream_t st);
 void launch_fused_bc(const DevState& d, cudaStream_t st);   // far field of the fused path
 void launch_fused_init(const DevState& d, cudaStream_t st);
 void launch_fused_shift(const DevState& d, int dr, cudaStream_t st);
@@ -36,8 +35,10 @@ void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_do
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st);
 // u*, right-hand side (needs the band list; on the plain path also the moments)
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st);
-// substitution, spread, velocity correction, forces (needs rhs and factor)
-void launch_ibm_solve(const DevState& d, bool fused, cudaStream_t st);
+// substitution, spread, velocity correction, forces (needs rhs and factor);
+// on the fused path also the band nodes' re-collision (fields: write rho,
+// u, v there) and the cycle advance
+void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st);
 int ibm_finish_blocks(const DevState& d);
 // kernels of a step's geometry (motion through factorisation)
 bool is_geometry_kernel(const void* func);
@@ -76,12 +77,12 @@ void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle +=
 // Packed launches: one grid covers the blocks of several episodes, block b
 // running the kernel of episode e = max{e : boff[e] <= b} with local block
 // index b - boff[e] (multi.cuh).  The fused path's kernels only; the bulk
-// and band kernels take the field flag from each episode's state.
+// and closing kernels take the field flag from each episode's state.
 enum MultiKernel : int {
     MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
-    MK_USTAR, MK_RHS, MK_SPREAD, MK_FINISH, MK_FORCES, MK_ADVANCE,     // immersed boundary
+    MK_RHS, MK_SPREAD, MK_FINISH,                                      // immersed boundary
     MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
-    MK_BULK, MK_BAND, MK_BC,                                            // lattice
+    MK_BULK, MK_BC,                                                     // lattice
     MK_KINDS
 };
 struct MultiArgs {
