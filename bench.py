@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    p.add_argument("--workload", default="4000x2000", choices=["800x400", "4000x2000"])
+    p.add_argument("--workload", default="4000x2000", choices=["800x400", "4000x2000", "16000x8000"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the batched and served measurements")
     return p.parse_args()
@@ -63,7 +63,11 @@ def parse():
 
 def workload(name, steps):
     from lbm_mutiwing_b200 import workloads as wl
-    return wl.tandem_800x400(steps=steps) if name == "800x400" else wl.tandem_4000x2000(steps=steps)
+    if name == "800x400":
+        return wl.tandem_800x400(steps=steps)
+    if name == "16000x8000":
+        return wl.formation_16000x8000(steps=steps)
+    return wl.tandem_4000x2000(steps=steps)
 
 
 class Clocks:

@@ -27,6 +27,8 @@ MOTION_STREAM = 2
 STEP_FIELDS = 1
 STEP_ERR = 2
 FLAG_NO_GRAPHS = 1
+FLAG_SOLVE_STREAM = 2
+FLAG_NO_GRAPHS = 1
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}
@@ -117,9 +119,10 @@ def default_s() -> list:
 
 
 def make_config(ep, precision: int = PRECISION_FP64, motion_source: int = MOTION_FILE,
-                device: int = 0, s: Optional[Sequence[float]] = None, graphs: bool = True) -> LbmConfig:
+                device: int = 0, s: Optional[Sequence[float]] = None, graphs: bool = True,
+                flags: int = 0) -> LbmConfig:
     cfg = LbmConfig()
-    cfg.flags = 0 if graphs else FLAG_NO_GRAPHS
+    cfg.flags = (0 if graphs else FLAG_NO_GRAPHS) | flags
     cfg.nx, cfg.ny = ep.nx, ep.ny
     cfg.scale, cfg.uu, cfg.re = ep.scale, ep.uu, ep.re
     cfg.ox, cfg.oy = ep.ox, ep.oy
@@ -140,10 +143,10 @@ class Simulation:
 
     def __init__(self, ep, precision: int = PRECISION_FP64, motion_source: int = MOTION_FILE,
                  device: int = 0, s: Optional[Sequence[float]] = None, load_motion: bool = True,
-                 graphs: bool = True):
+                 graphs: bool = True, flags: int = 0):
         self.L = load_library()
         self.ep = ep
-        self.cfg = make_config(ep, precision, motion_source, device, s, graphs)
+        self.cfg = make_config(ep, precision, motion_source, device, s, graphs, flags)
         self.nx, self.ny, self.W = ep.nx, ep.ny, ep.wing_count
         self.precision = precision
         self.row_len = 4 + 12 * self.W

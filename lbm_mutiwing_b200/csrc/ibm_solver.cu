@@ -293,17 +293,34 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel_multi(MultiA
     ibm_factor_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
+// Streaming of a wing's factor through shared memory when it does not fit
+// whole: chunks of RING_ROWS consecutive rows (contiguous in global memory)
+// are brought in by bulk copies into a ring of slots, each slot led by a
+// zero row (the forward pass reads a little above the diagonal, which the
+// banded layout keeps at zero in the previous row).  The forward pass needs
+// the bw rows below the current panel, the backward pass the panel's own
+// rows; the next chunk is in flight while the current ones are used.
+constexpr int RING_ROWS = 16;
+constexpr int RING_MAX_SLOTS = 16;
+static_assert(RING_ROWS % PANEL == 0, "a panel's rows lie in one chunk");
+__host__ __device__ inline int ring_slots(int bw) { return (bw + PANEL + RING_ROWS - 1) / RING_ROWS + 2; }
+size_t ibm_solve_ring_bytes(int bw) { return (size_t)ring_slots(bw) * (RING_ROWS + 1) * ibm_ld(bw) * sizeof(double); }
+bool ibm_solve_ring_fits(int bw) { return ring_slots(bw) <= RING_MAX_SLOTS; }
+
 // Forward and backward substitution with the factor of wing w: warp 0 solves
 // for the x component, warp 1 for the y component, on shared-memory copies
-// of the per-panel inverses and pivots, of the factor (when it fits) and of
-// the right-hand sides.  Shared memory: [2 right-hand sides with zero tails]
-// [permutation][per-panel inverse blocks and pivots][factor].  Each lane
-// updates rows lane and lane + 32 below or above a panel (bw <= 64) or loops.
-// SMEM: the factor is copied to shared memory.
+// of the per-panel inverses and pivots, of the factor (whole when it fits,
+// else streamed through a ring of rows, else read from global memory) and
+// of the right-hand sides.  Shared memory: [2 right-hand sides with zero
+// tails][permutation][per-panel inverse blocks and pivots][factor or ring].
+// Each lane updates rows lane and lane + 32 below or above a panel
+// (bw <= 64) or loops.  SMEM: the factor is copied to shared memory whole.
 template <bool SMEM>
 __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const int bid_) {
     extern __shared__ __align__(16) double sm[];
     __shared__ uint64_t bar;
+    __shared__ uint64_t sbar[RING_MAX_SLOTS];
+    __shared__ uint32_t suse[RING_MAX_SLOTS];
     const int w = bid_;
     const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
     const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
@@ -336,9 +353,58 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
     }
     const double* A = (SMEM ? Sm : gS) + ld;   // row 0
     const int li = lane & (PANEL - 1);
+    // the streamed form (not SMEM, the ring fits)
+    const bool stream = !SMEM && d.solve_stream;
+    const int NB = ring_slots(bw), nrows = nw + PANEL + bw;
+    const int nq = (nrows + RING_ROWS - 1) / RING_ROWS;
+    double* ring = Sm;
+    auto rowp = [&](int i) -> const double* {   // row i (entry 0 = the diagonal)
+        if (!stream) return A + (long long)i * ld;
+        const int q = i / RING_ROWS;
+        return ring + ((q % NB) * (RING_ROWS + 1) + 1 + (i - q * RING_ROWS)) * ld;
+    };
+    auto issue = [&](int q) {   // thread 0: chunk q into its slot
+        const int s = q % NB;
+        const int rows = min(RING_ROWS, nrows - q * RING_ROWS);
+        const uint32_t bytes = (uint32_t)rows * ld * 8;
+        fence_async_smem();
+        mbar_arrive_expect_tx(&sbar[s], bytes);
+        bulk_load_all(ring + (s * (RING_ROWS + 1) + 1) * ld, gS + (1 + (long long)q * RING_ROWS) * ld, bytes, &sbar[s]);
+        suse[s] += 1;
+    };
+    auto wait_chunk = [&](int q) { return mbar_wait(&sbar[q % NB], (suse[q % NB] - 1) & 1); };
+    auto drain = [&]() {   // every issued copy complete (bounded)
+        bool all = true;
+        for (int s = 0; s < NB; ++s)
+            if (suse[s]) all &= mbar_wait(&sbar[s], (suse[s] - 1) & 1);
+        return all;
+    };
+    int qi = 0;   // next chunk to issue (thread 0)
+    if (stream) {
+        for (int t = tid; t < NB * ld; t += SOLVE_THREADS) ring[(t / ld) * (RING_ROWS + 1) * ld + t % ld] = 0.0;
+        if (tid < NB) {
+            mbar_init(&sbar[tid], 1);
+            suse[tid] = 0;
+        }
+        __syncthreads();
+    }
     // L' D v = r: per panel w_p = Li_p z_p, v_p = w_p / d, rows below -= L' w_p
     for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {
         const int np = min(PANEL, nw - k0);
+        if (stream) {   // rows k0 + np .. k0 + np + bw - 1 resident, the next chunk in flight
+            const int lo = (k0 + np) / RING_ROWS, hi = min(nq - 1, (k0 + np + bw - 1) / RING_ROWS);
+            __syncthreads();
+            if (tid == 0)
+                for (; qi < nq && qi <= hi + 1 && qi - NB < lo; ++qi) issue(qi);
+            __syncthreads();
+            bool ok = true;
+            for (int q = lo; q <= hi; ++q) ok &= wait_chunk(q);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+                drain();
+                return;
+            }
+        }
         const double* Li = Lsh + pan * IBM_PANEL_AUX;
         double zk[PANEL], lk[PANEL];
 #pragma unroll
@@ -362,7 +428,7 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
             for (int h = 0; h < 2; ++h) {
                 const int rb = min(rb0 + lane + 32 * h, bw - 1);
                 const int i = k0 + np + rb;
-                const double* row = A + i * ld + (i - k0);
+                const double* row = rowp(i) + (i - k0);
                 double a0 = 0.0, a1 = 0.0;
 #pragma unroll
                 for (int c = 0; c < PANEL / 2; ++c) {
@@ -381,8 +447,30 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
         __syncwarp();
     }
     // L'^T y = v: per panel (last first) y_p = Li_p^T v_p, rows above -= L'^T y_p
+    int qb = (npan - 1) * PANEL / RING_ROWS;   // next chunk to issue, downwards (thread 0)
+    if (stream) {   // no copy of the forward pass still in flight
+        const bool ok = drain();
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+            drain();
+            return;
+        }
+    }
     for (int pan = npan - 1; pan >= 0; --pan) {
         const int k0 = pan * PANEL;
+        if (stream) {   // the panel's rows (one chunk) resident, the chunk below in flight
+            const int c = k0 / RING_ROWS;
+            __syncthreads();
+            if (tid == 0)
+                for (; qb >= 0 && qb >= c - 1 && qb + NB > c; --qb) issue(qb);
+            __syncthreads();
+            const bool ok = wait_chunk(c);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+                drain();
+                return;
+            }
+        }
         const double* Li = Lsh + pan * IBM_PANEL_AUX;
         double vk[PANEL], lk[PANEL];
 #pragma unroll
@@ -407,7 +495,7 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
             for (int h = 0; h < 2; ++h) {
                 const int r = min(r0 + lane + 32 * h, above - 1);
                 const int j = k0 - 1 - r;
-                const double* col = A + k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+                const double* col = rowp(k0) + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
                 double a0 = 0.0, a1 = 0.0;
 #pragma unroll
                 for (int c = 0; c < PANEL / 2; ++c) {
@@ -425,6 +513,7 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
         if (lane < PANEL) z[k0 + lane] = yl;
         __syncwarp();
     }
+    if (stream && !drain() && lane == 0) solver_status(d, ST_COPY_TIMEOUT);
     double ym = 0.0;
 #pragma unroll 4
     for (int p = lane; p < nw; p += 32) {

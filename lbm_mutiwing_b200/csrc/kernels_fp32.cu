@@ -45,6 +45,9 @@ FusedConsts fused_consts(const DevState& d) {
 // the single-episode step the early test is faster overall: the bulk kernel
 // then draws a little less bandwidth from the concurrent immersed-boundary
 // chain, which is as long as the bulk kernel at 4001 x 2001.
+#ifndef BULK_EARLY_BAND_TEST
+#define BULK_EARLY_BAND_TEST 1
+#endif
 template <bool FIELDS, bool EARLY>
 __device__ __forceinline__ void fused_bulk_node(const float* __restrict__ gA, float* __restrict__ gB, int pitch,
                                                 long long plane, const FusedConsts& c, double* __restrict__ fo_rho,
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
     for (int r = 0; r < BULK_ROWS; ++r) {
         const int j = j0 + r;
         if (j > ny - 2) break;
-        fused_bulk_node<FIELDS, true>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
+        fused_bulk_node<FIELDS, BULK_EARLY_BAND_TEST != 0>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
     }
 }
 // Packed form: an episode's interior nodes, row by row without the border

@@ -879,8 +879,12 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     // substitution: the wing's factor goes to shared memory when it fits
     if (ibm_solve_smem(nwmax, bwmax, wmax, false) > smem_cap)
         return fail(h, "immersed boundary: too many segments for one substitution block");
-    d.solve_in_smem = ibm_solve_smem(nwmax, bwmax, wmax, true) <= smem_cap ? 1 : 0;
+    d.solve_in_smem = ibm_solve_smem(nwmax, bwmax, wmax, true) <= smem_cap && !(c.flags & LBM_FLAG_SOLVE_STREAM);
     d.solve_smem = (long long)ibm_solve_smem(nwmax, bwmax, wmax, d.solve_in_smem != 0);
+    // else a ring of factor rows when it fits (wings of many markers)
+    d.solve_stream = !d.solve_in_smem && ibm_solve_ring_fits(bwmax) &&
+                     ibm_solve_smem(nwmax, bwmax, wmax, false) + ibm_solve_ring_bytes(bwmax) <= smem_cap;
+    if (d.solve_stream) d.solve_smem += (long long)ibm_solve_ring_bytes(bwmax);
     CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))

@@ -146,6 +146,7 @@ struct DevState {
     double* linv;                // inverses of the factor's diagonal blocks, per wing and panel
     const long long* wing_linv_ofs;  // W offsets into linv
     int solve_in_smem;           // the substitution copies the wing's factor to shared memory
+    int solve_stream;            // otherwise it streams the factor through a ring of rows in shared memory
     long long solve_smem;        // dynamic shared memory of the substitution kernel (bytes)
     // configuration of wing placement
     double wing_x_origin, wing_x_spacing, wing_y_origin, xc, yc;

@@ -47,6 +47,10 @@ bool is_factor_kernel(const void* func);
 cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem);
 // dynamic shared memory of the substitution kernel
 size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool factor_in_smem);
+// shared memory of the row ring when the factor is streamed, and whether
+// its slot count is within the kernel's barrier table
+size_t ibm_solve_ring_bytes(int bw);
+bool ibm_solve_ring_fits(int bw);
 // shared memory of the factorisation kernel ahead of the wing's storage
 // (a multiple of 16 bytes)
 size_t ibm_factor_staging_bytes(int bw_max);

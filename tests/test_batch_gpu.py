@@ -100,3 +100,24 @@ def test_batch_rejects_bad_input(gpu_lib):
         before = s.f()
         batch.step([s], 0)
         _same(before, s.f())
+
+
+def test_streamed_substitution_matches_whole_factor(gpu_lib):
+    """The substitution streaming each wing's factor through a ring of rows
+    in shared memory (the form wings too large for shared memory take) gives
+    the same bits as the substitution on the whole factor; run alone and
+    packed."""
+    ep = small("s", 2, (5.0, 2.5), markers=160)
+    ref = api.Simulation(ep, api.PRECISION_FP32)
+    st = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
+    st2 = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
+    try:
+        rows_ref = ref.step(12)
+        _same(rows_ref, st.step(12))
+        _same(ref.f(), st.f())
+        with api.Batch(0) as batch:
+            _same(rows_ref, batch.step([st2], 12)[0])
+        _same(ref.f(), st2.f())
+    finally:
+        for s_ in (ref, st, st2):
+            s_.close()
