@@ -56,6 +56,22 @@ constexpr int BORDER_GAP = 3;           // support boxes keep this many nodes of
 
 __device__ inline void set_status(const DevState& d, int bit) { atomicOr(d.status, bit); }
 
+// Grids.  The per-slot kernels (claims, spread) and the assembly of G loop
+// over d.slot_items items per thread, and the motion kernel clears the
+// previous band in a loop.  One episode uses one item per thread (its
+// latency-bound chains want the most threads); packed batches use several,
+// so a step dispatches a few thousand blocks of immersed-boundary work
+// instead of tens of thousands, which would hold up the bulk kernel's
+// dispatch (they run at higher priority).  Results do not depend on it.
+__host__ __device__ inline int grid_of(long long n, int threads) { return (int)(n <= 0 ? 1 : (n + threads - 1) / threads); }
+__host__ __device__ inline int geometry_grid(const DevState& d) {
+    return grid_of(d.npts > 12 * d.nseg ? d.npts : 12 * d.nseg, 128);
+}
+__host__ __device__ inline int slot_grid(const DevState& d) {
+    return grid_of((long long)d.nseg * BOX_SLOTS, 256 * d.slot_items);
+}
+__host__ __device__ inline int assemble_grid(const DevState& d) { return grid_of(d.lband_total, 256 * d.slot_items); }
+
 // Exactly rounded FP64 steps for the marker and box arithmetic.
 __device__ inline double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ inline double add(double a, double b) { return __dadd_rn(a, b); }
@@ -208,8 +224,9 @@ __device__ __forceinline__ void ibm_geometry_kernel_body(const DevState& d, cons
             (axis == 0 ? d.xb2 : d.yb2)[s] = c2;
         }
     }
-    if (t < d.band_n[0]) {
-        const long long p = pidx(d, d.band_ij[2 * t], d.band_ij[2 * t + 1]);
+    const int nclear = d.band_n[0], stride = geometry_grid(d) * 128;
+    for (int b = t; b < nclear; b += stride) {
+        const long long p = pidx(d, d.band_ij[2 * b], d.band_ij[2 * b + 1]);
         d.band_map[p] = BAND_EMPTY;
         if (d.band_bits) atomicAnd(d.band_bits + (p >> 5), ~(1u << (p & 31)));
         if (d.precision == 0) { d.gfx[p] = 0.0; d.gfy[p] = 0.0; }
@@ -228,12 +245,13 @@ __device__ inline bool box_empty(const DevState& d, int s) {
 
 // claims: lowest segment index wins (airfoil.f90:322-333)
 __device__ __forceinline__ void ibm_claim_kernel_body(const DevState& d, const int bid_) {
-    const int t = bid_ * blockDim.x + threadIdx.x;
-    if (t >= d.nseg * BOX_SLOTS) return;
-    const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
-    if (box_empty(d, s)) return;
-    const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
-    if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
+    const int n = d.nseg * BOX_SLOTS, stride = slot_grid(d) * 256;
+    for (int t = bid_ * 256 + threadIdx.x; t < n; t += stride) {
+        const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+        if (box_empty(d, s)) continue;
+        const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
+        if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
+    }
 }
 __global__ void ibm_claim_kernel(DevState d) { ibm_claim_kernel_body(d, blockIdx.x); }
 __global__ void ibm_claim_kernel_multi(MultiArgs m) {
@@ -519,15 +537,15 @@ __device__ inline double gram(const DevState& d, int a, int c) {
 // wing w starts at lband[lofs_w + (p + 1) * ld]; entry dd holds G(p, p - dd).
 // Every slot of the storage is written, zero zones included.
 __device__ __forceinline__ void ibm_assemble_kernel_body(const DevState& d, const int bid_) {
-    const long long total = d.lband_total;
-    const long long t = bid_ * (long long)blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    int w = 0;
-    while (w + 1 < d.wing_count && t >= d.wing_lofs[w + 1]) ++w;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
-    const long long r = t - d.wing_lofs[w];
-    const int p = (int)(r / ld) - 1, dd = (int)(r % ld), q = p - dd;
-    d.lband[t] = (p >= 0 && p < nw && q >= 0 && dd <= bw) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
+    const long long total = d.lband_total, stride = (long long)assemble_grid(d) * 256;
+    for (long long t = bid_ * 256LL + threadIdx.x; t < total; t += stride) {
+        int w = 0;
+        while (w + 1 < d.wing_count && t >= d.wing_lofs[w + 1]) ++w;
+        const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+        const long long r = t - d.wing_lofs[w];
+        const int p = (int)(r / ld) - 1, dd = (int)(r % ld), q = p - dd;
+        d.lband[t] = (p >= 0 && p < nw && q >= 0 && dd <= bw) ? gram(d, d.perm[s0 + p], d.perm[s0 + q]) : 0.0;
+    }
 }
 __global__ void ibm_assemble_kernel(DevState d) { ibm_assemble_kernel_body(d, blockIdx.x); }
 __global__ void ibm_assemble_kernel_multi(MultiArgs m) {
@@ -554,17 +572,18 @@ __device__ inline int spread_exponent(const DevState& d) {
 // du = X^T y: every (segment, slot) contribution is rounded once to a 64-bit
 // fixed-point number and added with an integer atomic.
 __device__ __forceinline__ void ibm_spread_kernel_body(const DevState& d, const int bid_) {
-    const int t = bid_ * blockDim.x + threadIdx.x;
-    if (t >= d.nseg * BOX_SLOTS) return;
-    const int bi = d.pb[t];
-    if (bi < 0) return;
-    const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+    const int n = d.nseg * BOX_SLOTS, stride = slot_grid(d) * 256;
     const int e = spread_exponent(d);
-    const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
-    atomicAdd(reinterpret_cast<unsigned long long*>(d.band_du) + bi,
-              (unsigned long long)__double2ll_rn(ldexp(wv * d.rx[s], e)));
-    atomicAdd(reinterpret_cast<unsigned long long*>(d.band_dv) + bi,
-              (unsigned long long)__double2ll_rn(ldexp(wv * d.ry[s], e)));
+    for (int t = bid_ * 256 + threadIdx.x; t < n; t += stride) {
+        const int bi = d.pb[t];
+        if (bi < 0) continue;
+        const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+        const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
+        atomicAdd(reinterpret_cast<unsigned long long*>(d.band_du) + bi,
+                  (unsigned long long)__double2ll_rn(ldexp(wv * d.rx[s], e)));
+        atomicAdd(reinterpret_cast<unsigned long long*>(d.band_dv) + bi,
+                  (unsigned long long)__double2ll_rn(ldexp(wv * d.ry[s], e)));
+    }
 }
 __global__ void ibm_spread_kernel(DevState d) { ibm_spread_kernel_body(d, blockIdx.x); }
 __global__ void ibm_spread_kernel_multi(MultiArgs m) {
@@ -898,18 +917,16 @@ bool is_geometry_kernel(const void* func) {
 }
 
 void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done) {
-    const long long n1 = std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap);
-    ibm_geometry_kernel<<<blocks(n1, 128), 128, 0, st>>>(d);
+    ibm_geometry_kernel<<<geometry_grid(d), 128, 0, st>>>(d);
     if (geometry_done) cudaEventRecord(geometry_done, st);
-    ibm_claim_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
+    ibm_claim_kernel<<<slot_grid(d), 256, 0, st>>>(d);
     ibm_count_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
     ibm_scan_kernel<<<1, 1024, 0, st>>>(d);
     ibm_list_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
 }
 
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
-    const long long total = d.lband_total;
-    ibm_assemble_kernel<<<blocks(total, 256), 256, 0, st>>>(d);
+    ibm_assemble_kernel<<<assemble_grid(d), 256, 0, st>>>(d);
     launch_ibm_factor_blocks(d, factor_smem, st);
 }
 
@@ -924,7 +941,7 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
 
 void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st) {
     launch_ibm_substitution(d, (size_t)d.solve_smem, st);
-    ibm_spread_kernel<<<blocks((long long)d.nseg * BOX_SLOTS, 256), 256, 0, st>>>(d);
+    ibm_spread_kernel<<<slot_grid(d), 256, 0, st>>>(d);
     const int nbk = ibm_finish_blocks(d);
     if (fused) {
         if (fields)
@@ -945,14 +962,14 @@ void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kern
 // cycle)
 int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     switch (k) {
-    case MK_GEOMETRY: return blocks(std::max<long long>(std::max(d.npts, 12 * d.nseg), d.band_cap), 128);
-    case MK_CLAIM: return blocks((long long)d.nseg * BOX_SLOTS, 256);
+    case MK_GEOMETRY: return geometry_grid(d);
+    case MK_CLAIM: return slot_grid(d);
     case MK_COUNT: return blocks(d.nseg, 64);
     case MK_SCAN: return 1;
     case MK_LIST: return blocks(d.nseg, 64);
-    case MK_ASSEMBLE: return blocks(d.lband_total, 256);
-    case MK_RHS: return blocks(32LL * d.nseg, 128);
-    case MK_SPREAD: return blocks((long long)d.nseg * BOX_SLOTS, 256);
+    case MK_ASSEMBLE: return assemble_grid(d);
+    case MK_RHS: return blocks(32LL * d.nseg, 256);   // 8 segments per block
+    case MK_SPREAD: return slot_grid(d);
     case MK_FINISH: return ibm_finish_blocks(d);
     default: return -1;
     }
@@ -966,7 +983,7 @@ bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st
     case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
     case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
     case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
+    case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
     case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
     case MK_FINISH: ibm_close_kernel_multi<<<nb, FINISH_THREADS, 0, st>>>(m); return true;
     default: return false;

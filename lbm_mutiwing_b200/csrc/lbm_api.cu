@@ -658,6 +658,7 @@ int multi_blocks(MultiKernel k, const DevState& d) {
 // and the geometry built one step ahead, each for the two plane parities /
 // geometry sets a step can start from.
 constexpr int BV_PLAIN = 0, BV_SECOND_LAST = 2, BV_LAST = 4, BV_AHEAD = 6, BV_COUNT = 8;
+constexpr int BATCH_SLOT_ITEMS = 4;   // per-slot items per thread in packed launches
 
 void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out) {
     for (int ph = 0; ph < 2; ++ph) {
@@ -668,6 +669,7 @@ void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out
         use_geo(d, h->geo[g]);
         d.diag = 0;
         d.write_fields = 0;
+        d.slot_items = BATCH_SLOT_ITEMS;
         out[BV_PLAIN + ph] = d;
         DevState sl = d;
         sl.write_fields = want_err ? 1 : 0;
@@ -809,6 +811,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     if (dalloc(h, &d.band_map, N)) return -1;
     if (c.precision != LBM_PRECISION_FP64 && dalloc(h, &d.band_bits, band_bits_words(d))) return -1;
     d.band_cap = std::max(64, BOX_SLOTS * ns);
+    d.slot_items = 1;
     const int cap = d.band_cap;
     int* band_n = nullptr;
     if (dalloc(h, &band_n, 2) || dalloc(h, &d.band_ij, 2 * (size_t)cap) || dalloc(h, &d.band_wing, cap) ||
@@ -1146,7 +1149,8 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     size_t factor_smem = 0, solve_smem = 0;
     for (int k = 0; k < MK_KINDS; ++k)
         for (int e = 0; e < nh; ++e) {
-            const long long nb = (long long)boff[(size_t)k * (nh + 1) + e] + multi_blocks((MultiKernel)k, hs[order[e]]->d);
+            const long long nb = (long long)boff[(size_t)k * (nh + 1) + e] +
+                                 multi_blocks((MultiKernel)k, var[(size_t)order[e] * BV_COUNT + BV_PLAIN]);
             if (nb > INT32_MAX) return batch_fail(b, "batch too large for one launch");
             boff[(size_t)k * (nh + 1) + e + 1] = (int)nb;
         }

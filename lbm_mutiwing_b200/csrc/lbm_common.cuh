@@ -165,6 +165,7 @@ struct DevState {
     long long* cycle;            // device copy of the current cycle number
     long long* gcycle;           // cycle of the next geometry to build (advanced by the band list kernel)
     int* fin_count;              // fused path: blocks of the closing kernel done this step
+    int slot_items;              // box slots (or G entries) per thread in the per-slot kernels
     double* force_rows;          // rows of 4 + 12 W, indexed by step within segment
     long long* row_index;        // step within segment
     int force_rows_cap;
