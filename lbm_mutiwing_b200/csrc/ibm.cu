@@ -71,6 +71,8 @@ __host__ __device__ inline int slot_grid(const DevState& d) {
     return grid_of((long long)d.nseg * BOX_SLOTS, 256 * d.slot_items);
 }
 __host__ __device__ inline int assemble_grid(const DevState& d) { return grid_of(d.lband_total, 256 * d.slot_items); }
+// rhs: one warp per segment, 128-thread blocks
+__host__ __device__ inline int rhs_grid(const DevState& d) { return grid_of(32LL * d.nseg, 128 * d.slot_items); }
 
 // Exactly rounded FP64 steps for the marker and box arithmetic.
 __device__ inline double mul(double a, double b) { return __dmul_rn(a, b); }
@@ -468,10 +470,7 @@ __device__ __forceinline__ void pulled_moments(const DevState& d, long long p, d
 // Fused path: the rhs with u* evaluated at each box node from the pulled
 // distributions (no separate u* pass), clearing the spread accumulators of
 // the band nodes it meets (every listed node lies in its claimer's box).
-__device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int bid_) {
-    const int s = (bid_ * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (s >= d.nseg) return;
+__device__ __forceinline__ void ibm_rhs_fused_seg(const DevState& d, const int s, const int lane) {
     const int nb = d.band_n[0];
     const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
     double bu = 0.0, bv = 0.0;
@@ -516,6 +515,10 @@ __device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int 
         d.qx[s] = ub - bu;   // kept for the residual diagnostic
         d.qy[s] = vb - bv;
     }
+}
+__device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int bid_) {
+    const int stride = rhs_grid(d) * 4;   // warps of the grid
+    for (int s = (bid_ * 128 + threadIdx.x) >> 5; s < d.nseg; s += stride) ibm_rhs_fused_seg(d, s, threadIdx.x & 31);
 }
 __global__ void ibm_rhs_fused_kernel(DevState d) { ibm_rhs_fused_body(d, blockIdx.x); }
 __global__ void ibm_rhs_fused_kernel_multi(MultiArgs m) {
@@ -817,11 +820,12 @@ __device__ __forceinline__ void band_recollide(const DevState& d, long long p, c
 // counter per episode) reduces the partials in block order, writes the
 // force row and sums (force_row_body) and advances the cycle counter, so
 // the chain ends in this one kernel.
+// Virtual block vb: band nodes vb * 256 .. vb * 256 + 255 and their partial
+// sums (the partition of ibm_finish_kernel whatever the grid).
 template <bool FIELDS>
-__device__ __forceinline__ void ibm_close_body(const DevState& d, const int bid_) {
+__device__ __forceinline__ void ibm_close_vblock(const DevState& d, const int bid_) {
     constexpr int NWARP = FINISH_THREADS / 32;
     __shared__ double red[NWARP][3];
-    __shared__ int last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = d.band_n[0];
     const int b = bid_ * FINISH_THREADS + tid;
@@ -877,10 +881,22 @@ __device__ __forceinline__ void ibm_close_body(const DevState& d, const int bid_
         }
         __syncthreads();
     }
+}
+// A block takes virtual blocks bid, bid + grid, ... (one alone, slot_items
+// in packed launches).
+__host__ __device__ inline int close_grid(const DevState& d) {
+    const int nvb = (int)(d.band_cap > 0 ? (d.band_cap + FINISH_THREADS - 1) / FINISH_THREADS : 1);
+    return (nvb + d.slot_items - 1) / d.slot_items;
+}
+template <bool FIELDS>
+__device__ __forceinline__ void ibm_close_body(const DevState& d, const int bid_) {
+    __shared__ int last;
+    const int tid = threadIdx.x, grid = close_grid(d), nvb = ibm_finish_blocks_dev(d);
+    for (int vb = bid_; vb < nvb; vb += grid) ibm_close_vblock<FIELDS>(d, vb);
     // the last block of the episode closes the step
     __threadfence();
     __syncthreads();
-    if (tid == 0) last = atomicAdd(d.fin_count, 1) == ibm_finish_blocks_dev(d) - 1;
+    if (tid == 0) last = atomicAdd(d.fin_count, 1) == grid - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
@@ -932,7 +948,7 @@ void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
 
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
     if (fused) {
-        ibm_rhs_fused_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
+        ibm_rhs_fused_kernel<<<rhs_grid(d), 128, 0, st>>>(d);
         return;
     }
     ibm_ustar_kernel<false><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
@@ -945,9 +961,9 @@ void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t s
     const int nbk = ibm_finish_blocks(d);
     if (fused) {
         if (fields)
-            ibm_close_kernel<true><<<nbk, FINISH_THREADS, 0, st>>>(d);
+            ibm_close_kernel<true><<<close_grid(d), FINISH_THREADS, 0, st>>>(d);
         else
-            ibm_close_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
+            ibm_close_kernel<false><<<close_grid(d), FINISH_THREADS, 0, st>>>(d);
         return;
     }
     ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
@@ -968,9 +984,9 @@ int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     case MK_SCAN: return 1;
     case MK_LIST: return blocks(d.nseg, 64);
     case MK_ASSEMBLE: return assemble_grid(d);
-    case MK_RHS: return blocks(32LL * d.nseg, 256);   // 8 segments per block
+    case MK_RHS: return rhs_grid(d);
     case MK_SPREAD: return slot_grid(d);
-    case MK_FINISH: return ibm_finish_blocks(d);
+    case MK_FINISH: return close_grid(d);
     default: return -1;
     }
 }
@@ -983,7 +999,7 @@ bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st
     case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
     case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
     case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
     case MK_FINISH: ibm_close_kernel_multi<<<nb, FINISH_THREADS, 0, st>>>(m); return true;
     default: return false;

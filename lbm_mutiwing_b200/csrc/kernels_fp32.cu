@@ -383,9 +383,13 @@ __device__ void far_edge(const DevState& d, int ie, int je, const FarMom& e, con
 // the corners of the top and bottom rows take the LODI state of the column
 // node inside them, as the reference's edge order left -> right -> top ->
 // bottom leaves it.
-__device__ __forceinline__ void fused_bc_kernel_body(const DevState& d, const int bid_) {
+// border nodes per thread: one alone, slot_items in packed launches
+__host__ __device__ inline int far_field_grid(const DevState& d) {
+    const int n = 2 * (d.ny - 2) + 2 * d.nx, per = 64 * d.slot_items;
+    return (n + per - 1) / per;
+}
+__device__ __forceinline__ void fused_bc_node(const DevState& d, int t) {
     const int nl = d.ny - 2;
-    int t = bid_ * blockDim.x + threadIdx.x;
     double fn[9];
     if (t < 2 * nl) {
         const int side = t < nl ? 0 : 1, j = 1 + (side == 0 ? t : t - nl);
@@ -410,16 +414,17 @@ __device__ __forceinline__ void fused_bc_kernel_body(const DevState& d, const in
         far_edge(d, i, je, FarMom{nb.r, 0.0, 0.0}, fn, nb);
     }
 }
+__device__ __forceinline__ void fused_bc_kernel_body(const DevState& d, const int bid_) {
+    const int n = 2 * (d.ny - 2) + 2 * d.nx, stride = far_field_grid(d) * 64;
+    for (int t = bid_ * 64 + threadIdx.x; t < n; t += stride) fused_bc_node(d, t);
+}
 __global__ void __launch_bounds__(64) fused_bc_kernel(DevState d) { fused_bc_kernel_body(d, blockIdx.x); }
 __global__ void __launch_bounds__(64) fused_bc_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     fused_bc_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-void launch_fused_bc(const DevState& d, cudaStream_t st) {
-    const int n = 2 * (d.ny - 2) + 2 * d.nx;
-    fused_bc_kernel<<<(n + 63) / 64, 64, 0, st>>>(d);
-}
+void launch_fused_bc(const DevState& d, cudaStream_t st) { fused_bc_kernel<<<far_field_grid(d), 64, 0, st>>>(d); }
 
 void launch_fused_init(const DevState& d, cudaStream_t st) { fused_init_kernel<<<1184, 256, 0, st>>>(d); }
 void launch_fused_shift(const DevState& d, int dr, cudaStream_t st) { fused_shift_kernel<<<1184, 256, 0, st>>>(d, dr); }
@@ -437,7 +442,7 @@ int multi_blocks_fused(MultiKernel k, const DevState& d) {
         const long long runs = ((long long)(d.nx - 2) * (d.ny - 2) + BULK_TX - 1) / BULK_TX;
         return (int)((runs + BULK_MULTI_RUNS - 1) / BULK_MULTI_RUNS);
     }
-    case MK_BC: return (2 * (d.ny - 2) + 2 * d.nx + 63) / 64;
+    case MK_BC: return far_field_grid(d);
     default: return -1;
     }
 }
