@@ -189,7 +189,29 @@ def config_of(ep, storage, world):
             "parallelism": f"{world} independent episodes (one per GPU)"}
 
 
-def serving_metrics(steps=200, requests=3, rate_hz=20.0):
+def served_metrics(clients=64, requests=3, rate_hz=20.0):
+    """`clients` online clients on the ZeroMQ server (client k runs mixed
+    episode k mod 64), Poisson arrivals at rate_hz per client, segments of
+    100-2000 steps, SAVE with p = 0.05: STEP latency at the client."""
+    import threading
+    from lbm_mutiwing_b200 import api, loadgen
+    from lbm_mutiwing_b200 import workloads as wl
+    from lbm_mutiwing_b200.serve import Server
+    srv = Server("tcp://127.0.0.1:0", wl.by_name, "mix:0", precision=api.PRECISION_FP32, workers=clients)
+    th = threading.Thread(target=srv.serve, kwargs={"idle_timeout_s": 600}, daemon=True)
+    th.start()
+    names = [f"mix:{k % 64}" for k in range(clients)]
+    res = loadgen.poisson_load(f"tcp://127.0.0.1:{srv.port}", names, wl.by_name, requests_per_client=requests,
+                               rate_hz=rate_hz)
+    srv.stop()
+    th.join(60)
+    srv.close()
+    return {"served_clients": clients, "served_rate_hz_per_client": rate_hz, "served_steps": len(res.step_latency_s),
+            "served_step_p50_ms": res.percentile(50) * 1e3, "served_step_p99_ms": res.percentile(99) * 1e3,
+            "served_mlups": res.mlups(), "served_errors": len(res.errors)}
+
+
+def serving_metrics(steps=200, requests=3, rate_hz=20.0, clients=64):
     """The seeded 64-episode mixed batch (grids 401x201 .. 2001x1001, 1-4
     wings): (1) every episode advanced `steps` steps, all resident and in
     flight at once (FP32; packed launches over all episodes, and each episode
@@ -198,11 +220,9 @@ def serving_metrics(steps=200, requests=3, rate_hz=20.0):
     the ZeroMQ server with Poisson arrivals, segments of 100-2000 steps, SAVE
     with p = 0.05: STEP latency percentiles at the client; (3) the FP32
     path's segment-averaged forces against FP64 for one client's segments."""
-    import threading
     from lbm_mutiwing_b200 import api, batch, loadgen
     from lbm_mutiwing_b200 import protocol as P
     from lbm_mutiwing_b200 import workloads as wl
-    from lbm_mutiwing_b200.serve import Server
     eps = wl.mixed_batch(64, steps=2 * steps + 16)
     nodes = sum(e.nx * e.ny for e in eps)
     sims = batch.create(eps, api.PRECISION_FP32)
@@ -218,15 +238,7 @@ def serving_metrics(steps=200, requests=3, rate_hz=20.0):
     batched_streams = nodes * steps / wall_streams / 1e6
     plain_s, plain_nu = batch.advance_one_at_a_time(eps, max(8, steps // 4))
     plain = plain_nu / plain_s / 1e6
-    srv = Server("tcp://127.0.0.1:0", wl.by_name, "mix:0", precision=api.PRECISION_FP32, workers=64)
-    th = threading.Thread(target=srv.serve, kwargs={"idle_timeout_s": 600}, daemon=True)
-    th.start()
-    names = [f"mix:{k}" for k in range(64)]
-    res = loadgen.poisson_load(f"tcp://127.0.0.1:{srv.port}", names, wl.by_name, requests_per_client=requests,
-                               rate_hz=rate_hz)
-    srv.stop()
-    th.join(60)
-    srv.close()
+    served = served_metrics(clients, requests, rate_hz)
     # FP32 vs FP64 segment-averaged forces of one client's segments
     ep = wl.by_name("mix:1")
     rng = np.random.default_rng(7)
@@ -250,9 +262,7 @@ def serving_metrics(steps=200, requests=3, rate_hz=20.0):
             "batched_fp32_mlups": batched, "batched_streams_fp32_mlups": batched_streams,
             "one_at_a_time_fp64_mlups": plain,
             "batched_over_one_at_a_time": batched / plain,
-            "served_clients": len(names), "served_steps": len(res.step_latency_s),
-            "served_step_p50_ms": res.percentile(50) * 1e3, "served_step_p99_ms": res.percentile(99) * 1e3,
-            "served_mlups": res.mlups(), "served_errors": len(res.errors),
+            **served,
             "fp32_vs_fp64_force_max_rel_err": err,
             "force_err_sample": "segment-averaged per-wing Fx, Fy, M of mix episode 1, 3 STEP segments"}
 

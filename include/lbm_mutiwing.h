@@ -157,6 +157,16 @@ int lbm_err_fields_noalloc(const double* u, const double* v, const double* u0, c
 int lbm_get_f(LbmHandle* h, double* f);
 int lbm_set_f(LbmHandle* h, const double* f);
 
+/* The rest of a checkpoint (saveflowfield / readflowfield,
+ * solution.f90:1616-1851): the border populations f0 kept since set-up
+ * (boundary_condition1 reads them; only move_mesh changes them) as
+ * 9 x (2 ny + 2 nx) doubles -- population k at k * (2 ny + 2 nx) + e, e
+ * running over the left column (j = 0 .. ny-1), the right column, the
+ * bottom row (i = 0 .. nx-1) and the top row -- and the lattice shift count
+ * movenum (move_mesh.f90).  Set replaces both. */
+int lbm_get_border_f0(LbmHandle* h, double* f0, int32_t* movenum);
+int lbm_set_border_f0(LbmHandle* h, const double* f0, int32_t movenum);
+
 /* Band of the last step (adjoint_p, adjoint_wing_id; airfoil.f90:322-333):
  * 3 ints per node (i, j, wing), 1-based, in the reference's order. */
 int lbm_get_band(LbmHandle* h, int32_t* n, int32_t* ij_wing, int32_t cap);

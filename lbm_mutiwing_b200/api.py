@@ -65,6 +65,8 @@ SIGNATURES = [
     ("lbm_err_fields_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                          C.c_int64, C.c_int32, C.c_void_p, D, C.c_char_p, C.c_int32]),
     ("lbm_get_f", C.c_int, [C.c_void_p, D]),
+    ("lbm_get_border_f0", C.c_int, [C.c_void_p, D, I32]),
+    ("lbm_set_border_f0", C.c_int, [C.c_void_p, D, C.c_int32]),
     ("lbm_set_f", C.c_int, [C.c_void_p, D]),
     ("lbm_get_band", C.c_int, [C.c_void_p, I32, I32, C.c_int32]),
     ("lbm_get_markers", C.c_int, [C.c_void_p, D, D, D, D]),
@@ -258,6 +260,19 @@ class Simulation:
     def set_f(self, f):
         a = np.ascontiguousarray(f, dtype=np.float64)
         self._check(self.L.lbm_set_f(self.h, _dp(a)))
+
+    def border_f0(self):
+        """(f0 of the border nodes, 9 x (2 ny + 2 nx); movenum)."""
+        out = np.zeros((9, 2 * self.ny + 2 * self.nx))
+        m = C.c_int32(0)
+        self._check(self.L.lbm_get_border_f0(self.h, _dp(out), C.byref(m)))
+        return out, m.value
+
+    def set_border_f0(self, f0, movenum: int):
+        a = np.ascontiguousarray(f0, dtype=np.float64)
+        if a.size != 9 * (2 * self.ny + 2 * self.nx):
+            raise LbmError("border f0 must hold 9 x (2 ny + 2 nx) values")
+        self._check(self.L.lbm_set_border_f0(self.h, _dp(a), int(movenum)))
 
     def band(self) -> np.ndarray:
         n = C.c_int32(0)

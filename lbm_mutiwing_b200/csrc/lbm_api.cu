@@ -1498,6 +1498,60 @@ int lbm_get_markers(LbmHandle* h, double* xb1, double* yb1, double* xb2, double*
     return 0;
 }
 
+// Border f0: the fused path keeps it in edge_f0; the plain path in the
+// border entries of its f0 planes (interior f0 is rewritten every step).
+static int border_f0_copy(LbmHandle* h, double* host, bool to_device) {
+    const DevState& d = h->d;
+    const long long per = 2LL * d.ny + 2LL * d.nx;
+    if (d.precision != 0) {
+        const size_t bytes = 9 * (size_t)per * sizeof(double);
+        CK(to_device ? cudaMemcpy(d.edge_f0, host, bytes, cudaMemcpyHostToDevice)
+                     : cudaMemcpy(host, d.edge_f0, bytes, cudaMemcpyDeviceToHost));
+        return 0;
+    }
+    for (int k = 0; k < 9; ++k) {
+        double* plane = d.f0 + k * d.plane;
+        double* e = host + k * per;
+        const size_t dp = sizeof(double) * d.pitch, one = sizeof(double);
+        // columns: one element per row; rows: contiguous
+        if (to_device) {
+            CK(cudaMemcpy2D(plane, dp, e, one, one, d.ny, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy2D(plane + d.nx - 1, dp, e + d.ny, one, one, d.ny, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(plane, e + 2 * d.ny, one * d.nx, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(plane + (long long)(d.ny - 1) * d.pitch, e + 2 * d.ny + d.nx, one * d.nx,
+                          cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy2D(e, one, plane, dp, one, d.ny, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy2D(e + d.ny, one, plane + d.nx - 1, dp, one, d.ny, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(e + 2 * d.ny, plane, one * d.nx, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(e + 2 * d.ny + d.nx, plane + (long long)(d.ny - 1) * d.pitch, one * d.nx,
+                          cudaMemcpyDeviceToHost));
+        }
+    }
+    return 0;
+}
+
+int lbm_get_border_f0(LbmHandle* h, double* f0, int32_t* movenum) {
+    DeviceLock lock(g_device_mutex);
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaDeviceSynchronize());
+    if (f0 && border_f0_copy(h, f0, false)) return -1;
+    if (movenum) *movenum = h->d.movenum;
+    return 0;
+}
+
+int lbm_set_border_f0(LbmHandle* h, const double* f0, int32_t movenum) {
+    DeviceLock lock(g_device_mutex);
+    if (!h) return -1;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaDeviceSynchronize());
+    if (f0 && border_f0_copy(h, const_cast<double*>(f0), true)) return -1;
+    h->d.movenum = movenum;
+    drop_graphs(h);   // movenum is baked into the step graphs
+    return 0;
+}
+
 int lbm_move_mesh(LbmHandle* h, int32_t dr) {
     DeviceLock lock(g_device_mutex);
     if (!h) return -1;
