@@ -8,7 +8,7 @@ Tolerances:
     order versus the oracle's dense LU), 1e-9 relative on forces and fields
     for well-conditioned marker sets;
   * fused FP32 path: 1e-3 relative on segment-averaged per-wing forces (the
-    north-star bar), 2e-4 relative L2 on u, v, p;
+    accuracy the FP32 path is built to), 2e-4 relative L2 on u, v, p;
   * cosine-spaced NACA sections put trailing-edge markers 0.025 lattice
     spacings apart, which makes X X^T numerically singular; there any two FP64
     solvers (two pivot orders of the reference's own LU included) differ by
