@@ -132,12 +132,9 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
 }
 // Packed form: an episode's interior nodes, row by row without the border
 // columns, in runs of BULK_TX consecutive nodes (a warp may straddle two
-// rows), so narrow lattices leave no thread idle; a block takes
-// BULK_MULTI_RUNS runs (2: 8% faster steps than 1 on the 64-episode mixed
-// batch; 4 no better, 8 worse).
-#ifndef BULK_MULTI_RUNS
-#define BULK_MULTI_RUNS 2
-#endif
+// rows), so narrow lattices leave no thread idle; a block takes RUNS runs
+// (1, 2 or 4: the batch engine times the three on a batch's first long call
+// and keeps the fastest; every node is computed the same way in each).
 // The episode's parameters are staged in shared memory by one thread, so
 // the kernel fits the single-episode kernel's register budget (eight
 // 256-thread blocks per SM).
@@ -150,17 +147,18 @@ struct BulkArgs {
     int pitch, w, n, l, fields;
     FusedConsts c;
 };
-template <bool FIELDS>
+template <bool FIELDS, int RUNS>
 __device__ __forceinline__ void fused_bulk_runs(const BulkArgs& a) {
 #pragma unroll
-    for (int r = 0; r < BULK_MULTI_RUNS; ++r) {
-        const int t = (a.l * BULK_MULTI_RUNS + r) * BULK_TX + threadIdx.x;
+    for (int r = 0; r < RUNS; ++r) {
+        const int t = (a.l * RUNS + r) * BULK_TX + threadIdx.x;
         if (t >= a.n) break;
         const int jj = t / a.w;
         fused_bulk_node<FIELDS, false>(a.gA, a.gB, a.pitch, a.plane, a.c, a.fo_rho, a.fo_u, a.fo_v, a.bits,
                                        t - jj * a.w + 1, jj + 1);
     }
 }
+template <int RUNS>
 __global__ void __launch_bounds__(BULK_TX, 8) fused_bulk_kernel_multi(MultiArgs m) {
     __shared__ BulkArgs a;
     if (threadIdx.x == 0) {
@@ -182,9 +180,9 @@ __global__ void __launch_bounds__(BULK_TX, 8) fused_bulk_kernel_multi(MultiArgs 
     }
     __syncthreads();
     if (a.fields)
-        fused_bulk_runs<true>(a);
+        fused_bulk_runs<true, RUNS>(a);
     else
-        fused_bulk_runs<false>(a);
+        fused_bulk_runs<false, RUNS>(a);
 }
 
 // Initial state (solution.f90:44-61): f = f0 = feq(1, UU, 0) on every node,
@@ -438,9 +436,12 @@ void launch_fused_import(const DevState& d, const double* f, float* g, cudaStrea
 // ------------------------------------------------------------ packed launches
 int multi_blocks_fused(MultiKernel k, const DevState& d) {
     switch (k) {
-    case MK_BULK: {
+    case MK_BULK1:
+    case MK_BULK2:
+    case MK_BULK4: {
+        const int per = k == MK_BULK1 ? 1 : k == MK_BULK2 ? 2 : 4;
         const long long runs = ((long long)(d.nx - 2) * (d.ny - 2) + BULK_TX - 1) / BULK_TX;
-        return (int)((runs + BULK_MULTI_RUNS - 1) / BULK_MULTI_RUNS);
+        return (int)((runs + per - 1) / per);
     }
     case MK_BC: return far_field_grid(d);
     default: return -1;
@@ -449,13 +450,19 @@ int multi_blocks_fused(MultiKernel k, const DevState& d) {
 
 bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st) {
     switch (k) {
-    case MK_BULK: fused_bulk_kernel_multi<<<blocks, BULK_TX, 0, st>>>(m); return true;
+    case MK_BULK1: fused_bulk_kernel_multi<1><<<blocks, BULK_TX, 0, st>>>(m); return true;
+    case MK_BULK2: fused_bulk_kernel_multi<2><<<blocks, BULK_TX, 0, st>>>(m); return true;
+    case MK_BULK4: fused_bulk_kernel_multi<4><<<blocks, BULK_TX, 0, st>>>(m); return true;
     case MK_BC: fused_bc_kernel_multi<<<blocks, 64, 0, st>>>(m); return true;
     default: return false;
     }
 }
 
-bool is_bulk_multi_kernel(const void* func) { return func == reinterpret_cast<const void*>(fused_bulk_kernel_multi); }
+bool is_bulk_multi_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(fused_bulk_kernel_multi<1>) ||
+           func == reinterpret_cast<const void*>(fused_bulk_kernel_multi<2>) ||
+           func == reinterpret_cast<const void*>(fused_bulk_kernel_multi<4>);
+}
 
 bool is_far_field_kernel(const void* func) { return func == reinterpret_cast<const void*>(fused_bc_kernel); }
 

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <queue>
 #include <string>
@@ -214,6 +215,10 @@ struct LbmBatch {
     size_t d_cap = 0;
     char* h_buf = nullptr;          // pinned staging of the tables
     size_t h_cap = 0;
+    // autotuning of the packed bulk kernel's runs per block: batch shape
+    // (sorted lattice sizes) -> fastest kind, and the events that time it
+    std::map<std::vector<long long>, int> bulk_kind;
+    cudaEvent_t ev_tune[4] = {};
 };
 
 namespace {
@@ -1089,6 +1094,7 @@ int lbm_batch_create(int32_t device, LbmBatch** out) {
         BCK(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, mid));
     for (cudaEvent_t* e : {&b->ev_start, &b->ev_bulk, &b->ev_ibm, &b->ev_bc, &b->ev_geom, &b->ev_list, &b->ev_fact})
         BCK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (cudaEvent_t& e : b->ev_tune) BCK(cudaEventCreate(&e));
     return 0;
 }
 
@@ -1244,11 +1250,47 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         for (MultiKernel k : {MK_ASSEMBLE, MK_FACTOR_SMEM, MK_FACTOR_GLOBAL}) launch(k, at, ne, sb);
         if (events) cudaEventRecord(b->ev_fact, sb);
     };
+    // The packed bulk kernel's runs per block: the tuned choice for this
+    // batch shape, else steps 1-6 of a call that keeps the same episodes
+    // stepping through step 7 time two steps of each candidate (same bits
+    // for every choice) and the fastest is kept for the rest of the call
+    // and for later calls on the same shape.
+    static const int cand[3] = {MK_BULK1, MK_BULK2, MK_BULK4};
+    int bulk = MK_BULK2;
+    bool tune = false;
+    std::vector<long long> shape;
+    if (K >= 8 && steps[1].a_cur == steps[7].a_cur) {
+        for (int e = 0; e < steps[1].a_cur; ++e)
+            shape.push_back((long long)hs[order[e]]->d.nx * 1000003LL + hs[order[e]]->d.ny);
+        std::sort(shape.begin(), shape.end());
+        const auto it = b->bulk_kind.find(shape);
+        if (it != b->bulk_kind.end()) bulk = it->second;
+        else tune = true;
+    }
     // the geometry of the first step (prime_geometry), then the steps as
     // enqueue_step orders them, every kernel packed over the batch
     if (K > 0) geometry(steps[0].cur, steps[0].a_cur, sm, sm, false);
     for (int64_t k = 0; k < K; ++k) {
         const StepTab& t = steps[k];
+        const bool trial = tune && k >= 1 && k <= 6;
+        if (trial && (k & 1)) cudaEventRecord(b->ev_tune[(k - 1) / 2], sm);
+        if (tune && k == 7) {   // the three trials are done: keep the fastest
+            cudaEventRecord(b->ev_tune[3], sm);
+            BCK(cudaEventSynchronize(b->ev_tune[3]));
+            float best = 0.f;
+            for (int c = 0; c < 3; ++c) {
+                float ms = 0.f;
+                BCK(cudaEventElapsedTime(&ms, b->ev_tune[c], b->ev_tune[c + 1]));
+                if (c == 0 || ms < best) {
+                    best = ms;
+                    bulk = cand[c];
+                }
+            }
+            if (b->bulk_kind.size() > 256) b->bulk_kind.clear();
+            b->bulk_kind[shape] = bulk;
+            tune = false;
+        }
+        const int kind = trial ? cand[(k - 1) / 2] : bulk;
         cudaEventRecord(b->ev_start, sm);
         for (cudaStream_t st : {b->s_bulk, b->s_ibm, b->s_bc}) cudaStreamWaitEvent(st, b->ev_start, 0);
         if (t.a_ahead) {
@@ -1260,7 +1302,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         for (MultiKernel k2 : {MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
             launch(k2, t.cur, t.a_cur, b->s_ibm);
         cudaEventRecord(b->ev_ibm, b->s_ibm);
-        launch(MK_BULK, t.cur, t.a_cur, b->s_bulk);
+        launch((MultiKernel)kind, t.cur, t.a_cur, b->s_bulk);
         cudaEventRecord(b->ev_bulk, b->s_bulk);
         cudaStreamWaitEvent(sm, b->ev_bulk, 0);
         cudaStreamWaitEvent(sm, b->ev_ibm, 0);
@@ -1315,6 +1357,8 @@ void lbm_batch_destroy(LbmBatch* b) {
     for (cudaStream_t s : {b->s_main, b->s_bulk, b->s_ibm, b->s_bc, b->s_aux, b->s_aux2})
         if (s) cudaStreamDestroy(s);
     for (cudaEvent_t e : {b->ev_start, b->ev_bulk, b->ev_ibm, b->ev_bc, b->ev_geom, b->ev_list, b->ev_fact})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->ev_tune)
         if (e) cudaEventDestroy(e);
     delete b;
 }

@@ -86,7 +86,7 @@ enum MultiKernel : int {
     MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
     MK_RHS, MK_SPREAD, MK_FINISH,                                      // immersed boundary
     MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
-    MK_BULK, MK_BC,                                                     // lattice
+    MK_BULK1, MK_BULK2, MK_BULK4, MK_BC,   // lattice (bulk: 1, 2 or 4 node runs per block)
     MK_KINDS
 };
 struct MultiArgs {

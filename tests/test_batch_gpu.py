@@ -1,7 +1,7 @@
 """Packed stepping (lbm_batch_step) against stepping each episode alone.
 
 Episodes of different lattice sizes, wing counts and step counts advance in
-one batch call; every force row, the distributions, the output fields and
+one batch call (long calls also time the packed bulk kernel's variants); every force row, the distributions, the output fields and
 the running sums must equal, bit for bit, those of the same episodes
 advanced one lbm_step call at a time, including over a second batch call,
 a single-episode call in between, and calls that write fields or the
@@ -83,6 +83,15 @@ def test_batch_equals_one_at_a_time(gpu_lib):
             rows_b = batch.step([packed[i] for i in sub], 6)
             for ra, rb in zip(rows_a, rows_b):
                 _same(ra, rb)
+            # long enough for the engine to time its bulk-kernel variants
+            # (steps 1-6 each run a different one), then with the choice kept
+            for _ in range(2):
+                rows_a = [s.step(9) for s in alone]
+                rows_b = batch.step(packed, 9)
+                for ra, rb in zip(rows_a, rows_b):
+                    _same(ra, rb)
+            for sa, sb in zip(alone, packed):
+                _compare_state(sa, sb)
     finally:
         for s in alone + packed:
             s.close()
