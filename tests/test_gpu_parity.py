@@ -31,7 +31,8 @@ def episode_a(steps=80):
 
 def episode_b(steps=60):
     """The 800x400 tandem coarsened to dx = 0.04, cosine-spaced markers."""
-    return wl.tandem_800x400(steps=steps, scale_factor=4)
+    return wl.tandem_pitch_heave("tandem_800x400_cosine", 8.0, 4.0, 0.04, 200.0, -2.0, 0.0, 50, steps,
+                                 spacing="cosine")
 
 
 def rel(a, b):
