@@ -1,7 +1,7 @@
 """Benchmark: MLUPS of the LBM_Mutiwing time step on B200.
 
 Default workload: the 4000x2000 two-wing case (4001 x 2001 nodes, dx = 0.01,
-Re 1000, two NACA0012 wings with 200 markers each (uniform in x), analytic
+Re 1000, two NACA0012 wings with 200 markers each at equal arc length, analytic
 pitch/heave motion), FP32 deviation storage, FP64 immersed boundary and force
 reductions.  A "step" is one lattice time step (evolution, solution.f90:272)
 of one episode; with N GPUs every rank advances its own episode (episodes are

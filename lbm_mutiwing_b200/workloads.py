@@ -24,18 +24,21 @@ import numpy as np
 PAI = 3.1415926535897932384626433832795  # main.f90:9
 
 
-def naca_loop(thickness: float, n_markers: int, spacing: str = "uniform") -> np.ndarray:
+def naca_loop(thickness: float, n_markers: int, spacing: str = "arc") -> np.ndarray:
     """Closed NACA 00xx loop, shape (n_markers + 1, 2), body frame.
 
     The symmetric 4-digit thickness law with the closed-trailing-edge
     coefficient (-0.1036) gives one shared trailing-edge point.  ``spacing`` is
+    ``"arc"`` (equal arc length along each surface; the default),
     ``"uniform"`` (uniform x, the style of the reference's shipped
-    boundary.dat; the default) or ``"cosine"`` (x = (1 - cos b) / 2, b
-    uniform).  Cosine spacing puts trailing-edge markers 0.025 lattice
-    spacings apart at 200 markers per chord of 100 nodes: the immersed-boundary
-    system becomes numerically singular there, and the reference's algorithm
-    (the FP64 oracle) diverges after about 1150 steps of the 800x400 case,
-    while uniform spacing runs stably.
+    boundary.dat) or ``"cosine"`` (x = (1 - cos b) / 2, b uniform).  At 200
+    markers on a chord of 100 nodes, arc spacing puts markers 1.0-1.02
+    lattice spacings apart everywhere; cosine spacing puts trailing-edge
+    markers 0.025 spacings apart, where the immersed-boundary system becomes
+    numerically singular and the reference's algorithm (the FP64 oracle)
+    diverges after about 1150 steps of the 800x400 case; uniform-x spacing
+    leaves leading-edge gaps of 2 spacings.  Arc and uniform-x spacing both
+    run 2000 steps of that case stably.
     """
     if n_markers < 4:
         raise ValueError("need at least 4 markers per wing")
@@ -48,16 +51,31 @@ def naca_loop(thickness: float, n_markers: int, spacing: str = "uniform") -> np.
             return 0.5 * (1.0 - np.cos(np.pi * b))
         if spacing == "uniform":
             return b
-        raise ValueError("spacing must be 'cosine' or 'uniform'")
+        raise ValueError("spacing must be 'cosine', 'uniform' or 'arc'")
 
     def yt(x):
         return 5.0 * thickness * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2
                                   + 0.2843 * x ** 3 - 0.1036 * x ** 4)
 
-    xu = xs(nh, nh)                     # LE .. TE, nh + 1 points
-    xl = xs(nl, nl)[::-1][1:]           # TE(excluded) .. LE, nl points
-    x = np.concatenate([xu, xl])
-    y = np.concatenate([yt(xu), -yt(xl)])
+    if spacing == "arc":
+        # equal arc length along each surface: a fine cosine sampling of the
+        # surface resampled at equal steps (both ends kept exactly)
+        xf = 0.5 * (1.0 - np.cos(np.pi * np.linspace(0.0, 1.0, 64 * n_markers + 1)))
+        yf = yt(xf)
+        s = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(xf), np.diff(yf)))])
+
+        def surface(m):
+            t = np.linspace(0.0, s[-1], m + 1)
+            return np.interp(t, s, xf), np.interp(t, s, yf)
+        xu, yu = surface(nh)
+        xl, yl = surface(nl)
+        x = np.concatenate([xu, xl[::-1][1:]])
+        y = np.concatenate([yu, -yl[::-1][1:]])
+    else:
+        xu = xs(nh, nh)                     # LE .. TE, nh + 1 points
+        xl = xs(nl, nl)[::-1][1:]           # TE(excluded) .. LE, nl points
+        x = np.concatenate([xu, xl])
+        y = np.concatenate([yt(xu), -yt(xl)])
     y[-1] = 0.0
     pts = np.stack([x - 0.25, y], axis=1)
     pts[-1] = pts[0]
@@ -141,7 +159,7 @@ def lattice(width: float, height: float, scale: float):
 def tandem_pitch_heave(name: str, width: float, height: float, scale: float, re: float,
                        x_first: float, y: float, n_markers: int, steps: int,
                        thickness: float = 0.12, lag: float = 0.25 * math.pi,
-                       spacing: str = "uniform", n_wings: int = 2, x_spacing: float = 1.5,
+                       spacing: str = "arc", n_wings: int = 2, x_spacing: float = 1.5,
                        pitch_deg: float = 15.0, heave: float = 0.5, freq: float = 0.5) -> Episode:
     """Tandem wings with the analytic pitch/heave law of the benchmark configs.
 
@@ -163,7 +181,7 @@ def tandem_pitch_heave(name: str, width: float, height: float, scale: float, re:
 def tandem_800x400(steps: int = 2000, scale_factor: int = 1) -> Episode:
     """800x400 lattice (8x4 chords, dx = 0.01), Re 200, NACA0012 tandem at
     corner-frame x = 2.0 / 3.5, y = 2.0 (centred frame -2.0 / -0.5, 0.0),
-    200 markers per wing, uniform in x (see naca_loop).  ``scale_factor`` > 1 coarsens the
+    200 markers per wing at equal arc length (see naca_loop).  ``scale_factor`` > 1 coarsens the
     lattice for quick tests (dx = 0.01 * scale_factor)."""
     return tandem_pitch_heave("tandem_800x400_re200", 8.0, 4.0, 0.01 * scale_factor, 200.0,
                               -2.0, 0.0, 200 // scale_factor, steps)
