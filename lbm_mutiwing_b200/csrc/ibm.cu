@@ -924,6 +924,17 @@ static inline int blocks(long long n, int t) { return (int)std::max<long long>(1
 
 int ibm_finish_blocks(const DevState& d) { return blocks(d.band_cap, FINISH_THREADS); }
 
+bool is_geometry_multi_kernel(const void* func) {
+    for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_claim_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_count_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_scan_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_list_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_assemble_kernel_multi)})
+        if (func == k) return true;
+    return is_factor_multi_kernel(func);
+}
+
 bool is_geometry_kernel(const void* func) {
     for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel), reinterpret_cast<const void*>(ibm_claim_kernel),
                           reinterpret_cast<const void*>(ibm_count_kernel), reinterpret_cast<const void*>(ibm_scan_kernel),

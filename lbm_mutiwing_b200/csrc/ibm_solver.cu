@@ -580,6 +580,11 @@ cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     return e;
 }
 
+bool is_factor_multi_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<true>) ||
+           func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<false>);
+}
+
 bool is_factor_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(ibm_factor_kernel<true>) ||
            func == reinterpret_cast<const void*>(ibm_factor_kernel<false>);

@@ -458,6 +458,8 @@ bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStrea
     }
 }
 
+bool is_far_field_multi_kernel(const void* func) { return func == reinterpret_cast<const void*>(fused_bc_kernel_multi); }
+
 bool is_bulk_multi_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(fused_bulk_kernel_multi<1>) ||
            func == reinterpret_cast<const void*>(fused_bulk_kernel_multi<2>) ||

@@ -219,6 +219,10 @@ struct LbmBatch {
     // (sorted lattice sizes) -> fastest kind, and the events that time it
     std::map<std::vector<long long>, int> bulk_kind;
     cudaEvent_t ev_tune[4] = {};
+    // CUDA graphs of two packed steps, by everything their launches bake in
+    // (table addresses, block offsets, bulk variant)
+    std::map<std::vector<long long>, cudaGraphExec_t> graphs;
+    int prio_lo = 0, prio_mid = 0, prio_hi = 0;
 };
 
 namespace {
@@ -639,6 +643,37 @@ int build_graph(LbmHandle* h, int p, int gs) {
     return 0;
 }
 
+void drop_batch_graphs(LbmBatch* b) {
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+}
+
+// A graph's kernel nodes run at the priority of the launch stream unless
+// they carry their own: bulk low; far field, geometry and factorisation
+// middle; the immersed-boundary chain high, as the batch's streams have.
+cudaError_t instantiate_with_priorities(LbmBatch* b, cudaGraph_t g, cudaGraphExec_t* out) {
+    size_t nn = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+    for (size_t k = 0; e == cudaSuccess && k < nn; ++k) {
+        cudaGraphNodeType ty;
+        e = cudaGraphNodeGetType(nodes[k], &ty);
+        if (e != cudaSuccess || ty != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        e = cudaGraphKernelNodeGetParams(nodes[k], &kp);
+        if (e != cudaSuccess) break;
+        cudaKernelNodeAttrValue v;
+        std::memset(&v, 0, sizeof(v));
+        v.priority = is_bulk_multi_kernel(kp.func) ? b->prio_lo
+                     : (is_far_field_multi_kernel(kp.func) || is_geometry_multi_kernel(kp.func)) ? b->prio_mid
+                                                                                                 : b->prio_hi;
+        e = cudaGraphKernelNodeSetAttribute(nodes[k], cudaKernelNodeAttributePriority, &v);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority);
+    return e;
+}
+
 int batch_fail(LbmBatch* b, const std::string& msg) {
     if (b) b->err = msg;
     return -1;
@@ -664,6 +699,7 @@ int multi_blocks(MultiKernel k, const DevState& d) {
 // geometry sets a step can start from.
 constexpr int BV_PLAIN = 0, BV_SECOND_LAST = 2, BV_LAST = 4, BV_AHEAD = 6, BV_COUNT = 8;
 constexpr int BATCH_SLOT_ITEMS = 4;   // per-slot items per thread in packed launches
+constexpr int64_t GRAPH_PAIR_MIN = 8;  // steady steps ahead before a step pair is captured
 
 void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out) {
     for (int ph = 0; ph < 2; ++ph) {
@@ -1087,6 +1123,9 @@ int lbm_batch_create(int32_t device, LbmBatch** out) {
     int lo = 0, hi = 0;
     BCK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     const int mid = (lo + hi) / 2;
+    b->prio_lo = lo;
+    b->prio_mid = mid;
+    b->prio_hi = hi;
     BCK(cudaStreamCreateWithPriority(&b->s_bulk, cudaStreamNonBlocking, lo));
     for (cudaStream_t* st : {&b->s_main, &b->s_ibm})
         BCK(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi));
@@ -1206,6 +1245,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     if (total > b->d_cap || total > b->h_cap) {
         DeviceLock lock(g_device_mutex);
         const size_t cap = std::max(total, (size_t)1 << 20) * 2;
+        drop_batch_graphs(b);   // they bake addresses in the old tables
         if (b->d_buf) cudaFree(b->d_buf);
         if (b->h_buf) cudaFreeHost(b->h_buf);
         b->d_buf = nullptr;
@@ -1267,6 +1307,37 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         if (it != b->bulk_kind.end()) bulk = it->second;
         else tune = true;
     }
+    // one packed step, as enqueue_step orders it
+    auto emit = [&](const StepTab& t, int kind) {
+        cudaEventRecord(b->ev_start, sm);
+        for (cudaStream_t st : {b->s_bulk, b->s_ibm, b->s_bc}) cudaStreamWaitEvent(st, b->ev_start, 0);
+        if (t.a_ahead) {
+            cudaStreamWaitEvent(b->s_aux, b->ev_start, 0);
+            geometry(t.ahead, t.a_ahead, b->s_aux, b->s_aux2, true);
+        }
+        launch(MK_BC, t.cur, t.a_cur, b->s_bc);
+        cudaEventRecord(b->ev_bc, b->s_bc);
+        for (MultiKernel k2 : {MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
+            launch(k2, t.cur, t.a_cur, b->s_ibm);
+        cudaEventRecord(b->ev_ibm, b->s_ibm);
+        launch((MultiKernel)kind, t.cur, t.a_cur, b->s_bulk);
+        cudaEventRecord(b->ev_bulk, b->s_bulk);
+        cudaStreamWaitEvent(sm, b->ev_bulk, 0);
+        cudaStreamWaitEvent(sm, b->ev_ibm, 0);
+        cudaStreamWaitEvent(sm, b->ev_bc, 0);
+        if (t.a_ahead) {   // the next step's geometry
+            cudaStreamWaitEvent(sm, b->ev_list, 0);
+            cudaStreamWaitEvent(sm, b->ev_fact, 0);
+        }
+    };
+    // steps from k on in a steady stretch of identical step pairs
+    auto same = [&](int64_t x, int64_t y) {
+        return steps[x].cur == steps[y].cur && steps[x].ahead == steps[y].ahead && steps[x].a_cur == steps[y].a_cur &&
+               steps[x].a_ahead == steps[y].a_ahead;
+    };
+    std::vector<int64_t> pair_run((size_t)K, 0);
+    for (int64_t k = K - 2; k >= 0; --k)
+        pair_run[k] = (k + 3 < K && same(k, k + 2) && same(k + 1, k + 3)) ? pair_run[k + 2] + 2 : 2;
     // the geometry of the first step (prime_geometry), then the steps as
     // enqueue_step orders them, every kernel packed over the batch
     if (K > 0) geometry(steps[0].cur, steps[0].a_cur, sm, sm, false);
@@ -1291,26 +1362,38 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
             tune = false;
         }
         const int kind = trial ? cand[(k - 1) / 2] : bulk;
-        cudaEventRecord(b->ev_start, sm);
-        for (cudaStream_t st : {b->s_bulk, b->s_ibm, b->s_bc}) cudaStreamWaitEvent(st, b->ev_start, 0);
-        if (t.a_ahead) {
-            cudaStreamWaitEvent(b->s_aux, b->ev_start, 0);
-            geometry(t.ahead, t.a_ahead, b->s_aux, b->s_aux2, true);
+        // a steady stretch (the same tables every other step) replays one
+        // graph per two steps: captured the first time, kept for later calls
+        if (!tune && k + 1 < K) {
+            std::vector<long long> key = {(long long)(uintptr_t)b->d_buf, (long long)off_boff, (long long)off_ptr, nh,
+                                          (long long)factor_smem, (long long)solve_smem, kind};
+            for (int q = 0; q < 2; ++q) {
+                const StepTab& u = steps[k + q];
+                key.insert(key.end(), {(long long)u.cur, (long long)u.ahead, u.a_cur, u.a_ahead});
+            }
+            key.insert(key.end(), boff.begin(), boff.end());
+            auto it = b->graphs.find(key);
+            if (it == b->graphs.end() && pair_run[k] >= GRAPH_PAIR_MIN) {
+                if (b->graphs.size() >= 64) drop_batch_graphs(b);
+                DeviceLock lock(g_device_mutex);
+                cudaGraph_t g = nullptr;
+                BCK(cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal));
+                emit(steps[k], kind);
+                emit(steps[k + 1], kind);
+                BCK(cudaStreamEndCapture(sm, &g));
+                cudaGraphExec_t ge = nullptr;
+                const cudaError_t e = instantiate_with_priorities(b, g, &ge);
+                cudaGraphDestroy(g);
+                BCK(e);
+                it = b->graphs.emplace(key, ge).first;
+            }
+            if (it != b->graphs.end()) {
+                BCK(cudaGraphLaunch(it->second, sm));
+                ++k;   // the pair's second step
+                continue;
+            }
         }
-        launch(MK_BC, t.cur, t.a_cur, b->s_bc);
-        cudaEventRecord(b->ev_bc, b->s_bc);
-        for (MultiKernel k2 : {MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
-            launch(k2, t.cur, t.a_cur, b->s_ibm);
-        cudaEventRecord(b->ev_ibm, b->s_ibm);
-        launch((MultiKernel)kind, t.cur, t.a_cur, b->s_bulk);
-        cudaEventRecord(b->ev_bulk, b->s_bulk);
-        cudaStreamWaitEvent(sm, b->ev_bulk, 0);
-        cudaStreamWaitEvent(sm, b->ev_ibm, 0);
-        cudaStreamWaitEvent(sm, b->ev_bc, 0);
-        if (t.a_ahead) {   // the next step's geometry
-            cudaStreamWaitEvent(sm, b->ev_list, 0);
-            cudaStreamWaitEvent(sm, b->ev_fact, 0);
-        }
+        emit(t, kind);
     }
     BCK(cudaStreamSynchronize(sm));
     BCK(cudaGetLastError());
@@ -1352,6 +1435,7 @@ void lbm_batch_destroy(LbmBatch* b) {
     cudaSetDevice(b->device);
     for (cudaStream_t s : {b->s_main, b->s_bulk, b->s_ibm, b->s_bc, b->s_aux, b->s_aux2})
         if (s) cudaStreamSynchronize(s);
+    drop_batch_graphs(b);
     if (b->d_buf) cudaFree(b->d_buf);
     if (b->h_buf) cudaFreeHost(b->h_buf);
     for (cudaStream_t s : {b->s_main, b->s_bulk, b->s_ibm, b->s_bc, b->s_aux, b->s_aux2})

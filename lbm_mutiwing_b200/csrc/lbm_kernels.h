@@ -103,5 +103,10 @@ bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_
 bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int blocks, size_t smem, cudaStream_t st);
 bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st);
 bool is_bulk_multi_kernel(const void* func);
+// packed kernels that take the middle priority (far field, geometry built
+// ahead, factorisation), for the nodes of packed step graphs
+bool is_far_field_multi_kernel(const void* func);
+bool is_geometry_multi_kernel(const void* func);
+bool is_factor_multi_kernel(const void* func);
 
 }  // namespace lbm

@@ -1,7 +1,8 @@
 """Packed stepping (lbm_batch_step) against stepping each episode alone.
 
 Episodes of different lattice sizes, wing counts and step counts advance in
-one batch call (long calls also time the packed bulk kernel's variants); every force row, the distributions, the output fields and
+one batch call (long calls also time the packed bulk kernel's variants and
+replay steady step pairs from CUDA graphs); every force row, the distributions, the output fields and
 the running sums must equal, bit for bit, those of the same episodes
 advanced one lbm_step call at a time, including over a second batch call,
 a single-episode call in between, and calls that write fields or the
@@ -16,8 +17,8 @@ from lbm_mutiwing_b200 import workloads as wl
 pytestmark = pytest.mark.gpu
 
 
-def small(name, wings, size, markers=60):
-    return wl.tandem_pitch_heave(name, size[0], size[1], 0.02, 100.0, -1.0, 0.0, markers, 40, n_wings=wings,
+def small(name, wings, size, markers=60, steps=40):
+    return wl.tandem_pitch_heave(name, size[0], size[1], 0.02, 100.0, -1.0, 0.0, markers, steps, n_wings=wings,
                                  x_spacing=1.5, spacing="uniform")
 
 
@@ -130,3 +131,24 @@ def test_streamed_substitution_matches_whole_factor(gpu_lib):
     finally:
         for s_ in (ref, st, st2):
             s_.close()
+
+
+def test_batch_graph_replay_equals_one_at_a_time(gpu_lib):
+    """Long packed calls replay steady pairs of steps from CUDA graphs
+    (captured on the first long stretch, reused by later calls): the same
+    bits as each episode stepped alone."""
+    eps = [small(n, w, size, steps=80) for n, w, size in EPISODES[:3]]
+    alone = [api.Simulation(ep, api.PRECISION_FP32) for ep in eps]
+    packed = [api.Simulation(ep, api.PRECISION_FP32) for ep in eps]
+    try:
+        with api.Batch(0) as batch:
+            for _ in range(3):
+                rows_a = [s.step(24) for s in alone]
+                rows_b = batch.step(packed, 24)
+                for ra, rb in zip(rows_a, rows_b):
+                    _same(ra, rb)
+            for sa, sb in zip(alone, packed):
+                _compare_state(sa, sb)
+    finally:
+        for s in alone + packed:
+            s.close()
