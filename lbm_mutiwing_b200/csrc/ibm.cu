@@ -25,13 +25,20 @@
 //   claim      lowest segment index claims each box node   | assemble  G
 //   count      claims per segment                          | factor    L' D L'^T
 //   scan       band-list offsets, coupled-wing check       |
-//   list       band list in the reference's order (segment, i, j)
+//   list       band list in the reference's order (segment, i, j), band
+//              bit plane; advances the geometry's cycle counter
+// then, plain FP64 path:
 //   ustar      u*, rho at band nodes; zeroed spread accumulators
 //   rhs        r = ub - X u* (one warp per segment)
 //   solve      forward and backward substitution (waits for the factor)
 //   spread     du = X^T y with fixed-point integer atomics
 //   finish     du, body force, per-block force partials
 //   forces     per-wing force and moment, force row
+// or, FP32 path (beside the bulk kernel):
+//   rhs        u* from the pulled distributions at each box node, r = ub - X u*
+//   solve, spread as above
+//   close      du, band-node re-collision, force partials; the last block
+//              writes the force row and advances the cycle counter
 //
 // Determinism: the band list is built in first-claimant order from an
 // atomicMin claim pass plus a prefix sum; the spread rounds every
@@ -364,40 +371,19 @@ __global__ void ibm_list_kernel_multi(MultiArgs m) {
     ibm_list_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// u*, rho at band nodes (solution.f90:510-554): the moment fields of the
-// plain path, or the moments of the pulled distributions of the fused path
-// (band nodes are interior nodes: boxes keep off the border).  Also zeroes
-// the spread accumulators.
-template <bool FUSED>
-__device__ __forceinline__ void ibm_ustar_kernel_body(const DevState& d, const int bid_) {
-    const int b = bid_ * blockDim.x + threadIdx.x;
+// Plain path: u*, rho at band nodes from the moment fields
+// (solution.f90:510-554), and the spread accumulators zeroed.  The FP32 path
+// evaluates u* inside its rhs kernel instead.
+__global__ void ibm_ustar_kernel(DevState d) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= d.band_n[0]) return;
-    const int i = d.band_ij[2 * b], j = d.band_ij[2 * b + 1];
-    const long long p = pidx(d, i, j);
+    const long long p = pidx(d, d.band_ij[2 * b], d.band_ij[2 * b + 1]);
     reinterpret_cast<unsigned long long*>(d.band_du)[b] = 0ull;
     reinterpret_cast<unsigned long long*>(d.band_dv)[b] = 0ull;
-    if (!FUSED) {
-        d.band_rho[b] = d.rho[p];
-        d.band_us[b] = d.u[p];
-        d.band_vs[b] = d.v[p];
-        return;
-    }
-    double f[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) f[k] = (double)d.gA[k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch] + weight(k);
-    double trho = 0.0, tu = 0.0, tv = 0.0;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        trho = trho + f[k];
-        tu = tu + (double)ex(k) * f[k];
-        tv = tv + (double)ey(k) * f[k];
-    }
-    d.band_rho[b] = trho;
-    d.band_us[b] = tu / trho;
-    d.band_vs[b] = tv / trho;
+    d.band_rho[b] = d.rho[p];
+    d.band_us[b] = d.u[p];
+    d.band_vs[b] = d.v[p];
 }
-template <bool FUSED>
-__global__ void ibm_ustar_kernel(DevState d) { ibm_ustar_kernel_body<FUSED>(d, blockIdx.x); }
 
 // r = ub - X u* (boundary_condition.f90:1540-1555, 1609-1629) and the band
 // index of each (segment, slot); one warp per segment, slots 0..35 over the
@@ -594,11 +580,10 @@ __global__ void ibm_spread_kernel_multi(MultiArgs m) {
     ibm_spread_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// du back to FP64, velocity correction and body force (plain path fields),
+// Plain path: du back to FP64, velocity correction and body force fields,
 // and per-block partial sums of each wing's force and moment over the
 // block's contiguous slice of the band list (each wing owns a contiguous
-// range: claim order).
-template <bool FUSED>
+// range: claim order).  The FP32 path does this in its closing kernel.
 __device__ __forceinline__ void ibm_finish_kernel_body(const DevState& d, const int bid_) {
     constexpr int NWARP = FINISH_THREADS / 32;
     __shared__ double red[NWARP][3];
@@ -618,7 +603,7 @@ __device__ __forceinline__ void ibm_finish_kernel_body(const DevState& d, const 
         const double rh = d.band_rho[b];
         t1 = 2.0 * rh * du;
         t2 = 2.0 * rh * dv;
-        if (!FUSED) {
+        {
             const long long p = pidx(d, i, j);
             d.u[p] = d.band_us[b] + du;
             d.v[p] = d.band_vs[b] + dv;
@@ -662,8 +647,7 @@ __device__ __forceinline__ void ibm_finish_kernel_body(const DevState& d, const 
         __syncthreads();
     }
 }
-template <bool FUSED>
-__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) { ibm_finish_kernel_body<FUSED>(d, blockIdx.x); }
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) { ibm_finish_kernel_body(d, blockIdx.x); }
 
 // Per-wing force and moment from the block partials (in block order), the
 // no-slip residual when diagnostics are on, and the force row; run by one
@@ -962,7 +946,7 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
         ibm_rhs_fused_kernel<<<rhs_grid(d), 128, 0, st>>>(d);
         return;
     }
-    ibm_ustar_kernel<false><<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
+    ibm_ustar_kernel<<<blocks(d.band_cap, 128), 128, 0, st>>>(d);
     ibm_rhs_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
 }
 
@@ -977,7 +961,7 @@ void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t s
             ibm_close_kernel<false><<<close_grid(d), FINISH_THREADS, 0, st>>>(d);
         return;
     }
-    ibm_finish_kernel<false><<<nbk, FINISH_THREADS, 0, st>>>(d);
+    ibm_finish_kernel<<<nbk, FINISH_THREADS, 0, st>>>(d);
     ibm_forces_kernel<<<1, 256, 0, st>>>(d);
 }
 
