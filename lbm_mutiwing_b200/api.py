@@ -318,12 +318,16 @@ class Simulation:
 
 class BatchStepError(LbmError):
     """Raised by Batch.step when episodes failed; rcs[i] != 0 marks them and
-    messages[i] holds each failed episode's error text."""
+    messages[i] holds each failed episode's error text.  When some rcs are
+    non-zero the call did step every episode (an episode fails its status
+    check after the steps): outs[i] holds the force rows of the others, whose
+    cycles have advanced."""
 
-    def __init__(self, msg, rcs, messages):
+    def __init__(self, msg, rcs, messages, outs=None):
         super().__init__(msg)
         self.rcs = rcs
         self.messages = messages
+        self.outs = outs if outs is not None else [None] * len(rcs)
 
 
 class Batch:
@@ -381,7 +385,13 @@ class Batch:
         if rc != 0:
             codes = list(rcs)
             msgs = [sims[i].L.lbm_last_error(sims[i].h).decode() if codes[i] else "" for i in range(n)]
-            raise BatchStepError(self.L.lbm_batch_last_error(self.h).decode(), codes, msgs)
+            stepped = any(codes)
+            if stepped:
+                for s, f0, k, c in zip(sims, first, ns, codes):
+                    if not c:
+                        s.cycle = f0 + k
+            raise BatchStepError(self.L.lbm_batch_last_error(self.h).decode(), codes, msgs,
+                                 [o if stepped and not c else None for o, c in zip(outs, codes)])
         for s, f0, k in zip(sims, first, ns):
             s.cycle = f0 + k
         return outs

@@ -75,11 +75,13 @@ class _StepRequest:
 
 class PackedStepper:
     """Continuous batching of step requests over FP32 episodes (see the
-    module text).  ``step`` has the signature of ``Simulation.step``."""
+    module text).  ``step`` has the signature of ``Simulation.step``.
+    ``batch`` (default: an ``api.Batch`` on ``device``) is anything with
+    ``step(sims, n_steps, first_cycles=, rows=, flags=)`` and ``close()``."""
 
-    def __init__(self, device: int = 0, chunk: int = 200):
+    def __init__(self, device: int = 0, chunk: int = 200, batch=None):
         self.chunk = chunk
-        self.batch = api.Batch(device)
+        self.batch = batch if batch is not None else api.Batch(device)
         self.cv = threading.Condition()
         self.pending: List[_StepRequest] = []
         self.closed = False
@@ -125,10 +127,12 @@ class PackedStepper:
                                            rows=True, flags=fl)
                 failed = [None] * len(active)
             except api.BatchStepError as e:
+                # episodes that failed their status check fail alone; the
+                # others were stepped and keep their rows
                 failed = [api.LbmError(m) if c else None for c, m in zip(e.rcs, e.messages)]
+                outs = list(e.outs)
                 if not any(failed):
                     failed = [api.LbmError(str(e))] * len(active)
-                outs = [None] * len(active)
             except Exception as e:   # noqa: BLE001 - handed to the waiting requests
                 failed = [e] * len(active)
                 outs = [None] * len(active)

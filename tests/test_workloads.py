@@ -44,3 +44,14 @@ def test_mixed_batch_is_seeded():
     assert [e.nx for e in a] == [e.nx for e in b]
     assert all(np.array_equal(x.motion, y.motion) for x, y in zip(a, b))
     assert {e.nx for e in wl.mixed_batch(64, steps=2)} <= {401, 801, 1201, 2001}
+
+
+def test_arc_spacing_is_even_and_closed():
+    # the default marker spacing: equal arc length along each surface
+    pts = wl.naca_loop(0.12, 200)
+    seg = np.hypot(*np.diff(pts * 100.0, axis=0).T)   # chord of 100 lattice spacings
+    assert 1.0 <= seg.min() and seg.max() <= 1.03
+    assert np.array_equal(pts[0], pts[-1])
+    assert abs(pts[100, 0] - 0.75) < 1e-15 and abs(pts[100, 1]) < 1e-15
+    cos = np.hypot(*np.diff(wl.naca_loop(0.12, 200, "cosine") * 100.0, axis=0).T)
+    assert cos.min() < 0.03   # what the arc spacing avoids
