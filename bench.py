@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--workload", default="4000x2000", choices=["800x400", "4000x2000", "16000x8000"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the batched and served measurements")
+    p.add_argument("--packed", action="store_true",
+                   help="only the 64-episode mixed batch in packed launches (lbm_batch_step): W warm-up steps, "
+                        "then K timed steps; one JSON line (for profiling the packed kernels)")
     return p.parse_args()
 
 
@@ -377,10 +380,37 @@ def run_ours(args):
     ranks.finish()
 
 
+def run_packed(args):
+    """The seeded 64-episode mixed batch, every kernel of a step one launch
+    over all episodes: W warm-up steps (long enough, from 8, to let the
+    engine tune its bulk kernel), then K timed steps (wall clock around the
+    synchronous call)."""
+    from lbm_mutiwing_b200 import api, batch, build
+    from lbm_mutiwing_b200 import workloads as wl
+    build.build()
+    K, Wm = args.steps, max(3, args.warmup)
+    eps = wl.mixed_batch(64, steps=K + Wm + 8)
+    nodes = sum(e.nx * e.ny for e in eps)
+    sims = batch.create(eps, api.PRECISION_FP32)
+    packed = api.Batch(0)
+    batch.advance_packed(sims, Wm, first_cycle=1, packed=packed)
+    wall = batch.advance_packed(sims, K, first_cycle=1 + Wm, packed=packed)
+    packed.close()
+    for s in sims:
+        s.close()
+    print(json.dumps({"metric": METRIC, "value": nodes * K / wall / 1e6, "unit": UNIT, "n_gpus": 1, "steps": K,
+                      "warmup": Wm, "ms_per_step": wall / K * 1e3, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": "mixed64_packed", "episodes": len(eps), "nodes": nodes,
+                                 "wings": sum(e.wing_count for e in eps)}}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.packed:
+        run_packed(args)
     else:
         run_ours(args)
 
