@@ -145,7 +145,8 @@ int lbm_err(LbmHandle* h, double* err);
  * serialised by the caller.  The first call on each device looks the array
  * up (cudaGetSymbolAddress); make it before any stream capture begins.
  * Kernels run on `stream` (a cudaStream_t, NULL for the default stream) of
- * `device`; the call waits for them and writes err on the host.  Returns 0,
+ * `device`; every call then synchronises `stream` and copies err to the
+ * host before it returns.  Returns 0,
  * or -1 (bad argument), -2 (too many rows), -3 (CUDA error) with the text in
  * msg (msg_cap bytes, may be NULL).  The caller's current device is kept. */
 #define LBM_NOALLOC_MAX_ROWS 16384

@@ -28,7 +28,6 @@ STEP_FIELDS = 1
 STEP_ERR = 2
 FLAG_NO_GRAPHS = 1
 FLAG_SOLVE_STREAM = 2
-FLAG_NO_GRAPHS = 1
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}
@@ -320,8 +319,8 @@ class BatchStepError(LbmError):
     """Raised by Batch.step when episodes failed; rcs[i] != 0 marks them and
     messages[i] holds each failed episode's error text.  When some rcs are
     non-zero the call did step every episode (an episode fails its status
-    check after the steps): outs[i] holds the force rows of the others, whose
-    cycles have advanced."""
+    check after the steps): outs[i] holds the force rows of the others, and
+    every episode's cycle has advanced with its device state."""
 
     def __init__(self, msg, rcs, messages, outs=None):
         super().__init__(msg)
@@ -387,9 +386,10 @@ class Batch:
             msgs = [sims[i].L.lbm_last_error(sims[i].h).decode() if codes[i] else "" for i in range(n)]
             stepped = any(codes)
             if stepped:
-                for s, f0, k, c in zip(sims, first, ns, codes):
-                    if not c:
-                        s.cycle = f0 + k
+                # every episode was stepped (the failed ones failed their
+                # status check afterwards): host cycles follow the device
+                for s, f0, k in zip(sims, first, ns):
+                    s.cycle = f0 + k
             raise BatchStepError(self.L.lbm_batch_last_error(self.h).decode(), codes, msgs,
                                  [o if stepped and not c else None for o, c in zip(outs, codes)])
         for s, f0, k in zip(sims, first, ns):

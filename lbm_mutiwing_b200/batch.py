@@ -161,6 +161,53 @@ class PackedStepper:
         self.batch.close()
 
 
+class PackedEngine:
+    """The packed engine of one GPU for ``sharded_packed_run``: creates FP32
+    episodes on ``device`` and advances them with ``lbm_batch_step``."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.batch = None
+
+    def create(self, eps: Sequence) -> List[api.Simulation]:
+        self.batch = api.Batch(self.device)
+        return create(eps, api.PRECISION_FP32, device=self.device)
+
+    def advance(self, sims, steps: int, first_cycle: int) -> float:
+        return advance_packed(sims, steps, first_cycle=first_cycle, packed=self.batch)
+
+    def close(self, sims) -> None:
+        for s in sims:
+            s.close()
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
+
+
+def sharded_packed_run(eps: Sequence, steps: int, warmup: int, rank: int, world: int, engine=None,
+                       barrier=None) -> Tuple[List[int], int, float]:
+    """This rank's shard of the episodes (balanced by node count with
+    ``ranks.shard``; the shards partition the episodes and need no data
+    exchange) advanced ``warmup`` untimed and then ``steps`` timed packed
+    steps on this rank's GPU.  Returns (episode indices, node updates of the
+    timed steps, wall seconds of the timed call, which returns once the
+    device work is done).  ``barrier`` (optional) runs just before the timed
+    call on every rank."""
+    from . import ranks
+    mine = ranks.shard([float(e.nx * e.ny) for e in eps], world)[rank]
+    engine = engine if engine is not None else PackedEngine()
+    sims = engine.create([eps[i] for i in mine])
+    try:
+        if sims:
+            engine.advance(sims, warmup, 1)
+        if barrier is not None:
+            barrier()
+        seconds = engine.advance(sims, steps, 1 + warmup) if sims else 0.0
+    finally:
+        engine.close(sims)
+    return mine, sum(eps[i].nx * eps[i].ny for i in mine) * steps, seconds
+
+
 def advance_one_at_a_time(eps: Sequence, steps: int, precision: int = api.PRECISION_FP64,
                           device: int = 0, warmup: int = 2) -> Tuple[float, int]:
     """Each episode alone (created, warmed up, timed, destroyed) in turn;

@@ -198,6 +198,14 @@ struct LbmHandle {
     cudaGraphExec_t gexec[2][GEO_SETS] = {};
     double* d_out = nullptr;        // strided output fields (SAVE)
     size_t out_cap = 0;   // by starting plane parity and geometry set
+    // Continuation state: the cycle the device counters hold after the last
+    // call (-1: unknown), and, on the fused path, the cycle whose geometry
+    // the last step of that call built into set gset (-1: none, or made
+    // stale by a change of motion or lattice shift).  A call that continues
+    // at next_cycle with a valid geometry writes no counter and builds no
+    // geometry before its first step.
+    int64_t next_cycle = -1;
+    int64_t geo_ready = -1;
 };
 
 // Packed stepping of many fused-path handles (lbm_batch_step): one launch per
@@ -397,6 +405,8 @@ int init_state(LbmHandle* h) {
     h->d.movenum = 0;
     h->fields_valid = false;
     h->err_valid = false;
+    h->next_cycle = 1;
+    h->geo_ready = -1;
     CK(cudaDeviceSynchronize());
     return 0;
 }
@@ -1013,6 +1023,7 @@ int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_
     if (dalloc(h, &h->d_step_table, st.size())) return -1;
     CK(cudaMemcpy(h->d_step_table, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->d.step_table = h->d_step_table;
+    h->geo_ready = -1;
     drop_graphs(h);
     h->d.step_rows = steps;
     h->d.motion_dt = dt;
@@ -1028,6 +1039,7 @@ int lbm_set_stream_rows(LbmHandle* h, const double* start_row, const double* tar
     CK(cudaMemcpyAsync(h->d.stream_start, h->pinned, nc * sizeof(double), cudaMemcpyHostToDevice, h->s_main));
     CK(cudaMemcpyAsync(h->d.stream_target, h->pinned + nc, nc * sizeof(double), cudaMemcpyHostToDevice, h->s_main));
     CK(cudaStreamSynchronize(h->s_main));
+    h->geo_ready = -1;   // the geometry built ahead followed the previous rows
     return 0;
 }
 
@@ -1058,22 +1070,44 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
         return fail(h, "no motion table loaded");
     CK(cudaSetDevice(h->cfg.device));
     if (ensure_rows(h, n_steps)) return -1;
-    long long init[2] = {(long long)first_cycle, 0};
-    CK(cudaMemcpyAsync(h->d.cycle, &init[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
-    CK(cudaMemcpyAsync(h->d.gcycle, &init[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
-    CK(cudaMemcpyAsync(h->d.row_index, &init[1], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
-    CK(cudaStreamSynchronize(h->s_main));
+    const bool fused = h->d.precision != 0;
+    // The counters (cycle, the geometry's cycle) are written only when the
+    // call does not continue where the last one ended, and then from pinned
+    // memory without a host wait (the previous call ended with a stream
+    // synchronisation, so the staging words are free).  On the fused path
+    // the last step of every call builds the next step's geometry; a
+    // continuing call starts from it, any other call builds its first
+    // geometry before its first step.
+    const bool cont = first_cycle == h->next_cycle;
+    const bool have_geo = fused && cont && h->geo_ready == first_cycle;
+    long long* stage = reinterpret_cast<long long*>(h->pinned + h->pinned_n - 2);
+    if (!cont && n_steps > 0) {
+        stage[0] = (long long)first_cycle;
+        CK(cudaMemcpyAsync(h->d.cycle, &stage[0], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
+    }
+    if (!have_geo && n_steps > 0) {
+        stage[1] = (long long)first_cycle;
+        CK(cudaMemcpyAsync(h->d.gcycle, &stage[1], sizeof(long long), cudaMemcpyHostToDevice, h->s_main));
+    }
+    CK(cudaMemsetAsync(h->d.row_index, 0, sizeof(long long), h->s_main));
+    if (n_steps > 0) h->next_cycle = h->geo_ready = -1;   // until the steps are enqueued
     const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
     const bool want_err = (flags & LBM_STEP_ERR) != 0;
     // all but the last two steps replay a two-step CUDA graph; the last two
     // may write fields or diagnostics and are launched directly
     const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
-    const bool fused = h->d.precision != 0;
-    if (fused && n_steps > 0) prime_geometry(h, n_steps);
+    if (fused && n_steps > 0 && !have_geo) prime_geometry(h, n_steps);
     int64_t n = 0;
-    if (graphs && fused) {
-        // whole graphs while the last two steps and the geometry they need
-        // stay outside
+    if (graphs && fused && n + GRAPH_STEPS <= n_steps - 2) {
+        // Both graphs a run can meet (plane parity and geometry set advance
+        // together, so after an odd step count the next call starts from the
+        // other pair) are built by the first call that replays one, so later
+        // calls capture nothing.
+        for (int q = 0; q < 2; ++q) {
+            const int p = h->parity ^ q, g = (h->gset + q) % GEO_SETS;
+            if (!h->gexec[p][g] && build_graph(h, p, g)) return -1;
+        }
+        // whole graphs while the last two steps stay outside
         for (; n + GRAPH_STEPS <= n_steps - 2; n += GRAPH_STEPS) {
             cudaGraphExec_t& ge = h->gexec[h->parity][h->gset];
             if (!ge && build_graph(h, h->parity, h->gset)) return -1;
@@ -1098,11 +1132,15 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
             }
             fields = true;
         }
-        enqueue_step(h, fields, last, n + GEO_AHEAD <= n_steps - 1, false);
+        enqueue_step(h, fields, last, true, false);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->s_main));
     CK(cudaGetLastError());
+    if (n_steps > 0) {
+        h->next_cycle = first_cycle + n_steps;
+        h->geo_ready = fused ? first_cycle + n_steps : -1;
+    }
     if (h->timing) collect_phase_times(h);
     if (force_rows && n_steps > 0)
         CK(cudaMemcpy(force_rows, h->d_rowbuf, sizeof(double) * h->row_len * n_steps, cudaMemcpyDeviceToHost));
@@ -1263,6 +1301,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     const DevState* dvar = reinterpret_cast<const DevState*>(b->d_buf + off_var);
     for (size_t q = 0; q < pool.size(); ++q) ptrs[q] = dvar + pool[q];
     cudaStream_t sm = b->s_main;
+    for (int i = 0; i < nh; ++i) hs[i]->next_cycle = hs[i]->geo_ready = -1;   // until the call completes
     BCK(cudaMemcpyAsync(b->d_buf, b->h_buf, total, cudaMemcpyHostToDevice, sm));
     for (int i = 0; i < nh; ++i) {
         for (long long* c : {hs[i]->d.cycle, hs[i]->d.gcycle})
@@ -1404,6 +1443,9 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         const int32_t fl = flags ? flags[i] : 0;
         const bool want_fields = (fl & LBM_STEP_FIELDS) != 0, want_err = (fl & LBM_STEP_ERR) != 0;
         for (bool& q : h->pending) q = false;
+        // packed steps leave no geometry built ahead for a later lbm_step
+        h->next_cycle = first_cycle[i] + ns;
+        h->geo_ready = -1;
         int rc = 0;
         if (ns > 0) {
             h->parity ^= (int)(ns & 1);
@@ -1676,6 +1718,7 @@ int lbm_set_border_f0(LbmHandle* h, const double* f0, int32_t movenum) {
     CK(cudaDeviceSynchronize());
     if (f0 && border_f0_copy(h, const_cast<double*>(f0), true)) return -1;
     h->d.movenum = movenum;
+    h->geo_ready = -1;
     drop_graphs(h);   // movenum is baked into the step graphs
     return 0;
 }
@@ -1694,6 +1737,7 @@ int lbm_move_mesh(LbmHandle* h, int32_t dr) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s_main));
     h->d.movenum += dr;
+    h->geo_ready = -1;
     drop_graphs(h);
     return 0;
 }

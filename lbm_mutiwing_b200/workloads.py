@@ -131,6 +131,8 @@ class Episode:
     markers: List[np.ndarray] = dataclasses.field(default_factory=list)
     motion: np.ndarray | None = None
     steps: int = 0
+    # draws of a seeded workload that the domain's size capped (mixed_batch)
+    meta: dict = dataclasses.field(default_factory=dict)
 
     @property
     def wing_count(self) -> int:
@@ -238,12 +240,16 @@ def mixed_batch(count: int = 64, seed: int = 20261203, steps: int = 1000) -> Lis
         nm = int(rng.integers(100, 301))
         ep.markers = [naca_loop(th, nm) for _ in range(nw)]
         wings = []
+        heave_capped = 0
         for k in range(nw):
-            wings.append(WingMotion(x=x0 + k * spacing_x, y=0.0,
-                                    pitch_amp=float(rng.uniform(5, 25)) * math.pi / 180.0,
-                                    heave_amp=min(float(rng.uniform(0.1, 0.6)), 0.3 * h - 0.5),
+            pitch = float(rng.uniform(5, 25)) * math.pi / 180.0
+            heave_draw = float(rng.uniform(0.1, 0.6))
+            heave_capped += heave_draw > 0.3 * h - 0.5
+            wings.append(WingMotion(x=x0 + k * spacing_x, y=0.0, pitch_amp=pitch,
+                                    heave_amp=min(heave_draw, 0.3 * h - 0.5),
                                     freq=float(rng.uniform(0.2, 1.0)),
                                     phase=float(rng.uniform(0, 2 * math.pi))))
+        ep.meta = {"wings_drawn": nw_draw, "wings_placed": nw, "heave_capped": int(heave_capped)}
         ep.motion = motion_table(wings, (steps + 1) * 0.01 * ep.uu, 0.01 * ep.uu)
         eps.append(ep)
     return eps

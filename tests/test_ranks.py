@@ -59,3 +59,63 @@ def test_single_rank_needs_no_process_group():
     assert ranks.allmax(3.5) == 3.5
     ranks.barrier()
     assert ranks.whole_job_rate(10.0, 1, 2.0) == 5.0
+
+
+class _FakeEngine:
+    """Stands in for the packed GPU engine: 'episodes' are names, advancing
+    records (episode, first cycle, steps) and takes a time proportional to
+    the node updates of the call."""
+
+    def __init__(self, log):
+        self.log = log
+
+    def create(self, eps):
+        return [e.name for e in eps]
+
+    def advance(self, sims, steps, first_cycle):
+        for s in sims:
+            self.log.append((s, first_cycle, steps))
+        return 1e-9 * steps * len(sims)
+
+    def close(self, sims):
+        self.log.append(("closed", len(sims)))
+
+
+def _batch_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from lbm_mutiwing_b200 import batch, workloads as wl
+    r, w, _ = ranks.init("gloo", timeout_s=60)
+    eps = wl.mixed_batch(16, steps=4)
+    log = []
+    mine, nu, sec = batch.sharded_packed_run(eps, 10, 3, r, w, engine=_FakeEngine(log), barrier=ranks.barrier)
+    smax = ranks.allmax(sec)
+    out.put((r, mine, nu, smax, log))
+    ranks.finish()
+
+
+def test_sharded_packed_batch_over_two_gloo_ranks():
+    """The mixed batch split over two ranks: every episode is advanced by
+    exactly one rank (warm-up from cycle 1, timed steps after it), the node
+    updates add up to the whole batch's, and both ranks see the slowest
+    rank's time."""
+    from lbm_mutiwing_b200 import workloads as wl
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in procs), key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    eps = wl.mixed_batch(16, steps=4)
+    (_, m0, n0, t0, log0), (_, m1, n1, t1, log1) = res
+    assert sorted(m0 + m1) == list(range(16)) and not set(m0) & set(m1)
+    assert n0 + n1 == sum(e.nx * e.ny for e in eps) * 10
+    assert t0 == t1 == max(1e-9 * 10 * len(m0), 1e-9 * 10 * len(m1))
+    for mine, log in ((m0, log0), (m1, log1)):
+        names = [eps[i].name for i in mine]
+        assert [x for x in log if x[0] != "closed"] == [(n, 1, 3) for n in names] + [(n, 4, 10) for n in names]
+        assert log[-1] == ("closed", len(mine))

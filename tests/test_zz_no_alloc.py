@@ -74,8 +74,13 @@ def test_noalloc_err_matches_lbm_err_twice(precision):
     L = api.load_library()
     ptrs = [x.data_ptr() for x in t]
     r1 = _call(L, ptrs, nx, ny, nx)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
     r2 = _call(L, ptrs, nx, ny, nx)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info(0)[0]
     assert r1[0] == 0 and r2[0] == 0, (r1, r2)
+    assert free_after == free_before            # the second call takes no device memory
     assert r1[1] == r2[1]                       # deterministic from call to call
     assert abs(r1[1] - ref) <= 1e-12 * ref      # same sums as lbm_err, other order
     assert abs(r1[1] - _oracle_order(u, v, u0, v0)) <= 1e-12 * ref
