@@ -207,6 +207,12 @@ void* lbm_stream(LbmHandle* h);
 /* Device memory the handle holds, in bytes. */
 int64_t lbm_device_bytes(const LbmHandle* h);
 
+/* Free and total memory of a CUDA device (cudaMemGetInfo), for admitting new
+ * episodes by the memory they would take: the online driver creates one
+ * episode per RESET (reset_zmq_episode, driver.f90:205-258).  The caller's
+ * current device is kept. */
+int lbm_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
+
 const char* lbm_last_error(const LbmHandle* h);
 void lbm_destroy(LbmHandle* h);
 

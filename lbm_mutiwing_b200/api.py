@@ -76,6 +76,7 @@ SIGNATURES = [
     ("lbm_get_phase_times", C.c_int, [C.c_void_p, D, C.c_int32]),
     ("lbm_stream", C.c_void_p, [C.c_void_p]),
     ("lbm_device_bytes", C.c_int64, [C.c_void_p]),
+    ("lbm_mem_info", C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("lbm_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_destroy", None, [C.c_void_p]),
     ("lbm_batch_create", C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
@@ -112,6 +113,25 @@ def load_library(path: str = LIB_PATH):
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(D)
+
+
+def mem_info(device: int = 0):
+    """(free, total) bytes of the device (lbm_mem_info)."""
+    L = load_library()
+    fr, to = C.c_int64(0), C.c_int64(0)
+    if L.lbm_mem_info(device, C.byref(fr), C.byref(to)) != 0:
+        raise LbmError(f"cannot query the memory of CUDA device {device}")
+    return fr.value, to.value
+
+
+def estimate_device_bytes(ep, precision: int) -> int:
+    """Upper bound of the device memory an episode takes before it is
+    created: per node the distributions (FP32 path: two copies of nine FP32
+    planes; FP64 path: f and f0 in FP64 and eight FP64 fields), the band maps
+    and bit planes, and the fields written on request (FP32 path), plus a
+    fixed 64 MB for the immersed-boundary arrays, force rows and graphs."""
+    per_node = 120 if precision == PRECISION_FP32 else 212
+    return per_node * ep.nx * ep.ny + (64 << 20)
 
 
 def default_s() -> list:

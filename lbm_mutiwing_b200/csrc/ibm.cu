@@ -241,6 +241,7 @@ __device__ __forceinline__ void ibm_geometry_kernel_body(const DevState& d, cons
         if (d.precision == 0) { d.gfx[p] = 0.0; d.gfy[p] = 0.0; }
     }
     if (t == 0 && d.wing_count > 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
+    if (t == 0) d.ibm_flags[0] = 0;   // set again by the count kernel when supports share nodes
 }
 __global__ void ibm_geometry_kernel(DevState d) { ibm_geometry_kernel_body(d, blockIdx.x); }
 __global__ void ibm_geometry_kernel_multi(MultiArgs m) {
@@ -268,14 +269,30 @@ __global__ void ibm_claim_kernel_multi(MultiArgs m) {
     ibm_claim_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
+// Claims per segment, and the coupling test: a box node claimed by a
+// segment of another wing lies in the supports of both wings, so G has
+// entries between them and the wings are solved jointly (the lowest segment
+// index claims a node, hence every shared node is seen from the higher
+// wing's side).
 __device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const int bid_) {
     const int s = bid_ * blockDim.x + threadIdx.x;
     if (s >= d.nseg) return;
     int c = 0;
-    if (!box_empty(d, s))
+    bool shared = false;
+    if (!box_empty(d, s)) {
+        const int w = d.seg_wing[s];
         for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
-            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) c += (d.band_map[pidx(d, i - 1, j - 1)] == s);
+            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
+                const int bm = d.band_map[pidx(d, i - 1, j - 1)];
+                c += (bm == s);
+                shared |= bm != s && bm >= 0 && bm < d.nseg && d.seg_wing[bm] != w;
+            }
+    }
     d.claim_cnt[s] = c;
+    if (shared) {
+        d.ibm_flags[0] = 1;
+        set_status(d, ST_WINGS_COUPLED);
+    }
 }
 __global__ void ibm_count_kernel(DevState d) { ibm_count_kernel_body(d, blockIdx.x); }
 __global__ void ibm_count_kernel_multi(MultiArgs m) {
@@ -283,13 +300,10 @@ __global__ void ibm_count_kernel_multi(MultiArgs m) {
     ibm_count_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// Exclusive scan of the claim counts (one block), band size, and the check
-// whether two wings' supports overlap (coupled solve).
+// Exclusive scan of the claim counts (one block) and the band size.
 __device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const int bid_) {
     __shared__ int wsum[32];
-    __shared__ int wbox[MAX_WINGS][4];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < d.wing_count) { wbox[tid][0] = 0x7fffffff; wbox[tid][1] = -1; wbox[tid][2] = 0x7fffffff; wbox[tid][3] = -1; }
     const int per = (d.nseg + nt - 1) / nt;
     const int lo = min(d.nseg, tid * per), hi = min(d.nseg, lo + per);
     int lsum = 0;
@@ -311,11 +325,6 @@ __device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const in
         const int c = d.claim_cnt[s];
         d.claim_cnt[s] = run;
         run += c;
-        if (!box_empty(d, s)) {
-            const int w = d.seg_wing[s];
-            atomicMin(&wbox[w][0], d.box[4 * s]); atomicMax(&wbox[w][1], d.box[4 * s + 1]);
-            atomicMin(&wbox[w][2], d.box[4 * s + 2]); atomicMax(&wbox[w][3], d.box[4 * s + 3]);
-        }
     }
     __syncthreads();
     if (tid == 0) {
@@ -323,14 +332,6 @@ __device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const in
         if (tot > d.band_cap) set_status(d, ST_BAND_OVERFLOW);
         d.band_n[0] = nb;
         d.claim_cnt[d.nseg] = nb;
-        int coupled = 0;
-        for (int a = 0; a < d.wing_count; ++a)
-            for (int b = a + 1; b < d.wing_count; ++b)
-                if (wbox[a][0] <= wbox[b][1] && wbox[b][0] <= wbox[a][1] && wbox[a][2] <= wbox[b][3] &&
-                    wbox[b][2] <= wbox[a][3])
-                    coupled = 1;
-        d.ibm_flags[0] = coupled;
-        if (coupled) set_status(d, ST_WINGS_COUPLED);
     }
 }
 __global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) { ibm_scan_kernel_body(d, blockIdx.x); }

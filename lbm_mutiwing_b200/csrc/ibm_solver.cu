@@ -307,6 +307,211 @@ __host__ __device__ inline int ring_slots(int bw) { return (bw + PANEL + RING_RO
 size_t ibm_solve_ring_bytes(int bw) { return (size_t)ring_slots(bw) * (RING_ROWS + 1) * ibm_ld(bw) * sizeof(double); }
 bool ibm_solve_ring_fits(int bw) { return ring_slots(bw) <= RING_MAX_SLOTS; }
 
+// ------------------------------------------------- joint solve of coupled wings
+// When two wings' supports share lattice nodes, G has entries between their
+// segments and the per-wing factors alone solve a different system from the
+// reference's one dense system over all segments (boundary_condition.f90:
+// 1609-1640).  The joint system G y = r is then solved by conjugate
+// gradients preconditioned with the per-wing factors (G is symmetric
+// positive definite, the preconditioner block diagonal), starting from the
+// per-wing solution.  One warp per velocity component; products G p are
+// formed as X (X^T p): a spread onto the band nodes with 64-bit fixed-point
+// integer atomics (order-independent, so results are reproducible) and an
+// interpolation back; dot products are lane-strided sums added by a fixed
+// butterfly.  The iteration stops when the recursive residual is below
+// CG_TOL of |r|, or after CG_MAXIT iterations (then ST_COUPLED_NOCONV).
+constexpr int CG_MAXIT = 200;
+constexpr double CG_TOL = 1e-13;
+
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// out = G in for one component; acc holds that component's band
+// accumulators, zero on entry and left zero.
+__device__ void cg_product(const DevState& d, const double* in, double* out, unsigned long long* acc, int lane) {
+    double m = 0.0;
+    for (int s = lane; s < d.nseg; s += 32) m = fmax(m, fabs(__ldcg(in + s)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int e2 = 0;
+    frexp(m > 0.0 ? 1024.0 * m : 1.0, &e2);
+    const int e = 62 - e2;   // every contribution below 2^52 after scaling, as in the spread
+    const int n = d.nseg * BOX_SLOTS;
+    for (int t = lane; t < n; t += 32) {
+        const int bi = d.pb[t];
+        if (bi < 0) continue;
+        const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
+        const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
+        atomicAdd(acc + bi, (unsigned long long)__double2ll_rn(ldexp(wv * __ldcg(in + s), e)));
+    }
+    __syncwarp();
+    for (int s = lane; s < d.nseg; s += 32) {
+        double v = 0.0;
+        for (int slot = 0; slot < BOX_SLOTS; ++slot) {
+            const int bi = d.pb[s * BOX_SLOTS + slot];
+            if (bi < 0) continue;
+            const double wv = d.kx[6 * s + slot / 6] * d.ky[6 * s + slot % 6];
+            v = v + wv * ldexp((double)(long long)__ldcg(acc + bi), -e);
+        }
+        out[s] = v;
+    }
+    __syncwarp();
+    for (int t = lane; t < n; t += 32) {
+        const int bi = d.pb[t];
+        if (bi >= 0) __stcg(acc + bi, 0ull);
+    }
+    __syncwarp();
+}
+
+// out = D^-1 in for one component, D the block-diagonal part of G: each
+// wing's forward and backward substitution with its banded factor and
+// per-panel inverses read from global memory, one warp, z a shared-memory
+// vector of at least nw_max + PANEL + bw_max doubles.
+__device__ void cg_precondition(const DevState& d, const double* in, double* out, double* z, int lane) {
+    const int li = lane & (PANEL - 1);
+    for (int w = 0; w < d.wing_count; ++w) {
+        const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+        const int npan = (nw + PANEL - 1) / PANEL;
+        const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
+        const double* L = d.linv + d.wing_linv_ofs[w];
+        const int* perm = d.perm + s0;
+        for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? in[perm[p]] : 0.0;
+        __syncwarp();
+        for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {   // L' D v = r
+            const int np = min(PANEL, nw - k0);
+            const double* Li = L + pan * IBM_PANEL_AUX;
+            double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < PANEL / 2; ++k) {
+                w0 = w0 + Li[li * PANEL + k] * z[k0 + k];
+                w1 = w1 + Li[li * PANEL + k + PANEL / 2] * z[k0 + k + PANEL / 2];
+            }
+            const double wl = w0 + w1;
+            double wc[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
+            for (int rb = lane; rb < bw; rb += 32) {
+                const int i = k0 + np + rb;
+                const double* row = A + (long long)i * ld + (i - k0);
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + row[-c] * wc[c];
+                    a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
+                }
+                z[i] -= a0 + a1;
+            }
+            if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
+            __syncwarp();
+        }
+        for (int pan = npan - 1; pan >= 0; --pan) {   // L'^T y = v
+            const int k0 = pan * PANEL;
+            const double* Li = L + pan * IBM_PANEL_AUX;
+            double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < PANEL / 2; ++k) {
+                y0 = y0 + Li[k * PANEL + li] * z[k0 + k];
+                y1 = y1 + Li[(k + PANEL / 2) * PANEL + li] * z[k0 + k + PANEL / 2];
+            }
+            const double yl = y0 + y1;
+            double yc[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
+            const int above = min(bw, k0);
+            for (int r = lane; r < above; r += 32) {
+                const int j = k0 - 1 - r;
+                const double* col = A + (long long)k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + col[c * (ld + 1)] * yc[c];
+                    a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
+                }
+                z[j] -= a0 + a1;
+            }
+            if (lane < PANEL) z[k0 + lane] = yl;
+            __syncwarp();
+        }
+        for (int p = lane; p < nw; p += 32) out[perm[p]] = z[p];
+        __syncwarp();
+    }
+}
+
+// The joint solve, warp `comp` for velocity component comp: y (rx or ry)
+// holds the per-wing solution on entry and the joint one on exit; the
+// right-hand side is qx or qy as the rhs kernel built it; the spread scale
+// of every wing (ymax) is recomputed.  y was written by the other wing
+// blocks, so it is read past the L1 cache (__ldcg).
+__device__ void cg_joint_solve(const DevState& d, double* z, int comp, int lane) {
+    const int n = d.nseg;
+    double* y = comp ? d.ry : d.rx;
+    const double* r0 = comp ? d.qy : d.qx;
+    double* res = d.cg_work + (size_t)(4 * comp + 0) * n;
+    double* zz = d.cg_work + (size_t)(4 * comp + 1) * n;
+    double* p = d.cg_work + (size_t)(4 * comp + 2) * n;
+    double* q = d.cg_work + (size_t)(4 * comp + 3) * n;
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(comp ? d.band_dv : d.band_du);
+    cg_product(d, y, q, acc, lane);
+    double rr0 = 0.0, rn = 0.0;
+    for (int s = lane; s < n; s += 32) {
+        const double rs = r0[s] - q[s];
+        res[s] = rs;
+        rr0 += r0[s] * r0[s];
+        rn += rs * rs;
+    }
+    rr0 = warp_sum(rr0);
+    rn = warp_sum(rn);
+    __syncwarp();
+    const double tol2 = CG_TOL * CG_TOL * rr0;
+    double rz = 0.0;
+    if (rn > tol2) {
+        cg_precondition(d, res, zz, z, lane);
+        for (int s = lane; s < n; s += 32) {
+            p[s] = zz[s];
+            rz += res[s] * zz[s];
+        }
+        rz = warp_sum(rz);
+        __syncwarp();
+    }
+    int it = 0;
+    for (; rn > tol2 && it < CG_MAXIT; ++it) {
+        cg_product(d, p, q, acc, lane);
+        double pq = 0.0;
+        for (int s = lane; s < n; s += 32) pq += p[s] * q[s];
+        pq = warp_sum(pq);
+        if (!(pq > 0.0)) break;
+        const double alpha = rz / pq;
+        rn = 0.0;
+        for (int s = lane; s < n; s += 32) {
+            y[s] = __ldcg(y + s) + alpha * p[s];
+            res[s] -= alpha * q[s];
+            rn += res[s] * res[s];
+        }
+        rn = warp_sum(rn);
+        __syncwarp();
+        cg_precondition(d, res, zz, z, lane);
+        double rz1 = 0.0;
+        for (int s = lane; s < n; s += 32) rz1 += res[s] * zz[s];
+        rz1 = warp_sum(rz1);
+        const double beta = rz1 / rz;
+        rz = rz1;
+        for (int s = lane; s < n; s += 32) p[s] = zz[s] + beta * p[s];
+        __syncwarp();
+    }
+    if (rn > tol2 && lane == 0) solver_status(d, ST_COUPLED_NOCONV);
+    for (int w = 0; w < d.wing_count; ++w) {
+        const int s0 = d.wing_sstart[w], nw = d.wing_npts[w] - 1;
+        double ym = 0.0;
+        for (int s = s0 + lane; s < s0 + nw; s += 32) ym = fmax(ym, fabs(__ldcg(y + s)));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
+        if (lane == 0) d.ymax[2 * w + comp] = ym;
+    }
+}
+
 // Forward and backward substitution with the factor of wing w: warp 0 solves
 // for the x component, warp 1 for the y component, on shared-memory copies
 // of the per-panel inverses and pivots, of the factor (whole when it fits,
@@ -522,6 +727,20 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
     }
     for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
     if (lane == 0) d.ymax[2 * w + comp] = ym;
+    // Supports of different wings share nodes: the last wing block to finish
+    // (a per-episode counter after a fence; no block waits) solves the joint
+    // system from the per-wing solutions, before the spread reads them.
+    if (d.wing_count > 1 && __ldcg(d.ibm_flags) != 0) {
+        __shared__ int last;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) last = atomicAdd(d.solve_count, 1) == d.wing_count - 1;
+        __syncthreads();
+        if (!last) return;
+        __threadfence();
+        if (tid == 0) *d.solve_count = 0;
+        cg_joint_solve(d, z, comp, lane);
+    }
 }
 template <bool SMEM>
 __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) { ibm_solve_kernel_body<SMEM>(d, blockIdx.x); }

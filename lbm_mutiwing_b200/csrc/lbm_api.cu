@@ -402,6 +402,7 @@ int init_state(LbmHandle* h) {
     CK(cudaMemcpy(d.cycle, &one, sizeof(long long), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.gcycle, &one, sizeof(long long), cudaMemcpyHostToDevice));
     CK(cudaMemset(d.fin_count, 0, sizeof(int)));
+    CK(cudaMemset(d.solve_count, 0, sizeof(int)));
     h->d.movenum = 0;
     h->fields_valid = false;
     h->err_valid = false;
@@ -432,10 +433,12 @@ int check_status(LbmHandle* h) {
     int st = 0;
     CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
     h->status_seen |= st;
-    const int fatal = ST_BAND_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION | ST_COPY_TIMEOUT;
+    const int fatal = ST_BAND_OVERFLOW | ST_BOX_OUTSIDE | ST_MOTION | ST_COPY_TIMEOUT | ST_COUPLED_NOCONV;
     if (st & fatal) {
         std::string m = "immersed boundary:";
         if (st & ST_BAND_OVERFLOW) m += " band capacity exceeded;";
+        if (st & ST_COUPLED_NOCONV)
+            m += " the joint solve of wings whose supports share lattice nodes did not reach its tolerance;";
         if (st & ST_BOX_OUTSIDE) m += " a wing's support box left the lattice;";
         if (st & ST_MOTION) m += " no motion rows loaded;";
         if (st & ST_COPY_TIMEOUT) m += " a shared-memory bulk copy timed out;";
@@ -881,7 +884,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         dalloc(h, &d.claim_cnt, nsz + 1) || dalloc(h, &d.kx, 6 * nsz) || dalloc(h, &d.ky, 6 * nsz) ||
         dalloc(h, &d.pb, nsz * BOX_SLOTS) || dalloc(h, &drpos, nsz) || dalloc(h, &d.band_claimer, (size_t)cap) ||
         dalloc(h, &d.rx, nsz) || dalloc(h, &d.ry, nsz) || dalloc(h, &d.qx, nsz) || dalloc(h, &d.qy, nsz) ||
-        dalloc(h, &d.px, nsz) || dalloc(h, &d.py, nsz) || dalloc(h, &d.zx, nsz) || dalloc(h, &d.zy, nsz) ||
+        dalloc(h, &d.cg_work, 8 * nsz) || dalloc(h, &d.solve_count, 1) ||
         dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
         dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &diofs, wz) ||
         dalloc(h, &d.linv, (size_t)std::max<long long>(1, itot)) || dalloc(h, &d.wm, wz) ||
@@ -1784,6 +1787,19 @@ int lbm_get_phase_times(LbmHandle* h, double* out, int32_t n) {
 void* lbm_stream(LbmHandle* h) { return h ? (void*)h->s_main : nullptr; }
 
 int64_t lbm_device_bytes(const LbmHandle* h) { return h ? h->dev_bytes : 0; }
+
+int lbm_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes) {
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return -1;
+    if (cudaSetDevice(device) != cudaSuccess) return -1;
+    size_t fr = 0, to = 0;
+    const cudaError_t e = cudaMemGetInfo(&fr, &to);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return -1;
+    if (free_bytes) *free_bytes = (int64_t)fr;
+    if (total_bytes) *total_bytes = (int64_t)to;
+    return 0;
+}
 
 const char* lbm_last_error(const LbmHandle* h) { return h ? h->err.c_str() : "null handle"; }
 

@@ -47,8 +47,8 @@ enum StatusBits : int {
     ST_BAND_OVERFLOW = 1,      // band list exceeded its capacity
     ST_BOX_OUTSIDE = 4,        // a segment box left the lattice
     ST_PIVOT_CLAMPED = 8,      // Cholesky pivot clamped (numerically singular IBM system)
-    ST_WINGS_COUPLED = 16,     // two wings share band nodes; block solve refined iteratively
-    ST_COUPLED_NOCONV = 32,    // refinement for coupled wings did not converge
+    ST_WINGS_COUPLED = 16,     // two wings' supports share lattice nodes: the joint system was solved
+    ST_COUPLED_NOCONV = 32,    // the joint solve of such wings did not reach its residual tolerance
     ST_MOTION = 64,            // no motion rows available
     ST_COPY_TIMEOUT = 128,     // a bulk shared-memory copy did not complete within its wait limit
 };
@@ -128,7 +128,9 @@ struct DevState {
     int diag;                    // compute the no-slip residual this step
     int write_fields;            // fused path: this step writes rho, u, v fields
     double *rx, *ry;             // nseg right-hand sides, overwritten by solutions
-    double *qx, *qy, *px, *py, *zx, *zy;  // nseg work vectors for coupled refinement
+    double *qx, *qy;             // nseg right-hand sides as built (residual diagnostic, joint solve)
+    double* cg_work;             // 8 nseg: residual, preconditioned residual, direction, product (x then y)
+    int* solve_count;            // wing blocks of the substitution done this step (joint solve)
     // banded Cholesky per wing (RCM order)
     const int* perm;             // nseg: local position -> global segment
     const int* wing_bw;          // W half bandwidths
@@ -137,7 +139,7 @@ struct DevState {
     long long lband_total;       // doubles in lband
     double* piv_floor;           // W pivot floors of the last factorisation
     double* ymax;                // 2 W largest |y| of the last solve, per component (spread scale)
-    int* ibm_flags;              // [0] wings with overlapping supports this step
+    int* ibm_flags;              // [0] two wings' supports share lattice nodes this step
     double* force_part;          // per-block partial force sums: blocks x W x 3
     int bw_max;                  // largest half bandwidth
     int nw_max;                  // largest segment count of a wing

@@ -10,8 +10,13 @@ batching.
   in rounds of at most ``chunk`` steps, and a request that arrives meanwhile
   joins at the next round -- it does not wait for the others' segments to
   end.  FP64 episodes (and ``packed=False``) step on their own CUDA streams.
-* Admission by device memory: a RESET that would exceed the memory budget
-  waits until running episodes end (STOP) and free their memory.
+* Admission by free device memory: a RESET that creates an episode is
+  admitted when the episode's estimated device memory fits in the device's
+  free memory (cudaMemGetInfo) less a reserve and less what episodes admitted
+  but not yet created will take; otherwise it waits until running episodes
+  end (STOP) and free their memory.  Once created, an episode counts with
+  the memory its handle actually holds.  An optional byte budget bounds the
+  resident episodes as well.
 * Replies are the reference's text replies (``protocol``); per-request
   latency is recorded for p50 / p99.
 * ``single=True`` is the reference's one-client driver on a REP socket: one
@@ -52,6 +57,7 @@ class _Client:
     queue: Deque[Tuple[float, str]] = field(default_factory=deque)
     busy: bool = False
     bytes: int = 0
+    reserved: int = 0        # admission reservation until the episode exists
 
 
 def _default_sim_factory(ep, precision, device):
@@ -63,13 +69,19 @@ class Server:
     """Multi-client episode server.
 
     make_episode(name) -> Episode builds the episode a RESET names (the
-    default workload when the RESET names none).  budget_bytes bounds the
-    device memory of the resident episodes (None: no bound)."""
+    default workload when the RESET names none).  Admission: free_memory()
+    (default: the device's free bytes, lbm_mem_info; None disables the
+    check) less reserve_bytes must hold the new episode's estimate
+    (estimate(ep, precision), default api.estimate_device_bytes) plus the
+    estimates of episodes admitted and not yet created; budget_bytes (None:
+    no bound) also bounds the memory the resident episodes hold."""
 
     def __init__(self, endpoint: str, make_episode: Callable, default_workload: str, precision: int = 1,
                  device: int = 0, workers: int = 64, out_dir: Optional[str] = None,
                  budget_bytes: Optional[int] = None, single: bool = False, write_force_files: bool = False,
-                 sim_factory: Optional[Callable] = None, packed: bool = True, chunk: int = 200):
+                 sim_factory: Optional[Callable] = None, packed: bool = True, chunk: int = 200,
+                 free_memory: Optional[Callable[[], int]] = "device", reserve_bytes: int = 1 << 30,
+                 estimate: Optional[Callable] = None):
         import zmq
         self.zmq = zmq
         self.endpoint = endpoint
@@ -79,6 +91,15 @@ class Server:
         self.device = device
         self.out_dir = out_dir
         self.budget = budget_bytes
+        if free_memory == "device":
+            from .api import mem_info
+            free_memory = lambda: mem_info(device)[0]   # noqa: E731
+        self.free_memory = free_memory
+        self.reserve = reserve_bytes
+        if estimate is None:
+            from .api import estimate_device_bytes as estimate
+        self.estimate = estimate
+        self.pending_bytes = 0          # admitted RESETs whose episode is not created yet
         self.single = single
         self.write_force_files = write_force_files
         self.sim_factory = sim_factory or _default_sim_factory
@@ -144,6 +165,10 @@ class Server:
             reply = P.error_reply(str(e))
         except Exception as e:  # library errors become ERROR replies (driver.f90:135-138)
             reply = P.error_reply(str(e))
+        if c.reserved:   # an admitted RESET that created no episode gives its reservation back
+            with self.lock:
+                self.pending_bytes -= c.reserved
+            c.reserved = 0
         st = RequestStat(kind, time.perf_counter() - t_recv, node_updates)
         self.done.append((c.ident, reply, st))
         self._wake()
@@ -153,7 +178,12 @@ class Server:
         if c.session is None or name != c.workload:
             self._release(c)
             ep = self.make_episode(name)
-            sim = self.sim_factory(ep, self.precision, self.device)
+            try:
+                sim = self.sim_factory(ep, self.precision, self.device)
+            finally:
+                with self.lock:   # the admission reservation ends with the creation
+                    self.pending_bytes -= c.reserved
+                c.reserved = 0
             with self.lock:
                 self.episode_counter += 1
                 idx = self.episode_counter - 1
@@ -191,20 +221,34 @@ class Server:
         c.workload = None
 
     # -- admission
-    def _estimate(self, text: str) -> int:
+    def _need(self, c: _Client, text: str) -> int:
+        """Estimated bytes of the episode a RESET would create (0 when it
+        keeps the client's episode)."""
         toks = text.split()
-        name = toks[2] if len(toks) > 2 else self.default_workload
+        name = toks[2] if len(toks) > 2 else (c.workload or self.default_workload)
+        if c.session is not None and name == c.workload:
+            return 0
         try:
             ep = self.make_episode(name)
         except Exception:
-            return 0
-        return 120 * ep.nx * ep.ny + (64 << 20)
+            return 0          # the RESET fails on its own and takes no memory
+        return int(self.estimate(ep, self.precision))
 
-    def _admissible(self, c: _Client, text: str) -> bool:
-        if self.budget is None or c.session is not None:
+    def _admit(self, c: _Client, text: str) -> bool:
+        """Reserve the RESET's memory if it fits; False if it must wait."""
+        need = self._need(c, text)
+        if need == 0:
             return True
         with self.lock:
-            return self.resident_bytes + self._estimate(text) <= self.budget
+            if self.budget is not None and self.resident_bytes - c.bytes + need > self.budget:
+                return False
+            if self.free_memory is not None:
+                # a client's own episode is freed before its new one is made
+                if self.pending_bytes + need > self.free_memory() + c.bytes - self.reserve:
+                    return False
+            self.pending_bytes += need
+            c.reserved = need
+        return True
 
     # -- main loop
     def _dispatch(self, c: _Client):
@@ -212,7 +256,7 @@ class Server:
             return
         t_recv, text = c.queue[0]
         first = text.strip().split()[:1]
-        if first and first[0].upper() in ("RESET", "START") and not self._admissible(c, text):
+        if first and first[0].upper() in ("RESET", "START") and not self._admit(c, text):
             if c.ident not in self.waiting_admission:
                 self.waiting_admission.append(c.ident)
             return

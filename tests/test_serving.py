@@ -157,7 +157,9 @@ def test_session_sequencing_and_averages(tmp_path):
 # -- server
 def _server(**kw):
     from lbm_mutiwing_b200.serve import Server
-    srv = Server("tcp://127.0.0.1:0", make_episode, "small2", sim_factory=lambda ep, p, d: FakeSim(ep), **kw)
+    kw.setdefault("free_memory", None)
+    factory = kw.pop("sim_factory", lambda ep, p, d: FakeSim(ep))
+    srv = Server("tcp://127.0.0.1:0", make_episode, "small2", sim_factory=factory, **kw)
     th = threading.Thread(target=srv.serve, kwargs={"idle_timeout_s": 30}, daemon=True)
     th.start()
     return srv, th, f"tcp://127.0.0.1:{srv.port}"
@@ -194,10 +196,24 @@ def test_server_clients_alone_and_together():
         srv.close()
 
 
-def test_server_admission_waits_for_memory():
-    ep = make_episode("small2")
-    per = 120 * ep.nx * ep.ny + (64 << 20)
-    srv, th, addr = _server(budget_bytes=per + 1)   # room for one episode
+class FakeDevice:
+    """Device memory of FakeSim episodes: free = total - live episodes."""
+
+    def __init__(self, total):
+        self.total, self.live = total, []
+
+    def factory(self, ep, precision, device):
+        sim = FakeSim(ep)
+        self.live.append(sim)
+        return sim
+
+    def free(self):
+        return self.total - sum(s.device_bytes() for s in self.live if not s.closed)
+
+
+def _two_clients_one_fits(**kw):
+    """Client a's RESET is admitted, b's waits until a's STOP frees memory."""
+    srv, th, addr = _server(**kw)
     try:
         import zmq
         ctx = zmq.Context.instance()
@@ -224,10 +240,24 @@ def test_server_admission_waits_for_memory():
         srv.close()
 
 
+def test_server_admission_waits_for_free_device_memory():
+    ep = make_episode("small2")
+    per = 1000 * ep.nx * ep.ny                      # a FakeSim episode's device bytes
+    dev = FakeDevice(total=(3 * per) // 2 + (1 << 20))   # room for one episode and the reserve
+    _two_clients_one_fits(sim_factory=dev.factory, free_memory=dev.free, reserve_bytes=1 << 20,
+                          estimate=lambda e, p: 1000 * e.nx * e.ny)
+
+
+def test_server_admission_within_a_byte_budget():
+    ep = make_episode("small2")
+    per = 1000 * ep.nx * ep.ny
+    _two_clients_one_fits(budget_bytes=per + 1, estimate=lambda e, p: 1000 * e.nx * e.ny)
+
+
 def test_single_client_mode_stops_on_stop():
     from lbm_mutiwing_b200.serve import Server
     srv = Server("tcp://127.0.0.1:0", make_episode, "small2", single=True,
-                 sim_factory=lambda ep, p, d: FakeSim(ep))
+                 sim_factory=lambda ep, p, d: FakeSim(ep), free_memory=None)
     th = threading.Thread(target=srv.serve, daemon=True)
     th.start()
     addr = f"tcp://127.0.0.1:{srv.port}"

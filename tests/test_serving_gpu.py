@@ -27,7 +27,8 @@ def small(name, wings=2, size=(4.0, 2.0)):
                                  x_spacing=1.5, spacing="uniform")
 
 
-WORKLOADS = {"a": lambda: small("a", 2), "b": lambda: small("b", 1, (6.0, 3.0)), "c": lambda: small("c", 2, (5.0, 2.0))}
+WORKLOADS = {"a": lambda: small("a", 2), "b": lambda: small("b", 1, (6.0, 3.0)), "c": lambda: small("c", 2, (5.0, 2.0)),
+             "big": lambda: small("big", 2, (20.0, 10.0))}
 
 
 def make_episode(name):
@@ -191,3 +192,51 @@ def test_packed_rounds_equal_own_streams(gpu_lib):
     assert all(r.startswith("FORCE") for r in ref[0][:-1])
     for k in range(5):
         assert got[k] == ref[k], k
+
+
+def test_admission_waits_for_free_device_memory(gpu_lib):
+    """Device memory held by another user of the GPU leaves room for one
+    1001 x 501 episode: a second client's RESET waits (no reply) until the
+    first client's STOP frees its episode, then proceeds."""
+    import torch
+    import zmq
+    ep = make_episode("big")
+    with api.Simulation(ep, api.PRECISION_FP32, motion_source=api.MOTION_STREAM) as probe:
+        actual = probe.device_bytes()
+    need = api.estimate_device_bytes(ep, api.PRECISION_FP32)
+    assert actual <= need
+    reserve = 256 << 20
+    torch.cuda.synchronize()
+    free, _ = api.mem_info(0)
+    slack = actual // 2      # after one episode the free memory is short of a second estimate
+    hog = torch.empty(free - reserve - need - slack, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    srv, th, addr = _server(reserve_bytes=reserve)
+    ctx = zmq.Context.instance()
+    a, b = ctx.socket(zmq.REQ), ctx.socket(zmq.REQ)
+    try:
+        for sck in (a, b):
+            sck.setsockopt(zmq.LINGER, 0)
+            sck.connect(addr)
+        a.setsockopt(zmq.RCVTIMEO, 60000)
+        a.send_string("RESET 0.0 big")
+        assert a.recv().decode().startswith("FORCE")
+        b.setsockopt(zmq.RCVTIMEO, 1500)
+        b.send_string("RESET 0.0 big")
+        with pytest.raises(zmq.Again):
+            b.recv()
+        a.send_string("STOP")
+        assert a.recv().decode() == "STATUS STOPPING"
+        b.setsockopt(zmq.RCVTIMEO, 60000)
+        assert b.recv().decode().startswith("FORCE")
+        b.send_string("STOP")
+        assert b.recv().decode() == "STATUS STOPPING"
+    finally:
+        a.close(0)
+        b.close(0)
+        srv.stop()
+        th.join(30)
+        srv.close()
+        del hog
+        torch.cuda.empty_cache()
+
