@@ -15,32 +15,31 @@
 // over the common node columns i and rows j of the two boxes.  G is
 // assembled per wing in a banded layout after a reverse Cuthill-McKee
 // ordering fixed at set-up (rigid wings keep their pairwise distances) and
-// factored as L' D L'^T, panel by panel, one thread block per wing, and
-// the factor gives G^-1 explicitly (one warp per column).  G depends on the
-// geometry only, so assembly, factorisation and inverse run on a side
-// stream while the band list is built (on the FP32 path a step ahead), and
-// the step itself only multiplies by G^-1.
+// factored as L' D L'^T, panel by panel, one thread block per wing, and the
+// unit lower diagonal blocks of L' are inverted in panels of 32 rows.  G
+// depends on the geometry only, so assembly, factorisation and panel
+// inverses run on a side stream while the band list is built (on the FP32
+// path a step ahead), and the step itself substitutes 32 rows at a time.
 //
 // Kernels of one step's geometry (main chain | side chain):
 //   geometry   motion, markers, midpoints, support boxes, kernel values,
 //              clearing of the previous band             (move_boundary)
 //   claim      lowest segment index claims each box node   | assemble  G
 //   count      claims per segment, coupled-wing check      | factor    L' D L'^T
-//   scan       band-list offsets                           | inverse   G^-1
+//   scan       band-list offsets                           | panels    32-row block inverses
 //   list       band list in the reference's order (segment, i, j), band
 //              bit plane; advances the geometry's cycle counter
 // then, plain FP64 path:
 //   ustar      u*, rho at band nodes; zeroed spread accumulators
 //   rhs        r = ub - X u* (one warp per segment)
-//   apply      y = G^-1 r per wing from the explicit inverse built with the
-//              geometry (and the joint solve of wings whose supports share
-//              nodes)
+//   solve      G y = r per wing in 32-row panels (and the joint solve of
+//              wings whose supports share nodes)
 //   spread     du = X^T y with fixed-point integer atomics
 //   finish     du, body force, per-block force partials
 //   forces     per-wing force and moment, force row
 // or, FP32 path (beside the bulk kernel):
 //   rhs        u* from the pulled distributions at each box node, r = ub - X u*
-//   apply, spread as above
+//   solve, spread as above
 //   close      du, band-node re-collision, force partials; the last block
 //              writes the force row and advances the cycle counter
 //
@@ -396,7 +395,6 @@ __global__ void ibm_ustar_kernel(DevState d) {
 __device__ __forceinline__ void ibm_rhs_kernel_body(const DevState& d, const int bid_) {
     const int s = (bid_ * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (bid_ == 0 && threadIdx.x < 2 * d.wing_count) d.ymax[threadIdx.x] = 0.0;   // the apply kernel's maxima
     if (s >= d.nseg) return;
     const int nb = d.band_n[0];
     const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
@@ -509,7 +507,6 @@ __device__ __forceinline__ void ibm_rhs_fused_seg(const DevState& d, const int s
     }
 }
 __device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int bid_) {
-    if (bid_ == 0 && threadIdx.x < 2 * d.wing_count) d.ymax[threadIdx.x] = 0.0;   // the apply kernel's maxima
     const int stride = rhs_grid(d) * 4;   // warps of the grid
     for (int s = (bid_ * 128 + threadIdx.x) >> 5; s < d.nseg; s += stride) ibm_rhs_fused_seg(d, s, threadIdx.x & 31);
 }
@@ -958,7 +955,7 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
 }
 
 void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st) {
-    launch_ibm_apply(d, st);
+    launch_ibm_substitution(d, st);
     ibm_spread_kernel<<<slot_grid(d), 256, 0, st>>>(d);
     const int nbk = ibm_finish_blocks(d);
     if (fused) {

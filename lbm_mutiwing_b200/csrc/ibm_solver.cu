@@ -1,10 +1,9 @@
-// Banded L' D L'^T factorisation, explicit inverse and its application for
-// the immersed-boundary system G y = r of each wing (G = X X^T in reverse
-// Cuthill-McKee order; see ibm.cu for how G arises from
-// immersed_boundary_Wu, boundary_condition.f90:1558-1640).  The geometry
-// pipeline factors G and builds G^-1 column by column; the step's chain
-// then forms y = G^-1 r with one warp per segment instead of a sequential
-// substitution.
+// Banded L' D L'^T factorisation and substitution for the immersed-boundary
+// system G y = r of each wing (G = X X^T in reverse Cuthill-McKee order; see
+// ibm.cu for how G arises from immersed_boundary_Wu,
+// boundary_condition.f90:1558-1640).  The geometry pipeline factors G and
+// inverts the unit lower diagonal blocks of L' in panels of 32 rows; the
+// step's chain then substitutes 32 rows per step.
 //
 // Blocked right-looking algorithm, PANEL = 8 columns at a time, one thread
 // block per wing, the wing's banded matrix held in shared memory (brought in
@@ -17,9 +16,10 @@
 //      warps 1.., while warp 0 updates the next panel's 8 x 8 diagonal block
 //      first and one thread factors it in registers (look-ahead: the
 //      sequential pivot chain of panel p + 1 overlaps panel p's update).
-// The substitution (one warp per right-hand side) applies each panel
-// through its stored 8 x 8 inverse and reciprocal pivots and updates the
-// rows below (forward) or above (backward) it.
+// The substitutions apply each panel through the inverse of its unit lower
+// block and the reciprocal pivots and update the rows below (forward) or
+// above (backward) it: on the chain in panels of 32 rows, in the joint solve
+// of coupled wings in the factor's panels of 8.
 //
 // The zero zones of the banded storage (entries past the bandwidth, rows past
 // the last segment) make every panel-shaped read in bounds and zero where it
@@ -364,8 +364,12 @@ __device__ void warp_substitute(const double* A, int ld, const double* L, int nw
     }
 }
 
-// Per-warp vector length of the substitution (even: 16-byte multiples).
-__host__ __device__ inline int inv_zlen(int nw_max, int bw_max) { return (nw_max + PANEL + bw_max + 1) & ~1; }
+// Rows of a substitution panel on the step's chain (four factor panels).
+constexpr int QP = 32;
+constexpr int QP_AUX = 2 * QP * QP;   // a panel's inverse block M, row-major, then M^T
+__host__ __device__ inline int qpanels(int nw) { return (nw + QP - 1) / QP; }
+// Per-warp vector length of the substitutions (even: 16-byte multiples).
+__host__ __device__ inline int solve_zlen(int nw_max, int bw_max) { return (nw_max + QP + bw_max + 1) & ~1; }
 
 // ------------------------------------------------- joint solve of coupled wings
 // When two wings' supports share lattice nodes, G has entries between their
@@ -428,7 +432,7 @@ __device__ void cg_product(const DevState& d, const double* in, double* out, uns
 
 // out = D^-1 in for one component, D the block-diagonal part of G: each
 // wing's substitution with its banded factor and per-panel inverses read
-// from global memory, one warp, z a shared-memory vector of inv_zlen
+// from global memory, one warp, z a shared-memory vector of solve_zlen
 // doubles.
 __device__ void cg_precondition(const DevState& d, const double* in, double* out, double* z, int lane) {
     for (int w = 0; w < d.wing_count; ++w) {
@@ -515,129 +519,189 @@ __device__ void cg_joint_solve(const DevState& d, double* z, int comp, int lane)
 }
 
 
-// ------------------------------------------------------------ explicit inverse
-// G^-1 of each wing in the wing's own segment order, row-major nw x nw at
-// d.ginv + d.wing_gofs[w], built from the banded factor in the geometry
-// pipeline (a step ahead of its use, beside the running step): block b
-// takes INV_WARPS consecutive columns of one wing, warp q solves G z = e_c
-// for column c (the unit vector at the segment's RCM position, so the
-// forward pass starts at its panel) and writes z in segment order as row c
-// (G is symmetric).  SMEM: the wing's per-panel inverses and banded factor
-// are staged in shared memory by bulk copies on an mbarrier (bounded wait).
-constexpr int INV_WARPS = 4;
-constexpr int INV_THREADS = 32 * INV_WARPS;
+// ------------------------------------------------------------ panel inverses
+// For the step's substitution in panels of QP = 32 rows, the inverse M of
+// each panel's unit lower diagonal block B of L' (rows and columns k0 ..
+// k0 + 31 of a wing; identity past the wing's last segment), built in the
+// geometry pipeline beside the running step: one warp per panel, lane c
+// forms column c by block forward substitution over the panel's four factor
+// panels -- the entries of B outside the 8 x 8 diagonal blocks come from the
+// banded storage, the 8 x 8 diagonal blocks through their stored inverses
+// (the factorisation keeps only those).  Stored per panel as M row-major
+// then M^T, so that both substitution passes read 32 consecutive values per
+// warp load.
+constexpr int PANELS_WARPS = 4;
 
-template <bool SMEM>
-__device__ __forceinline__ void ibm_inverse_body(const DevState& d, int bid_) {
-    extern __shared__ __align__(16) double sm[];
-    __shared__ uint64_t bar;
+__device__ __forceinline__ void ibm_panels_body(const DevState& d, int bid_) {
+    __shared__ double X[PANELS_WARPS][QP][QP];
+    __shared__ double S8[PANELS_WARPS][PANEL][QP];
     const int tid = threadIdx.x, lane = tid & 31, q = tid >> 5;
-    int w = 0, b = bid_;
+    int w = 0, b = bid_ * PANELS_WARPS + q;
     for (; w < d.wing_count; ++w) {
-        const int nb = (d.wing_npts[w] - 1 + INV_WARPS - 1) / INV_WARPS;
-        if (b < nb) break;
-        b -= nb;
+        const int nq = qpanels(d.wing_npts[w] - 1);
+        if (b < nq) break;
+        b -= nq;
     }
     if (w >= d.wing_count) return;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
-    const int npan = (nw + PANEL - 1) / PANEL;
-    const int zlen = inv_zlen(d.nw_max, d.bw_max);
-    double* z = sm + q * zlen;
-    const double* L = d.linv + d.wing_linv_ofs[w];
-    const double* S = d.lband + d.wing_lofs[w];
-    if (SMEM) {
-        double* Ls = sm + INV_WARPS * zlen;
-        double* Ss = Ls + (long long)npan * IBM_PANEL_AUX;
-        const long long lbytes = (long long)npan * IBM_PANEL_AUX * 8, sbytes = ibm_wing_storage(nw, bw) * 8;
-        if (tid == 0) {
-            mbar_init(&bar, 1);
-            mbar_arrive_expect_tx(&bar, (uint32_t)(lbytes + sbytes));
-            bulk_load_all(Ls, L, lbytes, &bar);
-            bulk_load_all(Ss, S, sbytes, &bar);
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
+    const int k0 = b * QP, np = min(QP, nw - k0), c = lane;
+    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
+    const double* L8 = d.linv + d.wing_linv_ofs[w] + (long long)(k0 / PANEL) * IBM_PANEL_AUX;
+    double(*x)[QP] = X[q];
+    double(*s8)[QP] = S8[q];
+    for (int r = 0; r < QP; ++r) x[r][c] = (r == c) ? 1.0 : 0.0;
+    const int nb8 = (np + PANEL - 1) / PANEL;
+    for (int a8 = 0; a8 < nb8; ++a8) {
+        const int r0 = a8 * PANEL;
+        // s = e_c - (off-diagonal-block part of B) x over the earlier factor panels
+        for (int i = 0; i < PANEL; ++i) {
+            const int r = r0 + i;
+            double acc = 0.0;
+            if (r < np) {
+                const double* row = A + (long long)(k0 + r) * ld;   // entry r - m: column m of the panel
+                for (int m = max(c, r - bw); m < r0; ++m) acc = acc + row[r - m] * x[m][c];
+            }
+            s8[i][c] = x[r][c] - acc;
         }
-        __syncthreads();
-        const bool ok = mbar_wait(&bar, 0);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
-            mbar_wait(&bar, 0);   // let a late copy land before the block exits
-            return;
+        // x over this factor panel = (its inverse 8 x 8 block) s
+        const double* Li = L8 + a8 * IBM_PANEL_AUX;
+        for (int i = 0; i < PANEL; ++i) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < PANEL; ++k) v = v + Li[i * PANEL + k] * s8[k][c];
+            if (r0 + i < np) x[r0 + i][c] = v;
         }
-        L = Ls;
-        S = Ss;
     }
-    const int c = b * INV_WARPS + q;
-    if (c >= nw) return;
-    const int pos = d.rpos[s0 + c];
-    for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p == pos ? 1.0 : 0.0;
-    __syncwarp();
-    warp_substitute(S + ld, ld, L, nw, bw, z, lane, pos / PANEL);
-    double* row = d.ginv + d.wing_gofs[w] + (long long)c * nw;
-    for (int p = lane; p < nw; p += 32) row[d.perm[s0 + p] - s0] = z[p];
+    double* M = d.lq + d.wing_qofs[w] + (long long)b * QP_AUX;
+    for (int r = 0; r < QP; ++r) {
+        M[r * QP + c] = x[r][c];             // row r of M, lanes along the row
+        M[QP * QP + c * QP + r] = x[r][c];   // M^T: row c of M^T is column c of M
+    }
 }
-template <bool SMEM>
-__global__ void __launch_bounds__(INV_THREADS) ibm_inverse_kernel(DevState d) { ibm_inverse_body<SMEM>(d, blockIdx.x); }
-template <bool SMEM>
-__global__ void __launch_bounds__(INV_THREADS) ibm_inverse_kernel_multi(MultiArgs m) {
+__global__ void __launch_bounds__(32 * PANELS_WARPS) ibm_panels_kernel(DevState d) { ibm_panels_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(32 * PANELS_WARPS) ibm_panels_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
-    ibm_inverse_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+    ibm_panels_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// ------------------------------------------------------------ apply
-// y = G^-1 r for every wing, on the step's critical path: one warp per
-// segment (both velocity components), lane-strided dot products of the
-// segment's row of G^-1 with the wing's right-hand sides (qx, qy as the rhs
-// kernel built them) added by a fixed butterfly; y goes to rx, ry, and each
-// wing's largest |y| (the spread's fixed-point scale; the rhs kernel clears
-// ymax) by an integer atomicMax on the bits of a non-negative double.  When
-// supports of different wings share nodes, the last block to finish (a
-// per-episode counter after a fence; no block waits) solves the joint
-// system from these per-wing solutions before the spread reads them.
-constexpr int APPLY_THREADS = 256;
-__host__ __device__ inline int apply_blocks(const DevState& d) {
-    return (int)((32LL * d.nseg + APPLY_THREADS - 1) / APPLY_THREADS);
-}
+// ------------------------------------------------------------ substitution on the chain
+// G y = r for every wing: one block per wing, warp 0 for the x component,
+// warp 1 for y, in panels of 32 rows: per panel (forward) t = M z_p, rows
+// below -= L' t, z_p = D^-1 t; per panel, last first (backward) y_p = M^T
+// z_p, rows above -= L'^T y_p.  Every lane owns one row of a panel, so a
+// panel step is one 32-term dot product per lane instead of four dependent
+// 8-row steps.  The right-hand sides are read from qx, qy (as the rhs kernel
+// built them), the solutions written to rx, ry, and each wing's largest |y|
+// (the spread's fixed-point scale) to ymax.  When supports of different
+// wings share nodes, the last wing block to finish (a per-episode counter
+// after a fence; no block waits) solves the joint system from these
+// per-wing solutions before the spread reads them.
+constexpr int SOLVE_THREADS = 64;
 
-__device__ __forceinline__ void ibm_apply_body(const DevState& d, int bid_) {
+__device__ __forceinline__ void ibm_solve_body(const DevState& d, int bid_) {
     extern __shared__ __align__(16) double sm[];
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int s = (bid_ * APPLY_THREADS + tid) >> 5;
-    if (s < d.nseg) {
-        const int w = d.seg_wing[s], s0 = d.wing_sstart[w], nw = d.wing_npts[w] - 1;
-        const double* row = d.ginv + d.wing_gofs[w] + (long long)(s - s0) * nw;
-        const double* rx = d.qx + s0;
-        const double* ry = d.qy + s0;
-        double ax = 0.0, ay = 0.0;
-        for (int c = lane; c < nw; c += 32) {
-            const double g = row[c];
-            ax = ax + g * rx[c];
-            ay = ay + g * ry[c];
+    const int w = bid_;
+    const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+    const int nq = qpanels(nw);
+    const int zlen = solve_zlen(d.nw_max, d.bw_max);
+    double* z = sm + comp * zlen;
+    double* t = sm + 2 * zlen + comp * QP;
+    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
+    const double* Q = d.lq + d.wing_qofs[w];
+    const double* L8 = d.linv + d.wing_linv_ofs[w];
+    const int* perm = d.perm + s0;
+    const double* rin = comp ? d.qy : d.qx;
+    for (int p = lane; p < nw + QP + bw; p += 32) z[p] = p < nw ? rin[perm[p]] : 0.0;
+    __syncwarp();
+    for (int qi = 0; qi < nq; ++qi) {   // L' D v = r
+        const int k0 = qi * QP, np = min(QP, nw - k0);
+        const double* MT = Q + (long long)qi * QP_AUX + QP * QP;
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < QP; c += 4) {
+            w0 = w0 + MT[c * QP + lane] * z[k0 + c];
+            w1 = w1 + MT[(c + 1) * QP + lane] * z[k0 + c + 1];
+            w2 = w2 + MT[(c + 2) * QP + lane] * z[k0 + c + 2];
+            w3 = w3 + MT[(c + 3) * QP + lane] * z[k0 + c + 3];
         }
-        ax = warp_sum(ax);
-        ay = warp_sum(ay);
-        if (lane == 0) {
-            d.rx[s] = ax;
-            d.ry[s] = ay;
-            unsigned long long* ym = reinterpret_cast<unsigned long long*>(d.ymax) + 2 * w;
-            atomicMax(ym, (unsigned long long)__double_as_longlong(fabs(ax)));
-            atomicMax(ym + 1, (unsigned long long)__double_as_longlong(fabs(ay)));
+        const double tl = (w0 + w1) + (w2 + w3);
+        t[lane] = tl;
+        __syncwarp();
+        for (int rb = lane; rb < bw; rb += 32) {
+            const int i = k0 + np + rb;
+            const double* row = A + (long long)i * ld + (i - k0);   // L'(i, k0 + c) at row[-c]
+            double a0 = 0.0, a1 = 0.0;
+            int c = max(0, i - k0 - bw);
+            for (; c + 1 < np; c += 2) {
+                a0 = a0 + row[-c] * t[c];
+                a1 = a1 + row[-(c + 1)] * t[c + 1];
+            }
+            if (c < np) a0 = a0 + row[-c] * t[c];
+            z[i] -= a0 + a1;
         }
+        if (lane < np) {
+            const int k = k0 + lane;
+            z[k] = tl * L8[(long long)(k / PANEL) * IBM_PANEL_AUX + PANEL * PANEL + (k % PANEL)];
+        }
+        __syncwarp();
     }
+    for (int qi = nq - 1; qi >= 0; --qi) {   // L'^T y = v
+        const int k0 = qi * QP, np = min(QP, nw - k0);
+        const double* M = Q + (long long)qi * QP_AUX;
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < QP; c += 4) {
+            y0 = y0 + M[c * QP + lane] * z[k0 + c];
+            y1 = y1 + M[(c + 1) * QP + lane] * z[k0 + c + 1];
+            y2 = y2 + M[(c + 2) * QP + lane] * z[k0 + c + 2];
+            y3 = y3 + M[(c + 3) * QP + lane] * z[k0 + c + 3];
+        }
+        const double yl = (y0 + y1) + (y2 + y3);
+        t[lane] = yl;
+        __syncwarp();
+        const int above = min(bw, k0);   // rows k0 - above .. k0 - 1
+        for (int r = lane; r < above; r += 32) {
+            const int j = k0 - 1 - r;
+            const double* col = A + (long long)k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+            const int cmax = min(np, bw - (k0 - j) + 1);
+            double a0 = 0.0, a1 = 0.0;
+            int c = 0;
+            for (; c + 1 < cmax; c += 2) {
+                a0 = a0 + col[c * (ld + 1)] * t[c];
+                a1 = a1 + col[(c + 1) * (ld + 1)] * t[c + 1];
+            }
+            if (c < cmax) a0 = a0 + col[c * (ld + 1)] * t[c];
+            z[j] -= a0 + a1;
+        }
+        if (lane < np) z[k0 + lane] = yl;
+        __syncwarp();
+    }
+    double* rout = comp ? d.ry : d.rx;
+    double ym = 0.0;
+    for (int p = lane; p < nw; p += 32) {
+        rout[perm[p]] = z[p];
+        ym = fmax(ym, fabs(z[p]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
+    if (lane == 0) d.ymax[2 * w + comp] = ym;
     if (d.wing_count > 1 && __ldcg(d.ibm_flags) != 0) {
         __shared__ int last;
         __threadfence();
         __syncthreads();
-        if (tid == 0) last = atomicAdd(d.solve_count, 1) == apply_blocks(d) - 1;
+        if (tid == 0) last = atomicAdd(d.solve_count, 1) == d.wing_count - 1;
         __syncthreads();
         if (!last) return;
         __threadfence();
         if (tid == 0) *d.solve_count = 0;
-        if (tid < 64) cg_joint_solve(d, sm + (tid >> 5) * inv_zlen(d.nw_max, d.bw_max), tid >> 5, lane);
+        cg_joint_solve(d, z, comp, lane);
     }
 }
-__global__ void __launch_bounds__(APPLY_THREADS) ibm_apply_kernel(DevState d) { ibm_apply_body(d, blockIdx.x); }
-__global__ void __launch_bounds__(APPLY_THREADS) ibm_apply_kernel_multi(MultiArgs m) {
+__global__ void __launch_bounds__(SOLVE_THREADS, 1) ibm_solve_kernel(DevState d) { ibm_solve_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
-    ibm_apply_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+    ibm_solve_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
 // ------------------------------------------------------------ host side
@@ -648,17 +712,16 @@ size_t ibm_factor_staging_bytes(int bw_max) {
     return rows + (tl + 15) / 16 * 16;
 }
 
-size_t ibm_inverse_smem(int nw_max, int bw_max, long long wing_storage_max, bool in_smem) {
-    const size_t z = (size_t)INV_WARPS * inv_zlen(nw_max, bw_max) * sizeof(double);
-    return z + (in_smem ? (size_t)(ibm_linv_storage(nw_max) + wing_storage_max) * sizeof(double) : 0);
+size_t ibm_solve_smem(int nw_max, int bw_max) {
+    return (size_t)(2 * solve_zlen(nw_max, bw_max) + 2 * QP) * sizeof(double);
 }
 
-size_t ibm_apply_smem(int nw_max, int bw_max) { return (size_t)2 * inv_zlen(nw_max, bw_max) * sizeof(double); }
+long long ibm_panel_storage(int nw) { return (long long)qpanels(nw) * QP_AUX; }
 
-int ibm_inverse_blocks(const int* points_per_wing, int wing_count) {
+int ibm_panel_blocks(const int* points_per_wing, int wing_count) {
     int n = 0;
-    for (int w = 0; w < wing_count; ++w) n += (points_per_wing[w] - 1 + INV_WARPS - 1) / INV_WARPS;
-    return n;
+    for (int w = 0; w < wing_count; ++w) n += qpanels(points_per_wing[w] - 1);
+    return (n + PANELS_WARPS - 1) / PANELS_WARPS;
 }
 
 // The dynamic shared-memory limit is a per-device property of each kernel,
@@ -676,43 +739,35 @@ static cudaError_t raise_smem_limit(K kernel, int optin) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
-cudaError_t ibm_prepare(size_t factor_smem, size_t inverse_smem, size_t apply_smem) {
+cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     int dev = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    if (factor_smem + 16 * 1024 > (size_t)optin || inverse_smem + 1024 > (size_t)optin ||
-        apply_smem + 1024 > (size_t)optin)
-        return cudaErrorInvalidValue;
+    if (factor_smem + 16 * 1024 > (size_t)optin || solve_smem + 1024 > (size_t)optin) return cudaErrorInvalidValue;
     std::lock_guard<std::mutex> lock(g_prepare_mutex);
     if (dev < 64 && (g_prepared_devices >> dev) & 1ULL) return cudaSuccess;
     e = raise_smem_limit(ibm_factor_kernel<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel<false>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<false>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_inverse_kernel<true>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_inverse_kernel<false>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_inverse_kernel_multi<true>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_inverse_kernel_multi<false>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_apply_kernel, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_apply_kernel_multi, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi, optin);
     if (e == cudaSuccess && dev < 64) g_prepared_devices |= 1ULL << dev;
     return e;
 }
 
-// Factorisation and inverse: kernels of the geometry pipeline.
+// Factorisation and panel inverses: kernels of the geometry pipeline.
 bool is_factor_multi_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<true>) ||
            func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<false>) ||
-           func == reinterpret_cast<const void*>(ibm_inverse_kernel_multi<true>) ||
-           func == reinterpret_cast<const void*>(ibm_inverse_kernel_multi<false>);
+           func == reinterpret_cast<const void*>(ibm_panels_kernel_multi);
 }
 
 bool is_factor_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(ibm_factor_kernel<true>) ||
            func == reinterpret_cast<const void*>(ibm_factor_kernel<false>) ||
-           func == reinterpret_cast<const void*>(ibm_inverse_kernel<true>) ||
-           func == reinterpret_cast<const void*>(ibm_inverse_kernel<false>);
+           func == reinterpret_cast<const void*>(ibm_panels_kernel);
 }
 
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st) {
@@ -721,28 +776,24 @@ void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_
         ibm_factor_kernel<true><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
     else
         ibm_factor_kernel<false><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
-    if (d.inv_in_smem)
-        ibm_inverse_kernel<true><<<d.inv_blocks, INV_THREADS, (size_t)d.inv_smem, st>>>(d);
-    else
-        ibm_inverse_kernel<false><<<d.inv_blocks, INV_THREADS, (size_t)d.inv_smem, st>>>(d);
+    ibm_panels_kernel<<<d.panel_blocks, 32 * PANELS_WARPS, 0, st>>>(d);
 }
 
-void launch_ibm_apply(const DevState& d, cudaStream_t st) {
+void launch_ibm_substitution(const DevState& d, cudaStream_t st) {
     if (d.wing_count <= 0) return;
-    ibm_apply_kernel<<<apply_blocks(d), APPLY_THREADS, (size_t)d.apply_smem, st>>>(d);
+    ibm_solve_kernel<<<d.wing_count, SOLVE_THREADS, (size_t)d.solve_smem, st>>>(d);
 }
 
-// Packed launches: one block per wing of every episode (factorisation),
-// the inverse's column blocks, the apply's segment warps; episodes whose
-// factor (or inverse) does not take the kind's shared-memory form get no
-// blocks in it.  The dynamic shared memory is the largest of the batch.
+// Packed launches: one block per wing of every episode (factorisation,
+// substitution), the panel inverses' warps; episodes whose factor does not
+// take the kind's shared-memory form get no blocks in it.  The dynamic
+// shared memory is the largest of the batch.
 int multi_blocks_solver(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_FACTOR_SMEM: return d.factor_in_smem ? d.wing_count : 0;
     case MK_FACTOR_GLOBAL: return d.factor_in_smem ? 0 : d.wing_count;
-    case MK_INVERSE_SMEM: return d.inv_in_smem ? d.inv_blocks : 0;
-    case MK_INVERSE_GLOBAL: return d.inv_in_smem ? 0 : d.inv_blocks;
-    case MK_APPLY: return d.wing_count > 0 ? apply_blocks(d) : 0;
+    case MK_PANELS: return d.wing_count > 0 ? d.panel_blocks : 0;
+    case MK_SOLVE: return d.wing_count;
     default: return -1;
     }
 }
@@ -751,9 +802,8 @@ bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int nb, size_t smem,
     switch (k) {
     case MK_FACTOR_SMEM: ibm_factor_kernel_multi<true><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
     case MK_FACTOR_GLOBAL: ibm_factor_kernel_multi<false><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
-    case MK_INVERSE_SMEM: ibm_inverse_kernel_multi<true><<<nb, INV_THREADS, smem, st>>>(m); return true;
-    case MK_INVERSE_GLOBAL: ibm_inverse_kernel_multi<false><<<nb, INV_THREADS, smem, st>>>(m); return true;
-    case MK_APPLY: ibm_apply_kernel_multi<<<nb, APPLY_THREADS, smem, st>>>(m); return true;
+    case MK_PANELS: ibm_panels_kernel_multi<<<nb, 32 * PANELS_WARPS, 0, st>>>(m); return true;
+    case MK_SOLVE: ibm_solve_kernel_multi<<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
     default: return false;
     }
 }

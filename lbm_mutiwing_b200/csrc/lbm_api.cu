@@ -123,7 +123,7 @@ struct GeoSet {
     int *box = nullptr, *claim_cnt = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
     int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
     unsigned* band_bits = nullptr;
-    double *lband = nullptr, *linv = nullptr, *ginv = nullptr;
+    double *lband = nullptr, *linv = nullptr, *lq = nullptr;
 };
 
 static GeoSet geo_of(const DevState& d) {
@@ -132,7 +132,7 @@ static GeoSet geo_of(const DevState& d) {
     g.box = d.box; g.claim_cnt = d.claim_cnt; g.pb = d.pb; g.band_claimer = d.band_claimer;
     g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
     g.band_bits = d.band_bits;
-    g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv; g.ginv = d.ginv;
+    g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv; g.lq = d.lq;
     return g;
 }
 
@@ -141,7 +141,7 @@ static void use_geo(DevState& d, const GeoSet& g) {
     d.box = g.box; d.claim_cnt = g.claim_cnt; d.pb = g.pb; d.band_claimer = g.band_claimer;
     d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
     d.band_bits = g.band_bits;
-    d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv; d.ginv = g.ginv;
+    d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv; d.lq = g.lq;
 }
 
 struct LbmHandle {
@@ -828,8 +828,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     // RCM order and half bandwidth per wing
     std::vector<int> perm(ns), bw(W), rpos(ns);
-    std::vector<long long> lofs(W), iofs(W), gofs(W);
-    long long ltot = 0, itot = 0, gtot = 0;
+    std::vector<long long> lofs(W), iofs(W), qofs(W);
+    long long ltot = 0, itot = 0, qtot = 0;
     for (int w = 0; w < W; ++w) {
         const int nw = npts[w] - 1;
         std::vector<double> mx(nw), my(nw);
@@ -848,8 +848,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         ltot += ibm_wing_storage(nw, bw[w]);
         iofs[w] = itot;
         itot += ibm_linv_storage(nw);
-        gofs[w] = gtot;   // the wing's explicit inverse, nw x nw
-        gtot += (long long)nw * nw;
+        qofs[w] = qtot;   // the wing's 32-row panel inverses
+        qtot += ibm_panel_storage(nw);
     }
 
     // allocations
@@ -877,7 +877,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.band_n = band_n;
     int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr,
         *drpos = nullptr;
-    long long *dlofs = nullptr, *diofs = nullptr, *dgofs = nullptr;
+    long long *dlofs = nullptr, *diofs = nullptr, *dqofs = nullptr;
     double *xb0 = nullptr, *yb0 = nullptr;
     const size_t nsz = std::max(1, ns), npz = std::max(1, np), wz = std::max(1, W);
     if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
@@ -890,7 +890,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
         dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &diofs, wz) ||
         dalloc(h, &d.linv, (size_t)std::max<long long>(1, itot)) || dalloc(h, &d.wm, wz) ||
-        dalloc(h, &d.ginv, (size_t)std::max<long long>(1, gtot)) || dalloc(h, &dgofs, wz) ||
+        dalloc(h, &d.lq, (size_t)std::max<long long>(1, qtot)) || dalloc(h, &dqofs, wz) ||
         dalloc(h, &d.rel_pos, wz) || dalloc(h, &d.cycle, 1) || dalloc(h, &d.row_index, 1) ||
         dalloc(h, &d.gcycle, 1) || dalloc(h, &d.fin_count, 1) ||
         dalloc(h, &d.sum_row, (size_t)h->row_len) || dalloc(h, &d.sample_count, 1) || dalloc(h, &d.status, 1) ||
@@ -910,12 +910,12 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         CK(cudaMemcpy(dbw, bw.data(), W * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dlofs, lofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(diofs, iofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(dgofs, gofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dqofs, qofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
     }
     d.wing_pstart = pst; d.wing_sstart = sst; d.wing_npts = npw; d.seg_wing = sgw;
     d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs; d.rpos = drpos;
     d.wing_linv_ofs = diofs;
-    d.wing_gofs = dgofs;
+    d.wing_qofs = dqofs;
     h->ppw.assign(npts.begin(), npts.end());
     // dynamic shared memory of the factorisation kernel (one block per wing):
     // [staged panel rows][pair table][the wing's banded factor, if it fits]
@@ -938,15 +938,11 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.factor_in_smem = base + (size_t)wmax * sizeof(double) <= smem_cap ? 1 : 0;
     h->factor_smem = d.factor_in_smem ? base + (size_t)wmax * sizeof(double) : base;
     if (h->factor_smem > smem_cap) return fail(h, "immersed boundary: too many segments for one factorisation block");
-    // explicit inverse: the wing's factor is staged in shared memory when it
-    // fits, else read from global memory
-    if (ibm_inverse_smem(nwmax, bwmax, wmax, false) > smem_cap)
-        return fail(h, "immersed boundary: too many segments for the inverse kernel");
-    d.inv_in_smem = ibm_inverse_smem(nwmax, bwmax, wmax, true) <= smem_cap;
-    d.inv_smem = (long long)ibm_inverse_smem(nwmax, bwmax, wmax, d.inv_in_smem != 0);
-    d.inv_blocks = ibm_inverse_blocks(npts.data(), W);
-    d.apply_smem = (long long)ibm_apply_smem(nwmax, bwmax);
-    CK(ibm_prepare(h->factor_smem, (size_t)d.inv_smem, (size_t)d.apply_smem));
+    // substitution in 32-row panels: two vectors per wing block
+    d.solve_smem = (long long)ibm_solve_smem(nwmax, bwmax);
+    if ((size_t)d.solve_smem > smem_cap) return fail(h, "immersed boundary: too many segments for one substitution block");
+    d.panel_blocks = ibm_panel_blocks(npts.data(), W);
+    CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
         return -1;
@@ -963,7 +959,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             dalloc(h, &g.band_bits, band_bits_words(d)) ||
             dalloc(h, &g.ibm_flags, 4) || dalloc(h, &g.lband, (size_t)std::max<long long>(1, ltot)) ||
             dalloc(h, &g.linv, (size_t)std::max<long long>(1, itot)) ||
-            dalloc(h, &g.ginv, (size_t)std::max<long long>(1, gtot)))
+            dalloc(h, &g.lq, (size_t)std::max<long long>(1, qtot)))
             return -1;
     }
     if (ensure_rows(h, 1024)) return -1;
@@ -1237,7 +1233,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     };
     // block offsets of every packed kernel, in episode order
     std::vector<int> boff((size_t)MK_KINDS * (nh + 1), 0);
-    size_t factor_smem = 0, inv_smem = 0, apply_smem = 0;
+    size_t factor_smem = 0, solve_smem = 0;
     for (int k = 0; k < MK_KINDS; ++k)
         for (int e = 0; e < nh; ++e) {
             const long long nb = (long long)boff[(size_t)k * (nh + 1) + e] +
@@ -1247,8 +1243,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         }
     for (int e = 0; e < nh; ++e) {
         factor_smem = std::max(factor_smem, hs[order[e]]->factor_smem);
-        inv_smem = std::max(inv_smem, (size_t)hs[order[e]]->d.inv_smem);
-        apply_smem = std::max(apply_smem, (size_t)hs[order[e]]->d.apply_smem);
+        solve_smem = std::max(solve_smem, (size_t)hs[order[e]]->d.solve_smem);
     }
     // state-pointer tables of every step (variant indices, reused from two
     // steps earlier while the episode set and flags are unchanged)
@@ -1324,9 +1319,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         const int nb = boff[(size_t)k * (nh + 1) + ne];
         if (nb <= 0) return;
         MultiArgs m{reinterpret_cast<const DevState* const*>(b->d_buf + off_ptr) + at, bo, ne};
-        const size_t smem = (k == MK_FACTOR_SMEM || k == MK_FACTOR_GLOBAL) ? factor_smem
-                            : k == MK_APPLY                                ? apply_smem
-                                                                           : inv_smem;
+        const size_t smem = (k == MK_FACTOR_SMEM || k == MK_FACTOR_GLOBAL) ? factor_smem : solve_smem;
         if (!launch_multi_ibm(k, m, nb, st) && !launch_multi_solver(k, m, nb, smem, st)) launch_multi_fused(k, m, nb, st);
     };
     auto geometry = [&](size_t at, int ne, cudaStream_t sa, cudaStream_t sb, bool events) {
@@ -1337,8 +1330,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
             cudaEventRecord(b->ev_list, sa);
             cudaStreamWaitEvent(sb, b->ev_geom, 0);
         }
-        for (MultiKernel k : {MK_ASSEMBLE, MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_INVERSE_SMEM, MK_INVERSE_GLOBAL})
-            launch(k, at, ne, sb);
+        for (MultiKernel k : {MK_ASSEMBLE, MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_PANELS}) launch(k, at, ne, sb);
         if (events) cudaEventRecord(b->ev_fact, sb);
     };
     // The packed bulk kernel's runs per block: the tuned choice for this
@@ -1368,7 +1360,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         }
         launch(MK_BC, t.cur, t.a_cur, b->s_bc);
         cudaEventRecord(b->ev_bc, b->s_bc);
-        for (MultiKernel k2 : {MK_RHS, MK_APPLY, MK_SPREAD, MK_FINISH})
+        for (MultiKernel k2 : {MK_RHS, MK_SOLVE, MK_SPREAD, MK_FINISH})
             launch(k2, t.cur, t.a_cur, b->s_ibm);
         cudaEventRecord(b->ev_ibm, b->s_ibm);
         launch((MultiKernel)kind, t.cur, t.a_cur, b->s_bulk);
@@ -1417,7 +1409,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         // graph per two steps: captured the first time, kept for later calls
         if (!tune && k + 1 < K) {
             std::vector<long long> key = {(long long)(uintptr_t)b->d_buf, (long long)off_boff, (long long)off_ptr, nh,
-                                          (long long)factor_smem, (long long)inv_smem, (long long)apply_smem, kind};
+                                          (long long)factor_smem, (long long)solve_smem, kind};
             for (int q = 0; q < 2; ++q) {
                 const StepTab& u = steps[k + q];
                 key.insert(key.end(), {(long long)u.cur, (long long)u.ahead, u.a_cur, u.a_ahead});

@@ -147,12 +147,10 @@ struct DevState {
     long long factor_smem_off;   // its byte offset in the factor kernel's shared memory
     double* linv;                // inverses of the factor's diagonal blocks, per wing and panel
     const long long* wing_linv_ofs;  // W offsets into linv
-    double* ginv;                // explicit G^-1 per wing (segment order, nw x nw row-major)
-    const long long* wing_gofs;  // W offsets into ginv
-    int inv_in_smem;             // the inverse kernel stages the wing's factor in shared memory
-    int inv_blocks;              // blocks of the inverse kernel
-    long long inv_smem;          // dynamic shared memory of the inverse kernel (bytes)
-    long long apply_smem;        // dynamic shared memory of the apply kernel (bytes)
+    double* lq;                  // per wing and 32-row panel: inverse M of its unit lower block, then M^T
+    const long long* wing_qofs;  // W offsets into lq
+    int panel_blocks;            // blocks of the panel-inverse kernel
+    long long solve_smem;        // dynamic shared memory of the substitution kernel (bytes)
     // configuration of wing placement
     double wing_x_origin, wing_x_spacing, wing_y_origin, xc, yc;
     // motion source
