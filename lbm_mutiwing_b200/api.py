@@ -27,6 +27,7 @@ MOTION_STREAM = 2
 STEP_FIELDS = 1
 STEP_ERR = 2
 FLAG_NO_GRAPHS = 1
+FLAG_SOLVE_STREAM = 2
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}

@@ -15,25 +15,22 @@
 // over the common node columns i and rows j of the two boxes.  G is
 // assembled per wing in a banded layout after a reverse Cuthill-McKee
 // ordering fixed at set-up (rigid wings keep their pairwise distances) and
-// factored as L' D L'^T, panel by panel, one thread block per wing, and the
-// unit lower diagonal blocks of L' are inverted in panels of 32 rows.  G
-// depends on the geometry only, so assembly, factorisation and panel
-// inverses run on a side stream while the band list is built (on the FP32
-// path a step ahead), and the step itself substitutes 32 rows at a time.
+// factored as L' D L'^T, panel by panel, one thread block per wing.  G
+// depends on the geometry only, so assembly and factorisation run on a side
+// stream while the band list and the right-hand side are built.
 //
-// Kernels of one step's geometry (main chain | side chain):
+// Kernels of one step (main chain | side chain):
 //   geometry   motion, markers, midpoints, support boxes, kernel values,
 //              clearing of the previous band             (move_boundary)
 //   claim      lowest segment index claims each box node   | assemble  G
-//   count      claims per segment, coupled-wing check      | factor    L' D L'^T
-//   scan       band-list offsets                           | panels    32-row block inverses
+//   count      claims per segment                          | factor    L' D L'^T
+//   scan       band-list offsets, coupled-wing check       |
 //   list       band list in the reference's order (segment, i, j), band
 //              bit plane; advances the geometry's cycle counter
 // then, plain FP64 path:
 //   ustar      u*, rho at band nodes; zeroed spread accumulators
 //   rhs        r = ub - X u* (one warp per segment)
-//   solve      G y = r per wing in 32-row panels (and the joint solve of
-//              wings whose supports share nodes)
+//   solve      forward and backward substitution (waits for the factor)
 //   spread     du = X^T y with fixed-point integer atomics
 //   finish     du, body force, per-block force partials
 //   forces     per-wing force and moment, force row
@@ -955,7 +952,7 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
 }
 
 void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st) {
-    launch_ibm_substitution(d, st);
+    launch_ibm_substitution(d, (size_t)d.solve_smem, st);
     ibm_spread_kernel<<<slot_grid(d), 256, 0, st>>>(d);
     const int nbk = ibm_finish_blocks(d);
     if (fused) {

@@ -1,9 +1,7 @@
 // Banded L' D L'^T factorisation and substitution for the immersed-boundary
 // system G y = r of each wing (G = X X^T in reverse Cuthill-McKee order; see
 // ibm.cu for how G arises from immersed_boundary_Wu,
-// boundary_condition.f90:1558-1640).  The geometry pipeline factors G and
-// inverts the unit lower diagonal blocks of L' in panels of 32 rows; the
-// step's chain then substitutes 32 rows per step.
+// boundary_condition.f90:1558-1640).
 //
 // Blocked right-looking algorithm, PANEL = 8 columns at a time, one thread
 // block per wing, the wing's banded matrix held in shared memory (brought in
@@ -16,10 +14,9 @@
 //      warps 1.., while warp 0 updates the next panel's 8 x 8 diagonal block
 //      first and one thread factors it in registers (look-ahead: the
 //      sequential pivot chain of panel p + 1 overlaps panel p's update).
-// The substitutions apply each panel through the inverse of its unit lower
-// block and the reciprocal pivots and update the rows below (forward) or
-// above (backward) it: on the chain in panels of 32 rows, in the joint solve
-// of coupled wings in the factor's panels of 8.
+// The substitution applies each panel through its stored 8 x 8 inverse and
+// reciprocal pivots and updates the rows below (forward) or above
+// (backward) it, one warp per velocity component.
 //
 // The zero zones of the banded storage (entries past the bandwidth, rows past
 // the last segment) make every panel-shaped read in bounds and zero where it
@@ -35,6 +32,7 @@ namespace lbm {
 constexpr int PANEL = IBM_PANEL;
 constexpr int FACTOR_THREADS = 256;
 constexpr int FACTOR_WARPS = FACTOR_THREADS / 32;
+constexpr int SOLVE_THREADS = 64;
 constexpr int SP = PANEL + 1;           // odd row stride of staged panel rows
 constexpr int TILE = 4;                 // register tile of the trailing update
 static_assert(IBM_MAX_BANDWIDTH <= FACTOR_THREADS - 32, "rows below a panel leave the last warp free");
@@ -295,81 +293,19 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ibm_factor_kernel_multi(MultiA
     ibm_factor_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// ------------------------------------------------------------ substitution
-// One warp solves L' D L'^T x = z in place (z in shared memory, zero from
-// row nw up to nw + PANEL + bw): per panel (forward) w_p = Li_p z_p,
-// z_p = w_p / d, rows below -= L' w_p; per panel, last first (backward)
-// y_p = Li_p^T z_p, rows above -= L'^T y_p.  A: the wing's banded storage at
-// row 0; L: its per-panel inverses and reciprocal pivots.  The forward pass
-// starts at panel pan0 (z is zero before it, so earlier panels change
-// nothing).
-__device__ void warp_substitute(const double* A, int ld, const double* L, int nw, int bw, double* z, int lane,
-                                int pan0) {
-    const int li = lane & (PANEL - 1);
-    const int npan = (nw + PANEL - 1) / PANEL;
-    for (int pan = pan0, k0 = pan0 * PANEL; k0 < nw; k0 += PANEL, ++pan) {
-        const int np = min(PANEL, nw - k0);
-        const double* Li = L + pan * IBM_PANEL_AUX;
-        double w0 = 0.0, w1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < PANEL / 2; ++k) {
-            w0 = w0 + Li[li * PANEL + k] * z[k0 + k];
-            w1 = w1 + Li[li * PANEL + k + PANEL / 2] * z[k0 + k + PANEL / 2];
-        }
-        const double wl = w0 + w1;
-        double wc[PANEL];
-#pragma unroll
-        for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
-        for (int rb = lane; rb < bw; rb += 32) {
-            const int i = k0 + np + rb;
-            const double* row = A + (long long)i * ld + (i - k0);
-            double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-            for (int c = 0; c < PANEL / 2; ++c) {
-                a0 = a0 + row[-c] * wc[c];
-                a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
-            }
-            z[i] -= a0 + a1;
-        }
-        if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
-        __syncwarp();
-    }
-    for (int pan = npan - 1; pan >= 0; --pan) {
-        const int k0 = pan * PANEL;
-        const double* Li = L + pan * IBM_PANEL_AUX;
-        double y0 = 0.0, y1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < PANEL / 2; ++k) {
-            y0 = y0 + Li[k * PANEL + li] * z[k0 + k];
-            y1 = y1 + Li[(k + PANEL / 2) * PANEL + li] * z[k0 + k + PANEL / 2];
-        }
-        const double yl = y0 + y1;
-        double yc[PANEL];
-#pragma unroll
-        for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
-        const int above = min(bw, k0);
-        for (int r = lane; r < above; r += 32) {
-            const int j = k0 - 1 - r;
-            const double* col = A + (long long)k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
-            double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-            for (int c = 0; c < PANEL / 2; ++c) {
-                a0 = a0 + col[c * (ld + 1)] * yc[c];
-                a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
-            }
-            z[j] -= a0 + a1;
-        }
-        if (lane < PANEL) z[k0 + lane] = yl;
-        __syncwarp();
-    }
-}
-
-// Rows of a substitution panel on the step's chain (four factor panels).
-constexpr int QP = 32;
-constexpr int QP_AUX = 2 * QP * QP;   // a panel's inverse block M, row-major, then M^T
-__host__ __device__ inline int qpanels(int nw) { return (nw + QP - 1) / QP; }
-// Per-warp vector length of the substitutions (even: 16-byte multiples).
-__host__ __device__ inline int solve_zlen(int nw_max, int bw_max) { return (nw_max + QP + bw_max + 1) & ~1; }
+// Streaming of a wing's factor through shared memory when it does not fit
+// whole: chunks of RING_ROWS consecutive rows (contiguous in global memory)
+// are brought in by bulk copies into a ring of slots, each slot led by a
+// zero row (the forward pass reads a little above the diagonal, which the
+// banded layout keeps at zero in the previous row).  The forward pass needs
+// the bw rows below the current panel, the backward pass the panel's own
+// rows; the next chunk is in flight while the current ones are used.
+constexpr int RING_ROWS = 16;
+constexpr int RING_MAX_SLOTS = 16;
+static_assert(RING_ROWS % PANEL == 0, "a panel's rows lie in one chunk");
+__host__ __device__ inline int ring_slots(int bw) { return (bw + PANEL + RING_ROWS - 1) / RING_ROWS + 2; }
+size_t ibm_solve_ring_bytes(int bw) { return (size_t)ring_slots(bw) * (RING_ROWS + 1) * ibm_ld(bw) * sizeof(double); }
+bool ibm_solve_ring_fits(int bw) { return ring_slots(bw) <= RING_MAX_SLOTS; }
 
 // ------------------------------------------------- joint solve of coupled wings
 // When two wings' supports share lattice nodes, G has entries between their
@@ -378,7 +314,7 @@ __host__ __device__ inline int solve_zlen(int nw_max, int bw_max) { return (nw_m
 // 1609-1640).  The joint system G y = r is then solved by conjugate
 // gradients preconditioned with the per-wing factors (G is symmetric
 // positive definite, the preconditioner block diagonal), starting from the
-// per-wing solution G_w^-1 r_w.  One warp per velocity component; products G p are
+// per-wing solution.  One warp per velocity component; products G p are
 // formed as X (X^T p): a spread onto the band nodes with 64-bit fixed-point
 // integer atomics (order-independent, so results are reproducible) and an
 // interpolation back; dot products are lane-strided sums added by a fixed
@@ -431,16 +367,74 @@ __device__ void cg_product(const DevState& d, const double* in, double* out, uns
 }
 
 // out = D^-1 in for one component, D the block-diagonal part of G: each
-// wing's substitution with its banded factor and per-panel inverses read
-// from global memory, one warp, z a shared-memory vector of solve_zlen
-// doubles.
+// wing's forward and backward substitution with its banded factor and
+// per-panel inverses read from global memory, one warp, z a shared-memory
+// vector of at least nw_max + PANEL + bw_max doubles.
 __device__ void cg_precondition(const DevState& d, const double* in, double* out, double* z, int lane) {
+    const int li = lane & (PANEL - 1);
     for (int w = 0; w < d.wing_count; ++w) {
         const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
+        const int npan = (nw + PANEL - 1) / PANEL;
+        const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
+        const double* L = d.linv + d.wing_linv_ofs[w];
         const int* perm = d.perm + s0;
         for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? in[perm[p]] : 0.0;
         __syncwarp();
-        warp_substitute(d.lband + d.wing_lofs[w] + ld, ld, d.linv + d.wing_linv_ofs[w], nw, bw, z, lane, 0);
+        for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {   // L' D v = r
+            const int np = min(PANEL, nw - k0);
+            const double* Li = L + pan * IBM_PANEL_AUX;
+            double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < PANEL / 2; ++k) {
+                w0 = w0 + Li[li * PANEL + k] * z[k0 + k];
+                w1 = w1 + Li[li * PANEL + k + PANEL / 2] * z[k0 + k + PANEL / 2];
+            }
+            const double wl = w0 + w1;
+            double wc[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
+            for (int rb = lane; rb < bw; rb += 32) {
+                const int i = k0 + np + rb;
+                const double* row = A + (long long)i * ld + (i - k0);
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + row[-c] * wc[c];
+                    a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
+                }
+                z[i] -= a0 + a1;
+            }
+            if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
+            __syncwarp();
+        }
+        for (int pan = npan - 1; pan >= 0; --pan) {   // L'^T y = v
+            const int k0 = pan * PANEL;
+            const double* Li = L + pan * IBM_PANEL_AUX;
+            double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < PANEL / 2; ++k) {
+                y0 = y0 + Li[k * PANEL + li] * z[k0 + k];
+                y1 = y1 + Li[(k + PANEL / 2) * PANEL + li] * z[k0 + k + PANEL / 2];
+            }
+            const double yl = y0 + y1;
+            double yc[PANEL];
+#pragma unroll
+            for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
+            const int above = min(bw, k0);
+            for (int r = lane; r < above; r += 32) {
+                const int j = k0 - 1 - r;
+                const double* col = A + (long long)k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + col[c * (ld + 1)] * yc[c];
+                    a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
+                }
+                z[j] -= a0 + a1;
+            }
+            if (lane < PANEL) z[k0 + lane] = yl;
+            __syncwarp();
+        }
         for (int p = lane; p < nw; p += 32) out[perm[p]] = z[p];
         __syncwarp();
     }
@@ -518,174 +512,224 @@ __device__ void cg_joint_solve(const DevState& d, double* z, int comp, int lane)
     }
 }
 
-
-// ------------------------------------------------------------ panel inverses
-// For the step's substitution in panels of QP = 32 rows, the inverse M of
-// each panel's unit lower diagonal block B of L' (rows and columns k0 ..
-// k0 + 31 of a wing; identity past the wing's last segment), built in the
-// geometry pipeline beside the running step: one warp per panel, lane c
-// forms column c by block forward substitution over the panel's four factor
-// panels -- the entries of B outside the 8 x 8 diagonal blocks come from the
-// banded storage, the 8 x 8 diagonal blocks through their stored inverses
-// (the factorisation keeps only those).  Stored per panel as M row-major
-// then M^T, so that both substitution passes read 32 consecutive values per
-// warp load.
-constexpr int PANELS_WARPS = 4;
-
-__device__ __forceinline__ void ibm_panels_body(const DevState& d, int bid_) {
-    __shared__ double X[PANELS_WARPS][QP][QP];
-    __shared__ double S8[PANELS_WARPS][PANEL][QP];
-    const int tid = threadIdx.x, lane = tid & 31, q = tid >> 5;
-    int w = 0, b = bid_ * PANELS_WARPS + q;
-    for (; w < d.wing_count; ++w) {
-        const int nq = qpanels(d.wing_npts[w] - 1);
-        if (b < nq) break;
-        b -= nq;
-    }
-    if (w >= d.wing_count) return;
-    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw);
-    const int k0 = b * QP, np = min(QP, nw - k0), c = lane;
-    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
-    const double* L8 = d.linv + d.wing_linv_ofs[w] + (long long)(k0 / PANEL) * IBM_PANEL_AUX;
-    double(*x)[QP] = X[q];
-    double(*s8)[QP] = S8[q];
-    for (int r = 0; r < QP; ++r) x[r][c] = (r == c) ? 1.0 : 0.0;
-    const int nb8 = (np + PANEL - 1) / PANEL;
-    for (int a8 = 0; a8 < nb8; ++a8) {
-        const int r0 = a8 * PANEL;
-        // s = e_c - (off-diagonal-block part of B) x over the earlier factor panels
-        for (int i = 0; i < PANEL; ++i) {
-            const int r = r0 + i;
-            double acc = 0.0;
-            if (r < np) {
-                const double* row = A + (long long)(k0 + r) * ld;   // entry r - m: column m of the panel
-                for (int m = max(c, r - bw); m < r0; ++m) acc = acc + row[r - m] * x[m][c];
-            }
-            s8[i][c] = x[r][c] - acc;
-        }
-        // x over this factor panel = (its inverse 8 x 8 block) s
-        const double* Li = L8 + a8 * IBM_PANEL_AUX;
-        for (int i = 0; i < PANEL; ++i) {
-            double v = 0.0;
-#pragma unroll
-            for (int k = 0; k < PANEL; ++k) v = v + Li[i * PANEL + k] * s8[k][c];
-            if (r0 + i < np) x[r0 + i][c] = v;
-        }
-    }
-    double* M = d.lq + d.wing_qofs[w] + (long long)b * QP_AUX;
-    for (int r = 0; r < QP; ++r) {
-        M[r * QP + c] = x[r][c];             // row r of M, lanes along the row
-        M[QP * QP + c * QP + r] = x[r][c];   // M^T: row c of M^T is column c of M
-    }
-}
-__global__ void __launch_bounds__(32 * PANELS_WARPS) ibm_panels_kernel(DevState d) { ibm_panels_body(d, blockIdx.x); }
-__global__ void __launch_bounds__(32 * PANELS_WARPS) ibm_panels_kernel_multi(MultiArgs m) {
-    const int e = multi_episode(m, blockIdx.x);
-    ibm_panels_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
-}
-
-// ------------------------------------------------------------ substitution on the chain
-// G y = r for every wing: one block per wing, warp 0 for the x component,
-// warp 1 for y, in panels of 32 rows: per panel (forward) t = M z_p, rows
-// below -= L' t, z_p = D^-1 t; per panel, last first (backward) y_p = M^T
-// z_p, rows above -= L'^T y_p.  Every lane owns one row of a panel, so a
-// panel step is one 32-term dot product per lane instead of four dependent
-// 8-row steps.  The right-hand sides are read from qx, qy (as the rhs kernel
-// built them), the solutions written to rx, ry, and each wing's largest |y|
-// (the spread's fixed-point scale) to ymax.  When supports of different
-// wings share nodes, the last wing block to finish (a per-episode counter
-// after a fence; no block waits) solves the joint system from these
-// per-wing solutions before the spread reads them.
-constexpr int SOLVE_THREADS = 64;
-
-__device__ __forceinline__ void ibm_solve_body(const DevState& d, int bid_) {
+// Forward and backward substitution with the factor of wing w: warp 0 solves
+// for the x component, warp 1 for the y component, on shared-memory copies
+// of the per-panel inverses and pivots, of the factor (whole when it fits,
+// else streamed through a ring of rows, else read from global memory) and
+// of the right-hand sides.  Shared memory: [2 right-hand sides with zero
+// tails][permutation][per-panel inverse blocks and pivots][factor or ring].
+// Each lane updates rows lane and lane + 32 below or above a panel
+// (bw <= 64) or loops.  SMEM: the factor is copied to shared memory whole.
+template <bool SMEM>
+__device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const int bid_) {
     extern __shared__ __align__(16) double sm[];
+    __shared__ uint64_t bar;
+    __shared__ uint64_t sbar[RING_MAX_SLOTS];
+    __shared__ uint32_t suse[RING_MAX_SLOTS];
     const int w = bid_;
     const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
     const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], ld = ibm_ld(bw), s0 = d.wing_sstart[w];
-    const int nq = qpanels(nw);
-    const int zlen = solve_zlen(d.nw_max, d.bw_max);
+    const int npan = (nw + PANEL - 1) / PANEL;
+    const int zlen = d.nw_max + PANEL + d.bw_max;
     double* z = sm + comp * zlen;
-    double* t = sm + 2 * zlen + comp * QP;
-    const double* A = d.lband + d.wing_lofs[w] + ld;   // row 0
-    const double* Q = d.lq + d.wing_qofs[w];
-    const double* L8 = d.linv + d.wing_linv_ofs[w];
-    const int* perm = d.perm + s0;
-    const double* rin = comp ? d.qy : d.qx;
-    for (int p = lane; p < nw + QP + bw; p += 32) z[p] = p < nw ? rin[perm[p]] : 0.0;
-    __syncwarp();
-    for (int qi = 0; qi < nq; ++qi) {   // L' D v = r
-        const int k0 = qi * QP, np = min(QP, nw - k0);
-        const double* MT = Q + (long long)qi * QP_AUX + QP * QP;
-        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+    int* perm = reinterpret_cast<int*>(sm + 2 * zlen);
+    double* Lsh = reinterpret_cast<double*>(perm + ((d.nw_max + 3) & ~3));
+    double* Sm = Lsh + ibm_linv_storage(d.nw_max);
+    const double* gS = d.lband + d.wing_lofs[w];
+    const long long lbytes = (long long)npan * IBM_PANEL_AUX * 8;
+    const long long sbytes = SMEM ? ibm_wing_storage(nw, bw) * 8 : 0;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, (uint32_t)(lbytes + sbytes));
+        bulk_load_all(Lsh, d.linv + d.wing_linv_ofs[w], lbytes, &bar);
+        if (sbytes) bulk_load_all(Sm, gS, sbytes, &bar);
+    }
+#pragma unroll 4
+    for (int p = tid; p < nw; p += SOLVE_THREADS) perm[p] = d.perm[s0 + p];
+    __syncthreads();
+    double* rr = comp == 0 ? d.rx : d.ry;
 #pragma unroll 8
-        for (int c = 0; c < QP; c += 4) {
-            w0 = w0 + MT[c * QP + lane] * z[k0 + c];
-            w1 = w1 + MT[(c + 1) * QP + lane] * z[k0 + c + 1];
-            w2 = w2 + MT[(c + 2) * QP + lane] * z[k0 + c + 2];
-            w3 = w3 + MT[(c + 3) * QP + lane] * z[k0 + c + 3];
+    for (int p = lane; p < nw + PANEL + bw; p += 32) z[p] = p < nw ? rr[perm[p]] : 0.0;
+    const bool ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+        mbar_wait(&bar, 0);
+        return;
+    }
+    const double* A = (SMEM ? Sm : gS) + ld;   // row 0
+    const int li = lane & (PANEL - 1);
+    // the streamed form (not SMEM, the ring fits)
+    const bool stream = !SMEM && d.solve_stream;
+    const int NB = ring_slots(bw), nrows = nw + PANEL + bw;
+    const int nq = (nrows + RING_ROWS - 1) / RING_ROWS;
+    double* ring = Sm;
+    auto rowp = [&](int i) -> const double* {   // row i (entry 0 = the diagonal)
+        if (!stream) return A + (long long)i * ld;
+        const int q = i / RING_ROWS;
+        return ring + ((q % NB) * (RING_ROWS + 1) + 1 + (i - q * RING_ROWS)) * ld;
+    };
+    auto issue = [&](int q) {   // thread 0: chunk q into its slot
+        const int s = q % NB;
+        const int rows = min(RING_ROWS, nrows - q * RING_ROWS);
+        const uint32_t bytes = (uint32_t)rows * ld * 8;
+        fence_async_smem();
+        mbar_arrive_expect_tx(&sbar[s], bytes);
+        bulk_load_all(ring + (s * (RING_ROWS + 1) + 1) * ld, gS + (1 + (long long)q * RING_ROWS) * ld, bytes, &sbar[s]);
+        suse[s] += 1;
+    };
+    auto wait_chunk = [&](int q) { return mbar_wait(&sbar[q % NB], (suse[q % NB] - 1) & 1); };
+    auto drain = [&]() {   // every issued copy complete (bounded)
+        bool all = true;
+        for (int s = 0; s < NB; ++s)
+            if (suse[s]) all &= mbar_wait(&sbar[s], (suse[s] - 1) & 1);
+        return all;
+    };
+    int qi = 0;   // next chunk to issue (thread 0)
+    if (stream) {
+        for (int t = tid; t < NB * ld; t += SOLVE_THREADS) ring[(t / ld) * (RING_ROWS + 1) * ld + t % ld] = 0.0;
+        if (tid < NB) {
+            mbar_init(&sbar[tid], 1);
+            suse[tid] = 0;
         }
-        const double tl = (w0 + w1) + (w2 + w3);
-        t[lane] = tl;
-        __syncwarp();
-        for (int rb = lane; rb < bw; rb += 32) {
-            const int i = k0 + np + rb;
-            const double* row = A + (long long)i * ld + (i - k0);   // L'(i, k0 + c) at row[-c]
-            double a0 = 0.0, a1 = 0.0;
-            int c = max(0, i - k0 - bw);
-            for (; c + 1 < np; c += 2) {
-                a0 = a0 + row[-c] * t[c];
-                a1 = a1 + row[-(c + 1)] * t[c + 1];
+        __syncthreads();
+    }
+    // L' D v = r: per panel w_p = Li_p z_p, v_p = w_p / d, rows below -= L' w_p
+    for (int k0 = 0, pan = 0; k0 < nw; k0 += PANEL, ++pan) {
+        const int np = min(PANEL, nw - k0);
+        if (stream) {   // rows k0 + np .. k0 + np + bw - 1 resident, the next chunk in flight
+            const int lo = (k0 + np) / RING_ROWS, hi = min(nq - 1, (k0 + np + bw - 1) / RING_ROWS);
+            __syncthreads();
+            if (tid == 0)
+                for (; qi < nq && qi <= hi + 1 && qi - NB < lo; ++qi) issue(qi);
+            __syncthreads();
+            bool ok = true;
+            for (int q = lo; q <= hi; ++q) ok &= wait_chunk(q);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+                drain();
+                return;
             }
-            if (c < np) a0 = a0 + row[-c] * t[c];
-            z[i] -= a0 + a1;
         }
-        if (lane < np) {
-            const int k = k0 + lane;
-            z[k] = tl * L8[(long long)(k / PANEL) * IBM_PANEL_AUX + PANEL * PANEL + (k % PANEL)];
+        const double* Li = Lsh + pan * IBM_PANEL_AUX;
+        double zk[PANEL], lk[PANEL];
+#pragma unroll
+        for (int k = 0; k < PANEL; ++k) {
+            zk[k] = z[k0 + k];
+            lk[k] = Li[li * PANEL + k];
         }
+        double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < PANEL / 2; ++k) {
+            w0 = w0 + lk[k] * zk[k];
+            w1 = w1 + lk[k + PANEL / 2] * zk[k + PANEL / 2];
+        }
+        const double wl = w0 + w1;
+        double wc[PANEL];
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
+        for (int rb0 = 0; rb0 < bw; rb0 += 64) {
+            double acc[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rb = min(rb0 + lane + 32 * h, bw - 1);
+                const int i = k0 + np + rb;
+                const double* row = rowp(i) + (i - k0);
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + row[-c] * wc[c];
+                    a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
+                }
+                acc[h] = a0 + a1;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rb = rb0 + lane + 32 * h;
+                if (rb < bw) z[k0 + np + rb] -= acc[h];
+            }
+        }
+        if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
         __syncwarp();
     }
-    for (int qi = nq - 1; qi >= 0; --qi) {   // L'^T y = v
-        const int k0 = qi * QP, np = min(QP, nw - k0);
-        const double* M = Q + (long long)qi * QP_AUX;
-        double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
-#pragma unroll 8
-        for (int c = 0; c < QP; c += 4) {
-            y0 = y0 + M[c * QP + lane] * z[k0 + c];
-            y1 = y1 + M[(c + 1) * QP + lane] * z[k0 + c + 1];
-            y2 = y2 + M[(c + 2) * QP + lane] * z[k0 + c + 2];
-            y3 = y3 + M[(c + 3) * QP + lane] * z[k0 + c + 3];
+    // L'^T y = v: per panel (last first) y_p = Li_p^T v_p, rows above -= L'^T y_p
+    int qb = (npan - 1) * PANEL / RING_ROWS;   // next chunk to issue, downwards (thread 0)
+    if (stream) {   // no copy of the forward pass still in flight
+        const bool ok = drain();
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+            drain();
+            return;
         }
-        const double yl = (y0 + y1) + (y2 + y3);
-        t[lane] = yl;
-        __syncwarp();
+    }
+    for (int pan = npan - 1; pan >= 0; --pan) {
+        const int k0 = pan * PANEL;
+        if (stream) {   // the panel's rows (one chunk) resident, the chunk below in flight
+            const int c = k0 / RING_ROWS;
+            __syncthreads();
+            if (tid == 0)
+                for (; qb >= 0 && qb >= c - 1 && qb + NB > c; --qb) issue(qb);
+            __syncthreads();
+            const bool ok = wait_chunk(c);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+                drain();
+                return;
+            }
+        }
+        const double* Li = Lsh + pan * IBM_PANEL_AUX;
+        double vk[PANEL], lk[PANEL];
+#pragma unroll
+        for (int k = 0; k < PANEL; ++k) {
+            vk[k] = z[k0 + k];
+            lk[k] = Li[k * PANEL + li];
+        }
+        double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < PANEL / 2; ++k) {
+            y0 = y0 + lk[k] * vk[k];
+            y1 = y1 + lk[k + PANEL / 2] * vk[k + PANEL / 2];
+        }
+        const double yl = y0 + y1;
+        double yc[PANEL];
+#pragma unroll
+        for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
         const int above = min(bw, k0);   // rows k0 - above .. k0 - 1
-        for (int r = lane; r < above; r += 32) {
-            const int j = k0 - 1 - r;
-            const double* col = A + (long long)k0 * ld + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
-            const int cmax = min(np, bw - (k0 - j) + 1);
-            double a0 = 0.0, a1 = 0.0;
-            int c = 0;
-            for (; c + 1 < cmax; c += 2) {
-                a0 = a0 + col[c * (ld + 1)] * t[c];
-                a1 = a1 + col[(c + 1) * (ld + 1)] * t[c + 1];
+        for (int r0 = 0; r0 < above; r0 += 64) {
+            double acc[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = min(r0 + lane + 32 * h, above - 1);
+                const int j = k0 - 1 - r;
+                const double* col = rowp(k0) + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < PANEL / 2; ++c) {
+                    a0 = a0 + col[c * (ld + 1)] * yc[c];
+                    a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
+                }
+                acc[h] = a0 + a1;
             }
-            if (c < cmax) a0 = a0 + col[c * (ld + 1)] * t[c];
-            z[j] -= a0 + a1;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + lane + 32 * h;
+                if (r < above) z[k0 - 1 - r] -= acc[h];
+            }
         }
-        if (lane < np) z[k0 + lane] = yl;
+        if (lane < PANEL) z[k0 + lane] = yl;
         __syncwarp();
     }
-    double* rout = comp ? d.ry : d.rx;
+    if (stream && !drain() && lane == 0) solver_status(d, ST_COPY_TIMEOUT);
     double ym = 0.0;
+#pragma unroll 4
     for (int p = lane; p < nw; p += 32) {
-        rout[perm[p]] = z[p];
+        rr[perm[p]] = z[p];
         ym = fmax(ym, fabs(z[p]));
     }
-#pragma unroll
     for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
     if (lane == 0) d.ymax[2 * w + comp] = ym;
+    // Supports of different wings share nodes: the last wing block to finish
+    // (a per-episode counter after a fence; no block waits) solves the joint
+    // system from the per-wing solutions, before the spread reads them.
     if (d.wing_count > 1 && __ldcg(d.ibm_flags) != 0) {
         __shared__ int last;
         __threadfence();
@@ -698,13 +742,14 @@ __device__ __forceinline__ void ibm_solve_body(const DevState& d, int bid_) {
         cg_joint_solve(d, z, comp, lane);
     }
 }
-__global__ void __launch_bounds__(SOLVE_THREADS, 1) ibm_solve_kernel(DevState d) { ibm_solve_body(d, blockIdx.x); }
+template <bool SMEM>
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) { ibm_solve_kernel_body<SMEM>(d, blockIdx.x); }
+template <bool SMEM>
 __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
-    ibm_solve_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+    ibm_solve_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
-// ------------------------------------------------------------ host side
 size_t ibm_factor_staging_bytes(int bw_max) {
     const int nt = round_tile(bw_max) / TILE;
     const size_t rows = (size_t)2 * SP * round_tile(bw_max) * sizeof(double);   // a multiple of 16
@@ -712,16 +757,11 @@ size_t ibm_factor_staging_bytes(int bw_max) {
     return rows + (tl + 15) / 16 * 16;
 }
 
-size_t ibm_solve_smem(int nw_max, int bw_max) {
-    return (size_t)(2 * solve_zlen(nw_max, bw_max) + 2 * QP) * sizeof(double);
-}
-
-long long ibm_panel_storage(int nw) { return (long long)qpanels(nw) * QP_AUX; }
-
-int ibm_panel_blocks(const int* points_per_wing, int wing_count) {
-    int n = 0;
-    for (int w = 0; w < wing_count; ++w) n += qpanels(points_per_wing[w] - 1);
-    return (n + PANELS_WARPS - 1) / PANELS_WARPS;
+size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool factor_in_smem) {
+    const size_t z = (size_t)2 * (nw_max + PANEL + bw_max) * sizeof(double);
+    const size_t perm = (size_t)((nw_max + 3) & ~3) * sizeof(int);
+    const size_t inv = (size_t)ibm_linv_storage(nw_max) * sizeof(double);
+    return z + perm + inv + (factor_in_smem ? (size_t)wing_storage_max * sizeof(double) : 0);
 }
 
 // The dynamic shared-memory limit is a per-device property of each kernel,
@@ -749,25 +789,24 @@ cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     if (dev < 64 && (g_prepared_devices >> dev) & 1ULL) return cudaSuccess;
     e = raise_smem_limit(ibm_factor_kernel<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel<false>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel<false>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<false>, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel, optin);
-    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<true>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<false>, optin);
     if (e == cudaSuccess && dev < 64) g_prepared_devices |= 1ULL << dev;
     return e;
 }
 
-// Factorisation and panel inverses: kernels of the geometry pipeline.
 bool is_factor_multi_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<true>) ||
-           func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<false>) ||
-           func == reinterpret_cast<const void*>(ibm_panels_kernel_multi);
+           func == reinterpret_cast<const void*>(ibm_factor_kernel_multi<false>);
 }
 
 bool is_factor_kernel(const void* func) {
     return func == reinterpret_cast<const void*>(ibm_factor_kernel<true>) ||
-           func == reinterpret_cast<const void*>(ibm_factor_kernel<false>) ||
-           func == reinterpret_cast<const void*>(ibm_panels_kernel);
+           func == reinterpret_cast<const void*>(ibm_factor_kernel<false>);
 }
 
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st) {
@@ -776,24 +815,25 @@ void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_
         ibm_factor_kernel<true><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
     else
         ibm_factor_kernel<false><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
-    ibm_panels_kernel<<<d.panel_blocks, 32 * PANELS_WARPS, 0, st>>>(d);
 }
 
-void launch_ibm_substitution(const DevState& d, cudaStream_t st) {
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st) {
     if (d.wing_count <= 0) return;
-    ibm_solve_kernel<<<d.wing_count, SOLVE_THREADS, (size_t)d.solve_smem, st>>>(d);
+    if (d.solve_in_smem)
+        ibm_solve_kernel<true><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+    else
+        ibm_solve_kernel<false><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
 }
 
-// Packed launches: one block per wing of every episode (factorisation,
-// substitution), the panel inverses' warps; episodes whose factor does not
-// take the kind's shared-memory form get no blocks in it.  The dynamic
-// shared memory is the largest of the batch.
+// Packed launches: one block per wing of every episode; episodes whose
+// factor (or substitution) does not take the kind's shared-memory form get
+// no blocks in it.  The dynamic shared memory is the largest of the batch.
 int multi_blocks_solver(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_FACTOR_SMEM: return d.factor_in_smem ? d.wing_count : 0;
     case MK_FACTOR_GLOBAL: return d.factor_in_smem ? 0 : d.wing_count;
-    case MK_PANELS: return d.wing_count > 0 ? d.panel_blocks : 0;
-    case MK_SOLVE: return d.wing_count;
+    case MK_SOLVE_SMEM: return d.solve_in_smem ? d.wing_count : 0;
+    case MK_SOLVE_GLOBAL: return d.solve_in_smem ? 0 : d.wing_count;
     default: return -1;
     }
 }
@@ -802,8 +842,8 @@ bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int nb, size_t smem,
     switch (k) {
     case MK_FACTOR_SMEM: ibm_factor_kernel_multi<true><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
     case MK_FACTOR_GLOBAL: ibm_factor_kernel_multi<false><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
-    case MK_PANELS: ibm_panels_kernel_multi<<<nb, 32 * PANELS_WARPS, 0, st>>>(m); return true;
-    case MK_SOLVE: ibm_solve_kernel_multi<<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
+    case MK_SOLVE_SMEM: ibm_solve_kernel_multi<true><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
+    case MK_SOLVE_GLOBAL: ibm_solve_kernel_multi<false><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
     default: return false;
     }
 }

@@ -147,9 +147,8 @@ struct DevState {
     long long factor_smem_off;   // its byte offset in the factor kernel's shared memory
     double* linv;                // inverses of the factor's diagonal blocks, per wing and panel
     const long long* wing_linv_ofs;  // W offsets into linv
-    double* lq;                  // per wing and 32-row panel: inverse M of its unit lower block, then M^T
-    const long long* wing_qofs;  // W offsets into lq
-    int panel_blocks;            // blocks of the panel-inverse kernel
+    int solve_in_smem;           // the substitution copies the wing's factor to shared memory
+    int solve_stream;            // otherwise it streams the factor through a ring of rows in shared memory
     long long solve_smem;        // dynamic shared memory of the substitution kernel (bytes)
     // configuration of wing placement
     double wing_x_origin, wing_x_spacing, wing_y_origin, xc, yc;

@@ -43,23 +43,19 @@ int ibm_finish_blocks(const DevState& d);
 // kernels of a step's geometry (motion through factorisation)
 bool is_geometry_kernel(const void* func);
 bool is_factor_kernel(const void* func);
-// banded L' D L'^T factorisation, panel inverses and substitution
-// (ibm_solver.cu)
+// banded L' D L'^T factorisation and substitution (ibm_solver.cu)
 cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem);
-// dynamic shared memory of the substitution kernel (two vectors per wing
-// block, their panel buffers)
-size_t ibm_solve_smem(int nw_max, int bw_max);
-// doubles of a wing's panel inverses, and the blocks of the kernel that
-// builds them (four 32-row panels per block)
-long long ibm_panel_storage(int nw);
-int ibm_panel_blocks(const int* points_per_wing, int wing_count);
+// dynamic shared memory of the substitution kernel
+size_t ibm_solve_smem(int nw_max, int bw_max, long long wing_storage_max, bool factor_in_smem);
+// shared memory of the row ring when the factor is streamed, and whether
+// its slot count is within the kernel's barrier table
+size_t ibm_solve_ring_bytes(int bw);
+bool ibm_solve_ring_fits(int bw);
 // shared memory of the factorisation kernel ahead of the wing's storage
 // (a multiple of 16 bytes)
 size_t ibm_factor_staging_bytes(int bw_max);
-// factorisation and panel inverses of every wing (geometry pipeline)
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st);
-// G y = r per wing, joint solve of coupled wings (the step's chain)
-void launch_ibm_substitution(const DevState& d, cudaStream_t st);
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st);
 constexpr int IBM_PANEL = 8;            // columns per factorisation panel
 constexpr int IBM_MAX_BANDWIDTH = 160;  // staged panel rows and pair table stay within shared memory
 // Banded storage of a wing's G: row p holds G(p, p - dd) at dd = 0..bw.
@@ -89,7 +85,7 @@ void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle +=
 enum MultiKernel : int {
     MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
     MK_RHS, MK_SPREAD, MK_FINISH,                                      // immersed boundary
-    MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_PANELS, MK_SOLVE,   // banded solver
+    MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
     MK_BULK1, MK_BULK2, MK_BULK4, MK_BC,   // lattice (bulk: 1, 2 or 4 node runs per block)
     MK_KINDS
 };

@@ -112,11 +112,32 @@ def test_batch_rejects_bad_input(gpu_lib):
         _same(before, s.f())
 
 
-def test_inverse_of_a_wing_too_large_for_shared_memory(gpu_lib, oracle_lib):
+def test_streamed_substitution_matches_whole_factor(gpu_lib):
+    """The substitution streaming each wing's factor through a ring of rows
+    in shared memory (the form wings too large for shared memory take) gives
+    the same bits as the substitution on the whole factor; run alone and
+    packed."""
+    ep = small("s", 2, (5.0, 2.5), markers=160)
+    ref = api.Simulation(ep, api.PRECISION_FP32)
+    st = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
+    st2 = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
+    try:
+        rows_ref = ref.step(12)
+        _same(rows_ref, st.step(12))
+        _same(ref.f(), st.f())
+        with api.Batch(0) as batch:
+            _same(rows_ref, batch.step([st2], 12)[0])
+        _same(ref.f(), st2.f())
+    finally:
+        for s_ in (ref, st, st2):
+            s_.close()
+
+
+def test_wing_too_large_for_shared_memory_matches_oracle(gpu_lib, oracle_lib):
     """A 500-marker wing, whose banded factor does not fit in shared memory
-    (the inverse kernel then reads it from global memory): the FP64 path
-    against the oracle's dense LU (1e-9 relative on forces, no-slip residual
-    at solver tolerance), and the FP32 path the same bits alone and packed."""
+    whole (the substitution streams it through a ring of rows): the FP64
+    path against the oracle's dense LU (1e-9 relative on forces, no-slip
+    residual at solver tolerance)."""
     ep = wl.tandem_pitch_heave("big_wing", 2.4, 1.2, 0.004, 100.0, -0.4, 0.0, 500, 6, n_wings=1,
                                pitch_deg=5.0, heave=0.05, freq=2.0)
     o = oracle_lib.Oracle(ep)
@@ -126,16 +147,6 @@ def test_inverse_of_a_wing_too_large_for_shared_memory(gpu_lib, oracle_lib):
         assert s.ibm_residual() < 1e-10
     err = np.abs(r64[:, 1:4] - ro[:, 1:4]).max() / np.abs(ro[:, 1:4]).max()
     assert err < 1e-9, err
-    ref = api.Simulation(ep, api.PRECISION_FP32)
-    pk = api.Simulation(ep, api.PRECISION_FP32)
-    try:
-        rows_ref = ref.step(6)
-        with api.Batch(0) as batch:
-            _same(rows_ref, batch.step([pk], 6)[0])
-        _same(ref.f(), pk.f())
-    finally:
-        ref.close()
-        pk.close()
 
 
 def test_batch_graph_replay_equals_one_at_a_time(gpu_lib):
