@@ -1025,6 +1025,7 @@ int lbm_set_motion_table(LbmHandle* h, const double* rows, int64_t nrows, int32_
     }
     if (dalloc(h, &h->d_step_table, st.size())) return -1;
     CK(cudaMemcpy(h->d_step_table, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(nullptr));   // the copy lands before any step on the handle's streams
     h->d.step_table = h->d_step_table;
     h->geo_ready = -1;
     drop_graphs(h);
@@ -1495,8 +1496,13 @@ void lbm_batch_destroy(LbmBatch* b) {
 int lbm_get_sums(LbmHandle* h, double* sum_row, int32_t* sample_count, int32_t* row_len) {
     if (!h) return -1;
     CK(cudaSetDevice(h->cfg.device));
-    if (sum_row) CK(cudaMemcpy(sum_row, h->d.sum_row, sizeof(double) * h->row_len, cudaMemcpyDeviceToHost));
-    if (sample_count) CK(cudaMemcpy(sample_count, h->d.sample_count, sizeof(int), cudaMemcpyDeviceToHost));
+    // on the handle's stream: ordered after its steps (its streams do not
+    // synchronise with the legacy default stream)
+    if (sum_row)
+        CK(cudaMemcpyAsync(sum_row, h->d.sum_row, sizeof(double) * h->row_len, cudaMemcpyDeviceToHost, h->s_main));
+    if (sample_count)
+        CK(cudaMemcpyAsync(sample_count, h->d.sample_count, sizeof(int), cudaMemcpyDeviceToHost, h->s_main));
+    CK(cudaStreamSynchronize(h->s_main));
     if (row_len) *row_len = h->row_len;
     return 0;
 }
@@ -1504,8 +1510,10 @@ int lbm_get_sums(LbmHandle* h, double* sum_row, int32_t* sample_count, int32_t* 
 int lbm_reset_sums(LbmHandle* h) {
     if (!h) return -1;
     CK(cudaSetDevice(h->cfg.device));
-    CK(cudaMemset(h->d.sum_row, 0, sizeof(double) * h->row_len));
-    CK(cudaMemset(h->d.sample_count, 0, sizeof(int)));
+    // on the handle's stream, so the next step's force row is added after
+    // the clear
+    CK(cudaMemsetAsync(h->d.sum_row, 0, sizeof(double) * h->row_len, h->s_main));
+    CK(cudaMemsetAsync(h->d.sample_count, 0, sizeof(int), h->s_main));
     return 0;
 }
 
@@ -1622,13 +1630,14 @@ int lbm_set_f(LbmHandle* h, const double* f) {
     const size_t nn = (size_t)d.nx * d.ny;
     if (d.precision == 0) {
         for (int k = 0; k < 9; ++k)
-            CK(cudaMemcpy2D(d.f + k * d.plane, sizeof(double) * d.pitch, f + k * nn, sizeof(double) * d.nx,
-                            sizeof(double) * d.nx, d.ny, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy2DAsync(d.f + k * d.plane, sizeof(double) * d.pitch, f + k * nn, sizeof(double) * d.nx,
+                                 sizeof(double) * d.nx, d.ny, cudaMemcpyHostToDevice, h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
         return 0;
     }
     double* tmp = nullptr;
     CK(cudaMalloc((void**)&tmp, 9 * nn * sizeof(double)));
-    cudaError_t e = cudaMemcpy(tmp, f, 9 * nn * sizeof(double), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(tmp, f, 9 * nn * sizeof(double), cudaMemcpyHostToDevice, h->s_main);
     if (e == cudaSuccess) {
         launch_fused_import(d, tmp, d.gA, h->s_main);
         e = cudaStreamSynchronize(h->s_main);
@@ -1720,6 +1729,7 @@ int lbm_set_border_f0(LbmHandle* h, const double* f0, int32_t movenum) {
     CK(cudaSetDevice(h->cfg.device));
     CK(cudaDeviceSynchronize());
     if (f0 && border_f0_copy(h, const_cast<double*>(f0), true)) return -1;
+    CK(cudaDeviceSynchronize());   // the copies land before any step on the handle's streams
     h->d.movenum = movenum;
     h->geo_ready = -1;
     drop_graphs(h);   // movenum is baked into the step graphs
@@ -1758,8 +1768,10 @@ int lbm_status(LbmHandle* h, int32_t* bits) {
     if (!h || !bits) return -1;
     CK(cudaSetDevice(h->cfg.device));
     int st = 0;
-    CK(cudaMemcpy(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemset(h->d.status, 0, sizeof(int)));
+    CK(cudaMemcpyAsync(h->pinned + h->pinned_n - 3, h->d.status, sizeof(int), cudaMemcpyDeviceToHost, h->s_main));
+    CK(cudaMemsetAsync(h->d.status, 0, sizeof(int), h->s_main));
+    CK(cudaStreamSynchronize(h->s_main));
+    std::memcpy(&st, h->pinned + h->pinned_n - 3, sizeof(int));
     *bits = st | h->status_seen;
     h->status_seen = 0;
     return 0;
