@@ -1,5 +1,6 @@
 // Bulk copies between global and shared memory through the tensor memory
-// accelerator's untiled path (cp.async.bulk), completed on an mbarrier.
+// accelerator (untiled cp.async.bulk, and tiled tensor loads), completed on
+// an mbarrier.
 // Addresses must be 16-byte aligned and sizes multiples of 16 bytes.  Every
 // wait is bounded: a copy that does not complete within the limit makes the
 // caller report an error instead of spinning forever.
@@ -38,6 +39,18 @@ __device__ inline void bulk_load_all(void* dst_smem, const void* src, long long 
         const long long n = bytes - o < 65536 ? bytes - o : 65536;
         bulk_load(d + o, s + o, (uint32_t)n, bar);
     }
+}
+
+// Tiled tensor load of one box of a 3-D tensor map (this GPU's memory; no
+// multicast) at coordinates (x, y, z) into shared memory, completed on bar.
+// x times the element size must be a multiple of 16 bytes; dst 128-byte
+// aligned.
+__device__ inline void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // Waits for the barrier phase with the given parity; false after the limit.

@@ -11,6 +11,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/lbm_mutiwing.h"
 #include "lbm_kernels.h"
 
@@ -196,6 +198,10 @@ struct LbmHandle {
     // CUDA graphs of two consecutive steps, one per starting parity; any
     // change of a pointer or value baked into DevState drops them
     cudaGraphExec_t gexec[2][GEO_SETS] = {};
+    // tensor maps of the two plane copies (fused path), for the tiled bulk
+    // kernel; tmap_ok false keeps the kernel with global pulls
+    CUtensorMap tmap[2];
+    bool tmap_ok = false;
     double* d_out = nullptr;        // strided output fields (SAVE)
     size_t out_cap = 0;   // by starting plane parity and geometry set
     // Continuation state: the cycle the device counters hold after the last
@@ -577,7 +583,7 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         cudaEventRecord(h->ev_ibm, h->s_ibm);
         {
             PhaseMark pm(h, 1, h->s_main);
-            launch_fused_bulk(d, h->fc, fields, h->s_main);
+            launch_fused_bulk(d, h->fc, fields, h->tmap_ok ? &h->tmap[h->parity] : nullptr, h->s_main);
         }
         cudaStreamWaitEvent(h->s_main, h->ev_ibm, 0);
         cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
@@ -988,7 +994,11 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     CK(cudaMallocHost((void**)&h->pinned, sizeof(double) * 4096));
     h->pinned_n = 4096;
-    if (c.precision != LBM_PRECISION_FP64) h->fc = h->d.fc = fused_consts(d);
+    if (c.precision != LBM_PRECISION_FP64) {
+        h->fc = h->d.fc = fused_consts(d);
+        h->tmap_ok = fused_tensor_map(d, h->planes[0], &h->tmap[0]) == 0 &&
+                     fused_tensor_map(d, h->planes[1], &h->tmap[1]) == 0;
+    }
     if (init_state(h)) return -1;
     return 0;
 }

@@ -18,7 +18,13 @@ int err_partial_count();
 
 // fused FP32 path (kernels_fp32.cu)
 FusedConsts fused_consts(const DevState& d);
-void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, cudaStream_t st);
+// tmap (may be null): the CUtensorMap of d.gA's planes (fused_tensor_map);
+// steps that write no fields then stage their pulls through shared memory
+// by tensor loads
+void launch_fused_bulk(const DevState& d, const FusedConsts& c, bool fields, const void* tmap, cudaStream_t st);
+// Tensor map (a 128-byte CUtensorMap written to out) of the nine planes at
+// base, for the tiled bulk kernel; 0 on success.
+int fused_tensor_map(const DevState& d, const float* base, void* out);
 bool is_bulk_kernel(const void* func);   // the bulk kernel (low priority in graphs)
 bool is_far_field_kernel(const void* func);
 void launch_fused_bc(const DevState& d, cudaStream_t st);   // far field of the fused path
