@@ -53,35 +53,6 @@ __device__ inline void tma_load_3d(void* dst, const void* tmap, int x, int y, in
         : "memory");
 }
 
-// An L2 cache policy that evicts the lines it touches first.
-__device__ inline uint64_t l2_evict_first_policy() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-
-// tma_load_3d with an L2 cache policy for the lines it reads.
-__device__ inline void tma_load_3d_hint(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar,
-                                        uint64_t policy) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
-        "[%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar)), "l"(policy)
-        : "memory");
-}
-
-// Read-only global load of one float with an L2 cache policy.
-__device__ inline float ld_hint(const float* p, uint64_t policy) {
-    float v;
-    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(policy));
-    return v;
-}
-
-// Global store of one float with an L2 cache policy.
-__device__ inline void st_hint(float* p, float v, uint64_t policy) {
-    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(policy) : "memory");
-}
-
 // Waits for the barrier phase with the given parity; false after the limit.
 __device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity) {
     for (long long it = 0; it < MBAR_WAIT_LIMIT; ++it) {

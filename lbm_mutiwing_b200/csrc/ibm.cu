@@ -253,60 +253,64 @@ __device__ inline bool box_empty(const DevState& d, int s) {
     return d.box[4 * s + 1] < d.box[4 * s] || d.box[4 * s + 3] < d.box[4 * s + 2];
 }
 
-// move_boundary part 2 (airfoil.f90:322-333), one block per episode: the
-// claims (lowest segment index wins each box node), the slots each segment
-// claimed as a 36-bit mask in shared memory, the coupling test (a box node
-// claimed by a segment of another wing lies in the supports of both wings,
-// so G has entries between them and the wings are solved jointly; the
-// lowest index claims a node, hence every shared node is seen from the
-// higher wing's side), the exclusive scan of the claim counts in segment
-// order, and the band list in the reference's order (segment, then i, then
-// j: slot a * 6 + c is node (i1 + a, j1 + c), so a claimed slot's place is
-// its segment's offset plus the claimed slots before it) with the band_map
-// encoding -(b + 2) and the band bit plane.  Each phase is one pass over
-// the segments' box slots, with block barriers between them instead of
-// kernel boundaries.  The geometry's cycle counter moves on (the motion
-// kernel read it before).
-constexpr int BAND_THREADS = 1024;
-__device__ __forceinline__ void ibm_band_kernel_body(const DevState& d) {
-    extern __shared__ __align__(16) unsigned long long band_sm[];
-    __shared__ int wsum[BAND_THREADS / 32];
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    const int ns = d.nseg, n = ns * BOX_SLOTS;
-    unsigned long long* mask = band_sm;
-    int* offs = reinterpret_cast<int*>(mask + ns);
-    for (int t = tid; t < n; t += nt) {
+// claims: lowest segment index wins (airfoil.f90:322-333)
+__device__ __forceinline__ void ibm_claim_kernel_body(const DevState& d, const int bid_) {
+    const int n = d.nseg * BOX_SLOTS, stride = slot_grid(d) * 256;
+    for (int t = bid_ * 256 + threadIdx.x; t < n; t += stride) {
         const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
         if (box_empty(d, s)) continue;
         const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
         if (i <= d.box[4 * s + 1] && j <= d.box[4 * s + 3]) atomicMin(&d.band_map[pidx(d, i - 1, j - 1)], s);
     }
-    for (int s = tid; s < ns; s += nt) mask[s] = 0ull;
-    __syncthreads();
+}
+__global__ void ibm_claim_kernel(DevState d) { ibm_claim_kernel_body(d, blockIdx.x); }
+__global__ void ibm_claim_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_claim_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
+
+// Claims per segment, and the coupling test: a box node claimed by a
+// segment of another wing lies in the supports of both wings, so G has
+// entries between them and the wings are solved jointly (the lowest segment
+// index claims a node, hence every shared node is seen from the higher
+// wing's side).
+__device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const int bid_) {
+    const int s = bid_ * blockDim.x + threadIdx.x;
+    if (s >= d.nseg) return;
+    int c = 0;
     bool shared = false;
-    for (int t = tid; t < n; t += nt) {
-        const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
-        if (box_empty(d, s)) continue;
-        const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
-        if (i > d.box[4 * s + 1] || j > d.box[4 * s + 3]) continue;
-        const int bm = __ldcg(&d.band_map[pidx(d, i - 1, j - 1)]);
-        if (bm == s)
-            atomicOr(&mask[s], 1ull << slot);
-        else
-            shared |= bm >= 0 && bm < ns && d.seg_wing[bm] != d.seg_wing[s];
+    if (!box_empty(d, s)) {
+        const int w = d.seg_wing[s];
+        for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
+            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
+                const int bm = d.band_map[pidx(d, i - 1, j - 1)];
+                c += (bm == s);
+                shared |= bm != s && bm >= 0 && bm < d.nseg && d.seg_wing[bm] != w;
+            }
     }
-    if (__syncthreads_or(shared) && tid == 0) {
+    d.claim_cnt[s] = c;
+    if (shared) {
         d.ibm_flags[0] = 1;
         set_status(d, ST_WINGS_COUPLED);
     }
-    // exclusive scan of the claim counts: a chunk of segments per thread
-    const int per = (ns + nt - 1) / nt;
-    const int lo = min(ns, tid * per), hi = min(ns, lo + per);
+}
+__global__ void ibm_count_kernel(DevState d) { ibm_count_kernel_body(d, blockIdx.x); }
+__global__ void ibm_count_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_count_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
+
+// Exclusive scan of the claim counts (one block) and the band size.
+__device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const int bid_) {
+    __shared__ int wsum[32];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (d.nseg + nt - 1) / nt;
+    const int lo = min(d.nseg, tid * per), hi = min(d.nseg, lo + per);
     int lsum = 0;
-    for (int s = lo; s < hi; ++s) lsum += __popcll(mask[s]);
+    for (int s = lo; s < hi; ++s) lsum += d.claim_cnt[s];
     int x = lsum;
     for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        int y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) wsum[warp] = x;
@@ -318,43 +322,54 @@ __device__ __forceinline__ void ibm_band_kernel_body(const DevState& d) {
     }
     int run = base + x - lsum;
     for (int s = lo; s < hi; ++s) {
-        offs[s] = run;
-        run += __popcll(mask[s]);
+        const int c = d.claim_cnt[s];
+        d.claim_cnt[s] = run;
+        run += c;
     }
     __syncthreads();
-    const int nb = min(tot, d.band_cap);
     if (tid == 0) {
+        const int nb = min(tot, d.band_cap);
         if (tot > d.band_cap) set_status(d, ST_BAND_OVERFLOW);
         d.band_n[0] = nb;
+        d.claim_cnt[d.nseg] = nb;
     }
-    for (int t = tid; t < n; t += nt) {
-        const int s = t / BOX_SLOTS, slot = t % BOX_SLOTS;
-        const unsigned long long m = mask[s];
-        if (!((m >> slot) & 1ull)) continue;
-        const int b = offs[s] + __popcll(m & ((1ull << slot) - 1ull));
-        if (b >= nb) continue;
-        const int i = d.box[4 * s] + slot / 6, j = d.box[4 * s + 2] + slot % 6;
-        const long long p = pidx(d, i - 1, j - 1);
-        d.band_ij[2 * b] = i - 1;
-        d.band_ij[2 * b + 1] = j - 1;
-        d.band_wing[b] = d.seg_wing[s];
-        d.band_claimer[b] = s;
-        d.band_map[p] = -(b + 2);
-        if (d.band_bits) atomicOr(d.band_bits + (p >> 5), 1u << (p & 31));
-    }
-    if (tid == 0) *d.gcycle += 1;
 }
-__global__ void __launch_bounds__(BAND_THREADS) ibm_band_kernel(DevState d) { ibm_band_kernel_body(d); }
-__global__ void __launch_bounds__(BAND_THREADS) ibm_band_kernel_multi(MultiArgs m) {
-    ibm_band_kernel_body(*m.ds[multi_episode(m, blockIdx.x)]);
+__global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) { ibm_scan_kernel_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(1024) ibm_scan_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_scan_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
-size_t ibm_band_smem(int nseg) { return (size_t)nseg * 8 + ((size_t)nseg + 1) * 4; }
-cudaError_t ibm_band_prepare(size_t smem) {
-    if (smem <= 48 * 1024) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(ibm_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ibm_band_kernel_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return e;
+
+// Band list in the reference's order (segment, then i, then j) and the
+// band_map encoding -(b + 2); a node still holding its claimer's index is
+// never confused with another segment's index, so encoding as we go is safe.
+// The geometry's cycle counter moves on (the motion kernel read it before).
+__device__ __forceinline__ void ibm_list_kernel_body(const DevState& d, const int bid_) {
+    const int s = bid_ * blockDim.x + threadIdx.x;
+    if (s == 0) *d.gcycle += 1;
+    if (s >= d.nseg || box_empty(d, s)) return;
+    const int nb = d.band_n[0];
+    const int w = d.seg_wing[s];
+    int b = d.claim_cnt[s];
+    for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
+        for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
+            const long long p = pidx(d, i - 1, j - 1);
+            if (d.band_map[p] != s) continue;
+            if (b < nb) {
+                d.band_ij[2 * b] = i - 1;
+                d.band_ij[2 * b + 1] = j - 1;
+                d.band_wing[b] = w;
+                d.band_claimer[b] = s;
+                d.band_map[p] = -(b + 2);
+                if (d.band_bits) atomicOr(d.band_bits + (p >> 5), 1u << (p & 31));
+            }
+            ++b;
+        }
+}
+__global__ void ibm_list_kernel(DevState d) { ibm_list_kernel_body(d, blockIdx.x); }
+__global__ void ibm_list_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_list_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
 // Plain path: u*, rho at band nodes from the moment fields
@@ -896,15 +911,19 @@ int ibm_finish_blocks(const DevState& d) { return blocks(d.band_cap, FINISH_THRE
 
 bool is_geometry_multi_kernel(const void* func) {
     for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel_multi),
-                          reinterpret_cast<const void*>(ibm_band_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_claim_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_count_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_scan_kernel_multi),
+                          reinterpret_cast<const void*>(ibm_list_kernel_multi),
                           reinterpret_cast<const void*>(ibm_assemble_kernel_multi)})
         if (func == k) return true;
     return is_factor_multi_kernel(func);
 }
 
 bool is_geometry_kernel(const void* func) {
-    for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel), reinterpret_cast<const void*>(ibm_band_kernel),
-                          reinterpret_cast<const void*>(ibm_assemble_kernel)})
+    for (const void* k : {reinterpret_cast<const void*>(ibm_geometry_kernel), reinterpret_cast<const void*>(ibm_claim_kernel),
+                          reinterpret_cast<const void*>(ibm_count_kernel), reinterpret_cast<const void*>(ibm_scan_kernel),
+                          reinterpret_cast<const void*>(ibm_list_kernel), reinterpret_cast<const void*>(ibm_assemble_kernel)})
         if (func == k) return true;
     return is_factor_kernel(func);
 }
@@ -912,7 +931,10 @@ bool is_geometry_kernel(const void* func) {
 void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_done) {
     ibm_geometry_kernel<<<geometry_grid(d), 128, 0, st>>>(d);
     if (geometry_done) cudaEventRecord(geometry_done, st);
-    ibm_band_kernel<<<1, BAND_THREADS, ibm_band_smem(d.nseg), st>>>(d);
+    ibm_claim_kernel<<<slot_grid(d), 256, 0, st>>>(d);
+    ibm_count_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
+    ibm_scan_kernel<<<1, 1024, 0, st>>>(d);
+    ibm_list_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
 }
 
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
@@ -953,7 +975,10 @@ void launch_step_advance(const DevState& d, cudaStream_t st) { step_advance_kern
 int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_GEOMETRY: return geometry_grid(d);
-    case MK_BAND: return 1;
+    case MK_CLAIM: return slot_grid(d);
+    case MK_COUNT: return blocks(d.nseg, 64);
+    case MK_SCAN: return 1;
+    case MK_LIST: return blocks(d.nseg, 64);
     case MK_ASSEMBLE: return assemble_grid(d);
     case MK_RHS: return rhs_grid(d);
     case MK_SPREAD: return slot_grid(d);
@@ -962,10 +987,13 @@ int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     }
 }
 
-bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, size_t smem, cudaStream_t st) {
+bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st) {
     switch (k) {
     case MK_GEOMETRY: ibm_geometry_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
-    case MK_BAND: ibm_band_kernel_multi<<<nb, BAND_THREADS, smem, st>>>(m); return true;
+    case MK_CLAIM: ibm_claim_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
+    case MK_COUNT: ibm_count_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
+    case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
+    case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
     case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
     case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;

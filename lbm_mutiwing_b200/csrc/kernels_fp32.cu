@@ -99,7 +99,6 @@ __device__ __forceinline__ void fused_collide(const float g[9], const FusedConst
 // re-collision, which runs concurrently and writes them.  EARLY: the band
 // bit is tested before the nine pulls (one memory round trip ahead of
 // them); otherwise it is loaded beside them and only gates the stores.
-// Pulls and stores carry the L2 evict-first policy (see the tiled form).
 #ifndef BULK_EARLY_BAND_TEST
 #define BULK_EARLY_BAND_TEST 1
 #endif
@@ -107,18 +106,17 @@ template <bool FIELDS, bool EARLY>
 __device__ __forceinline__ void fused_bulk_node(const float* __restrict__ gA, float* __restrict__ gB, int pitch,
                                                 long long plane, const FusedConsts& c, double* __restrict__ fo_rho,
                                                 double* __restrict__ fo_u, double* __restrict__ fo_v,
-                                                const unsigned* __restrict__ bits, int i, int j,
-                                                uint64_t policy) {
+                                                const unsigned* __restrict__ bits, int i, int j) {
     const long long p = (long long)j * pitch + i;
     const unsigned word = __ldg(bits + (p >> 5));
     if (EARLY && ((word >> (p & 31)) & 1u)) return;
     float g[9], o[9], drho, jx, jy;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) g[k] = ld_hint(gA + k * plane + p - ex(k) - (long long)ey(k) * pitch, policy);
+    for (int k = 0; k < 9; ++k) g[k] = __ldg(gA + k * plane + p - ex(k) - (long long)ey(k) * pitch);
     fused_collide(g, c, o, drho, jx, jy);
     if (!EARLY && ((word >> (p & 31)) & 1u)) return;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) st_hint(gB + k * plane + p, o[k], policy);
+    for (int k = 0; k < 9; ++k) gB[k * plane + p] = o[k];
     if (FIELDS) {
         const double rho = 1.0 + (double)drho;
         fo_rho[p] = rho;
@@ -139,8 +137,7 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
     for (int r = 0; r < BULK_ROWS; ++r) {
         const int j = j0 + r;
         if (j > ny - 2) break;
-        fused_bulk_node<FIELDS, BULK_EARLY_BAND_TEST != 0>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j,
-                                                           l2_evict_first_policy());
+        fused_bulk_node<FIELDS, BULK_EARLY_BAND_TEST != 0>(gA, gB, pitch, plane, c, fo_rho, fo_u, fo_v, bits, i, j);
     }
 }
 // Tiled form of the common step (no fields written): a block takes the
@@ -151,12 +148,7 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
 // and box column cc + 4 - ex(k) the pull of column 128 tx + cc.  The 136
 // columns cover the +-1 shifts; the tiles either side share 8 columns (L2
 // hits).  Every value is then read once from shared memory, collided and
-// stored to the next planes.  The loads and stores carry an L2 evict-first
-// policy: the 1.15 GB a step streams through the 126 MB L2 then leaves the
-// immersed-boundary chain's and the geometry's working sets (band maps,
-// factors, marker arrays) resident, so those latency-bound kernels, which
-// run beside this one, do not wait on a saturated DRAM.  Blocks stay
-// short-lived (no persistent loop),
+// stored to the next planes.  Blocks stay short-lived (no persistent loop),
 // so the immersed-boundary chain's blocks, at higher priority, are
 // dispatched as bulk blocks retire.  Measured alone at 4001 x 2001: 96.7 us
 // against 103.2 us for the one-node-per-thread form with global pulls.
@@ -174,12 +166,11 @@ __global__ void __launch_bounds__(TMA_THREADS) fused_bulk_tma_kernel(const __gri
     float* S = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(tma_raw) + 127) & ~(uintptr_t)127);
     const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
     const int x0 = tx * TMA_TX, y0 = 1 + ty * TMA_TY;
-    const uint64_t policy = l2_evict_first_policy();
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         mbar_arrive_expect_tx(&bar, (uint32_t)(9 * TMA_TY * TMA_BOXW * sizeof(float)));
 #pragma unroll
-        for (int k = 0; k < 9; ++k) tma_load_3d_hint(S + k * TMA_CH, &tm, x0 - 4, y0 - ey(k), k, &bar, policy);
+        for (int k = 0; k < 9; ++k) tma_load_3d(S + k * TMA_CH, &tm, x0 - 4, y0 - ey(k), k, &bar);
     }
     __syncthreads();
     const bool ok = mbar_wait(&bar, 0);
@@ -199,7 +190,7 @@ __global__ void __launch_bounds__(TMA_THREADS) fused_bulk_tma_kernel(const __gri
         for (int k = 0; k < 9; ++k) g[k] = S[k * TMA_CH + r * TMA_BOXW + cc + 4 - ex(k)];
         fused_collide(g, c, o, drho, jx, jy);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) st_hint(gB + k * plane + p, o[k], policy);
+        for (int k = 0; k < 9; ++k) gB[k * plane + p] = o[k];
     }
 }
 
@@ -250,7 +241,7 @@ __device__ __forceinline__ void fused_bulk_runs(const BulkArgs& a) {
         if (t >= a.n) break;
         const int jj = t / a.w;
         fused_bulk_node<FIELDS, false>(a.gA, a.gB, a.pitch, a.plane, a.c, a.fo_rho, a.fo_u, a.fo_v, a.bits,
-                                       t - jj * a.w + 1, jj + 1, l2_evict_first_policy());
+                                       t - jj * a.w + 1, jj + 1);
     }
 }
 template <int RUNS>

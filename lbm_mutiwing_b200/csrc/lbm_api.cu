@@ -122,7 +122,7 @@ constexpr int GRAPH_STEPS = 2;
 struct GeoSet {
     WingMotion* wm = nullptr;
     double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
-    int *box = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
+    int *box = nullptr, *claim_cnt = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
     int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
     unsigned* band_bits = nullptr;
     double *lband = nullptr, *linv = nullptr;
@@ -131,7 +131,7 @@ struct GeoSet {
 static GeoSet geo_of(const DevState& d) {
     GeoSet g;
     g.wm = d.wm; g.xb1 = d.xb1; g.yb1 = d.yb1; g.xb2 = d.xb2; g.yb2 = d.yb2; g.kx = d.kx; g.ky = d.ky;
-    g.box = d.box; g.pb = d.pb; g.band_claimer = d.band_claimer;
+    g.box = d.box; g.claim_cnt = d.claim_cnt; g.pb = d.pb; g.band_claimer = d.band_claimer;
     g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
     g.band_bits = d.band_bits;
     g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv;
@@ -140,7 +140,7 @@ static GeoSet geo_of(const DevState& d) {
 
 static void use_geo(DevState& d, const GeoSet& g) {
     d.wm = g.wm; d.xb1 = g.xb1; d.yb1 = g.yb1; d.xb2 = g.xb2; d.yb2 = g.yb2; d.kx = g.kx; d.ky = g.ky;
-    d.box = g.box; d.pb = g.pb; d.band_claimer = g.band_claimer;
+    d.box = g.box; d.claim_cnt = g.claim_cnt; d.pb = g.pb; d.band_claimer = g.band_claimer;
     d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
     d.band_bits = g.band_bits;
     d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv;
@@ -887,7 +887,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
         dalloc(h, &xb0, npz) || dalloc(h, &yb0, npz) || dalloc(h, &d.xb1, npz) || dalloc(h, &d.yb1, npz) ||
         dalloc(h, &d.xb2, nsz) || dalloc(h, &d.yb2, nsz) || dalloc(h, &d.box, 4 * nsz) ||
-        dalloc(h, &d.kx, 6 * nsz) || dalloc(h, &d.ky, 6 * nsz) ||
+        dalloc(h, &d.claim_cnt, nsz + 1) || dalloc(h, &d.kx, 6 * nsz) || dalloc(h, &d.ky, 6 * nsz) ||
         dalloc(h, &d.pb, nsz * BOX_SLOTS) || dalloc(h, &drpos, nsz) || dalloc(h, &d.band_claimer, (size_t)cap) ||
         dalloc(h, &d.rx, nsz) || dalloc(h, &d.ry, nsz) || dalloc(h, &d.qx, nsz) || dalloc(h, &d.qy, nsz) ||
         dalloc(h, &d.cg_work, 8 * nsz) || dalloc(h, &d.solve_count, 1) ||
@@ -949,8 +949,6 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
                      ibm_solve_smem(nwmax, bwmax, wmax, false) + ibm_solve_ring_bytes(bwmax) <= smem_cap;
     if (d.solve_stream) d.solve_smem += (long long)ibm_solve_ring_bytes(bwmax);
     CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
-    if (ibm_band_smem(ns) > smem_cap) return fail(h, "immersed boundary: too many segments for the band kernel");
-    CK(ibm_band_prepare(ibm_band_smem(ns)));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
         return -1;
@@ -961,7 +959,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         GeoSet& g = h->geo[s];
         if (dalloc(h, &g.wm, wz) || dalloc(h, &g.xb1, npz) || dalloc(h, &g.yb1, npz) || dalloc(h, &g.xb2, nsz) ||
             dalloc(h, &g.yb2, nsz) || dalloc(h, &g.kx, 6 * nsz) || dalloc(h, &g.ky, 6 * nsz) ||
-            dalloc(h, &g.box, 4 * nsz) || dalloc(h, &g.pb, nsz * BOX_SLOTS) ||
+            dalloc(h, &g.box, 4 * nsz) || dalloc(h, &g.claim_cnt, nsz + 1) || dalloc(h, &g.pb, nsz * BOX_SLOTS) ||
             dalloc(h, &g.band_claimer, (size_t)cap) || dalloc(h, &g.band_n, 2) ||
             dalloc(h, &g.band_ij, 2 * (size_t)cap) || dalloc(h, &g.band_wing, cap) || dalloc(h, &g.band_map, N) ||
             dalloc(h, &g.band_bits, band_bits_words(d)) ||
@@ -1245,7 +1243,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     };
     // block offsets of every packed kernel, in episode order
     std::vector<int> boff((size_t)MK_KINDS * (nh + 1), 0);
-    size_t factor_smem = 0, solve_smem = 0, band_smem = 0;
+    size_t factor_smem = 0, solve_smem = 0;
     for (int k = 0; k < MK_KINDS; ++k)
         for (int e = 0; e < nh; ++e) {
             const long long nb = (long long)boff[(size_t)k * (nh + 1) + e] +
@@ -1256,7 +1254,6 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     for (int e = 0; e < nh; ++e) {
         factor_smem = std::max(factor_smem, hs[order[e]]->factor_smem);
         solve_smem = std::max(solve_smem, (size_t)hs[order[e]]->d.solve_smem);
-        band_smem = std::max(band_smem, ibm_band_smem(hs[order[e]]->d.nseg));
     }
     // state-pointer tables of every step (variant indices, reused from two
     // steps earlier while the episode set and flags are unchanged)
@@ -1333,13 +1330,12 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         if (nb <= 0) return;
         MultiArgs m{reinterpret_cast<const DevState* const*>(b->d_buf + off_ptr) + at, bo, ne};
         const size_t smem = (k == MK_FACTOR_SMEM || k == MK_FACTOR_GLOBAL) ? factor_smem : solve_smem;
-        if (!launch_multi_ibm(k, m, nb, k == MK_BAND ? band_smem : smem, st) && !launch_multi_solver(k, m, nb, smem, st))
-            launch_multi_fused(k, m, nb, st);
+        if (!launch_multi_ibm(k, m, nb, st) && !launch_multi_solver(k, m, nb, smem, st)) launch_multi_fused(k, m, nb, st);
     };
     auto geometry = [&](size_t at, int ne, cudaStream_t sa, cudaStream_t sb, bool events) {
         launch(MK_GEOMETRY, at, ne, sa);
         if (events) cudaEventRecord(b->ev_geom, sa);
-        launch(MK_BAND, at, ne, sa);
+        for (MultiKernel k : {MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST}) launch(k, at, ne, sa);
         if (events) {
             cudaEventRecord(b->ev_list, sa);
             cudaStreamWaitEvent(sb, b->ev_geom, 0);

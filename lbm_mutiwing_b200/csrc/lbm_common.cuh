@@ -120,6 +120,7 @@ struct DevState {
     const double *xb0, *yb0;     // npts, body frame
     double *xb1, *yb1, *xb2, *yb2;
     int* box;                    // 4 * nseg: i1 i2 j1 j2 (1-based, inclusive)
+    int* claim_cnt;              // nseg + 1: band-list offset of each segment's claims
     double *kx, *ky;             // 6 * nseg: delta values of each box column / row
     int* pb;                     // nseg * 36 band index per slot (-1 outside box)
     int* band_claimer;           // cap: segment that claimed each band node

@@ -89,7 +89,7 @@ void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle +=
 // index b - boff[e] (multi.cuh).  The fused path's kernels only; the bulk
 // and closing kernels take the field flag from each episode's state.
 enum MultiKernel : int {
-    MK_GEOMETRY, MK_BAND, MK_ASSEMBLE,   // geometry of a step
+    MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
     MK_RHS, MK_SPREAD, MK_FINISH,                                      // immersed boundary
     MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
     MK_BULK1, MK_BULK2, MK_BULK4, MK_BC,   // lattice (bulk: 1, 2 or 4 node runs per block)
@@ -105,11 +105,7 @@ struct MultiArgs {
 int multi_blocks_ibm(MultiKernel k, const DevState& d);
 int multi_blocks_solver(MultiKernel k, const DevState& d);
 int multi_blocks_fused(MultiKernel k, const DevState& d);
-bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int blocks, size_t smem, cudaStream_t st);
-// dynamic shared memory of the band kernel for nseg segments, and raising
-// its limit when that exceeds the default
-size_t ibm_band_smem(int nseg);
-cudaError_t ibm_band_prepare(size_t smem);
+bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st);
 bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int blocks, size_t smem, cudaStream_t st);
 bool launch_multi_fused(MultiKernel k, const MultiArgs& m, int blocks, cudaStream_t st);
 bool is_bulk_multi_kernel(const void* func);
