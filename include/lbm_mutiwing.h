@@ -43,8 +43,8 @@ extern "C" {
 
 /* LbmConfig.flags */
 #define LBM_FLAG_NO_GRAPHS 1   /* launch every kernel directly (no CUDA graph replay) */
-#define LBM_FLAG_SOLVE_STREAM 2  /* FP32 path: stream each wing's factor through shared memory in the
-                                    substitution even when it fits whole (same results; for testing) */
+#define LBM_FLAG_SOLVE_STREAM 2  /* stream each wing's factor through shared memory in an 8-row substitution
+                                    even when the wing fits whole or in 32-row panels (for testing) */
 
 /* lbm_step flags */
 #define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */

@@ -273,23 +273,29 @@ __global__ void ibm_claim_kernel_multi(MultiArgs m) {
 // segment of another wing lies in the supports of both wings, so G has
 // entries between them and the wings are solved jointly (the lowest segment
 // index claims a node, hence every shared node is seen from the higher
-// wing's side).
+// wing's side).  One warp per segment, a box slot per lane: every node's
+// claimer is loaded at once and counted by a ballot.
 __device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const int bid_) {
-    const int s = bid_ * blockDim.x + threadIdx.x;
+    const int s = (bid_ * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (s >= d.nseg) return;
     int c = 0;
     bool shared = false;
     if (!box_empty(d, s)) {
         const int w = d.seg_wing[s];
-        for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
-            for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
+        const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
+        for (int slot0 = 0; slot0 < BOX_SLOTS; slot0 += 32) {
+            const int slot = slot0 + lane, i = i1 + slot / 6, j = j1 + slot % 6;
+            bool mine = false;
+            if (slot < BOX_SLOTS && i <= i2 && j <= j2) {
                 const int bm = d.band_map[pidx(d, i - 1, j - 1)];
-                c += (bm == s);
+                mine = bm == s;
                 shared |= bm != s && bm >= 0 && bm < d.nseg && d.seg_wing[bm] != w;
             }
+            c += __popc(__ballot_sync(0xffffffffu, mine));
+        }
     }
-    d.claim_cnt[s] = c;
-    if (shared) {
+    if (lane == 0) d.claim_cnt[s] = c;
+    if (__any_sync(0xffffffffu, shared) && lane == 0) {
         d.ibm_flags[0] = 1;
         set_status(d, ST_WINGS_COUPLED);
     }
@@ -343,28 +349,38 @@ __global__ void __launch_bounds__(1024) ibm_scan_kernel_multi(MultiArgs m) {
 // Band list in the reference's order (segment, then i, then j) and the
 // band_map encoding -(b + 2); a node still holding its claimer's index is
 // never confused with another segment's index, so encoding as we go is safe.
-// The geometry's cycle counter moves on (the motion kernel read it before).
+// One warp per segment, a box slot per lane: slot a * 6 + c is node
+// (i1 + a, j1 + c), so a claimed slot's place is its segment's offset plus
+// the claimed slots before it (a ballot prefix).  The geometry's cycle
+// counter moves on (the motion kernel read it before).
 __device__ __forceinline__ void ibm_list_kernel_body(const DevState& d, const int bid_) {
-    const int s = bid_ * blockDim.x + threadIdx.x;
-    if (s == 0) *d.gcycle += 1;
+    const int s = (bid_ * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (s == 0 && lane == 0) *d.gcycle += 1;
     if (s >= d.nseg || box_empty(d, s)) return;
     const int nb = d.band_n[0];
     const int w = d.seg_wing[s];
+    const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
     int b = d.claim_cnt[s];
-    for (int i = d.box[4 * s]; i <= d.box[4 * s + 1]; ++i)
-        for (int j = d.box[4 * s + 2]; j <= d.box[4 * s + 3]; ++j) {
-            const long long p = pidx(d, i - 1, j - 1);
-            if (d.band_map[p] != s) continue;
-            if (b < nb) {
-                d.band_ij[2 * b] = i - 1;
-                d.band_ij[2 * b + 1] = j - 1;
-                d.band_wing[b] = w;
-                d.band_claimer[b] = s;
-                d.band_map[p] = -(b + 2);
-                if (d.band_bits) atomicOr(d.band_bits + (p >> 5), 1u << (p & 31));
-            }
-            ++b;
+    for (int slot0 = 0; slot0 < BOX_SLOTS; slot0 += 32) {
+        const int slot = slot0 + lane, i = i1 + slot / 6, j = j1 + slot % 6;
+        long long p = 0;
+        bool mine = false;
+        if (slot < BOX_SLOTS && i <= i2 && j <= j2) {
+            p = pidx(d, i - 1, j - 1);
+            mine = d.band_map[p] == s;
         }
+        const unsigned ball = __ballot_sync(0xffffffffu, mine);
+        const int bi = b + __popc(ball & ((1u << lane) - 1u));
+        if (mine && bi < nb) {
+            d.band_ij[2 * bi] = i - 1;
+            d.band_ij[2 * bi + 1] = j - 1;
+            d.band_wing[bi] = w;
+            d.band_claimer[bi] = s;
+            d.band_map[p] = -(bi + 2);
+            if (d.band_bits) atomicOr(d.band_bits + (p >> 5), 1u << (p & 31));
+        }
+        b += __popc(ball);
+    }
 }
 __global__ void ibm_list_kernel(DevState d) { ibm_list_kernel_body(d, blockIdx.x); }
 __global__ void ibm_list_kernel_multi(MultiArgs m) {
@@ -932,9 +948,9 @@ void launch_ibm_band(const DevState& d, cudaStream_t st, cudaEvent_t geometry_do
     ibm_geometry_kernel<<<geometry_grid(d), 128, 0, st>>>(d);
     if (geometry_done) cudaEventRecord(geometry_done, st);
     ibm_claim_kernel<<<slot_grid(d), 256, 0, st>>>(d);
-    ibm_count_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
+    ibm_count_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
     ibm_scan_kernel<<<1, 1024, 0, st>>>(d);
-    ibm_list_kernel<<<blocks(d.nseg, 64), 64, 0, st>>>(d);
+    ibm_list_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
 }
 
 void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st) {
@@ -976,9 +992,9 @@ int multi_blocks_ibm(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_GEOMETRY: return geometry_grid(d);
     case MK_CLAIM: return slot_grid(d);
-    case MK_COUNT: return blocks(d.nseg, 64);
+    case MK_COUNT: return blocks(32LL * d.nseg, 128);
     case MK_SCAN: return 1;
-    case MK_LIST: return blocks(d.nseg, 64);
+    case MK_LIST: return blocks(32LL * d.nseg, 128);
     case MK_ASSEMBLE: return assemble_grid(d);
     case MK_RHS: return rhs_grid(d);
     case MK_SPREAD: return slot_grid(d);
@@ -991,9 +1007,9 @@ bool launch_multi_ibm(MultiKernel k, const MultiArgs& m, int nb, cudaStream_t st
     switch (k) {
     case MK_GEOMETRY: ibm_geometry_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_CLAIM: ibm_claim_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
-    case MK_COUNT: ibm_count_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
+    case MK_COUNT: ibm_count_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_SCAN: ibm_scan_kernel_multi<<<nb, 1024, 0, st>>>(m); return true;
-    case MK_LIST: ibm_list_kernel_multi<<<nb, 64, 0, st>>>(m); return true;
+    case MK_LIST: ibm_list_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_ASSEMBLE: ibm_assemble_kernel_multi<<<nb, 256, 0, st>>>(m); return true;
     case MK_RHS: ibm_rhs_fused_kernel_multi<<<nb, 128, 0, st>>>(m); return true;
     case MK_SPREAD: ibm_spread_kernel_multi<<<nb, 256, 0, st>>>(m); return true;

@@ -102,6 +102,71 @@ __device__ inline bool factor_diagonal_block(const double* A, int ld, int k0, in
     return clamped;
 }
 
+// Substitution in panels of Q32 = 32 rows on the step's chain.  Per wing and
+// panel q (rows k0 = 32 q ..), built by the factorisation kernel from the
+// factor it holds: MT, the transposed inverse of the panel's unit lower
+// diagonal block of L' (MT[c][l] = M[l][c], rows padded to 33 doubles);
+// R, the coupling of the bw rows below the panel to the panel's columns
+// (R[rb][c] = L'(k0 + np + rb, k0 + c), padded to 33); and the panel's
+// reciprocal pivots.  Rows past the wing's last segment are identity in M
+// and zero in R and the pivots.
+constexpr int Q32 = 32, Q32P = 33;
+__host__ __device__ inline int qpanels(int nw) { return (nw + Q32 - 1) / Q32; }
+__host__ __device__ inline long long panel32_doubles(int bw) {
+    return ((long long)Q32P * (Q32 + bw) + Q32 + 1) & ~1LL;   // even: 16-byte multiples
+}
+long long ibm_panel32_storage(int nw, int bw) { return qpanels(nw) * panel32_doubles(bw); }
+
+// One warp builds panel q: lane c forms column c of M by block forward
+// substitution over the panel's four factor panels, the entries off the
+// 8 x 8 diagonal blocks from the banded storage A (row 0), the diagonal
+// blocks through their stored inverses in aux.
+__device__ __noinline__ void build_panel32(const double* A, int ld, const double* aux, int nw, int bw, int q,
+                                           double* out, int lane) {
+    const int k0 = q * Q32, np = min(Q32, nw - k0), c = lane;
+    double x[Q32];
+#pragma unroll
+    for (int a8 = 0; a8 < Q32 / PANEL; ++a8) {
+        double sv[PANEL];
+#pragma unroll
+        for (int i = 0; i < PANEL; ++i) {
+            const int r = a8 * PANEL + i;
+            double acc = (r == c) ? 1.0 : 0.0;
+            if (r < np) {
+                const double* row = A + (long long)(k0 + r) * ld;   // entry r - m: column k0 + m
+#pragma unroll
+                for (int m = 0; m < a8 * PANEL; ++m)
+                    if (m >= c && r - m <= bw) acc = acc - row[r - m] * x[m];
+            }
+            sv[i] = acc;
+        }
+        const bool in_wing = a8 * PANEL < np;
+        const double* Li = aux + (long long)(k0 / PANEL + a8) * IBM_PANEL_AUX;
+#pragma unroll
+        for (int i = 0; i < PANEL; ++i) {
+            double v = sv[i];
+            if (in_wing && a8 * PANEL + i < np) {
+                v = 0.0;
+#pragma unroll
+                for (int k = 0; k < PANEL; ++k) v = v + Li[i * PANEL + k] * sv[k];
+            }
+            x[a8 * PANEL + i] = v;
+        }
+    }
+    double* MT = out;
+    double* R = out + Q32P * Q32;
+    double* piv = R + Q32P * bw;
+#pragma unroll
+    for (int l = 0; l < Q32; ++l) MT[c * Q32P + l] = x[l];
+    for (int rb = 0; rb < bw; ++rb) {
+        const int dd = np + rb - c;   // row k0 + np + rb, column k0 + c
+        const int i = k0 + np + rb;
+        R[rb * Q32P + c] = (c < np && dd >= 1 && dd <= bw && i < nw) ? A[(long long)i * ld + dd] : 0.0;
+    }
+    const int k = k0 + lane;
+    piv[lane] = k < nw ? aux[(long long)(k / PANEL) * IBM_PANEL_AUX + PANEL * PANEL + (k % PANEL)] : 0.0;
+}
+
 // Storage (ibm_wing_storage): row p of wing w at S + (p + 1) * ld, entry dd
 // holding column p - dd.  On exit: L'(i, k) for every entry below the
 // diagonal blocks, and per panel the inverse of its unit lower diagonal
@@ -279,6 +344,11 @@ __device__ __forceinline__ void ibm_factor_kernel_body(const DevState& d, const 
         __syncthreads();
     }
     if (clamped) solver_status(d, ST_PIVOT_CLAMPED);
+    if (d.solve32) {
+        __syncthreads();   // the factor, the 8 x 8 inverses and the pivots are complete
+        for (int q = warp; q < qpanels(nw); q += FACTOR_WARPS)
+            build_panel32(A, ld, aux, nw, bw, q, d.lq + d.wing_qofs[w] + (long long)q * panel32_doubles(bw), lane);
+    }
     if (in_smem) {
         fence_async_smem();
         __syncthreads();
@@ -750,6 +820,128 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel_multi(MultiArg
     ibm_solve_kernel_body<SMEM>(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
+// Substitution in panels of 32 rows (wings whose panel data fit in shared
+// memory): one block per wing, warp 0 for the x component, warp 1 for y.
+// The wing's panel data (MT, R, pivots per panel) come in by one bulk copy.
+// Forward, per panel: t = M z_p (lane l: a 32-term dot product over MT's
+// column l), rows below -= R t, z_p = D^-1 t.  Backward, per panel, last
+// first: v = z_p - R^T y_below (lane c pulls the solved rows below), y_p =
+// M^T v.  14 dependent panel steps for a 200-segment wing instead of 50.
+// The right-hand sides and solutions, ymax and the joint solve of coupled
+// wings are as in the 8-row substitution.
+__device__ __forceinline__ void ibm_solve32_body(const DevState& d, const int bid_) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ uint64_t bar;
+    const int w = bid_;
+    const int tid = threadIdx.x, lane = tid & 31, comp = tid >> 5;
+    const int nw = d.wing_npts[w] - 1, bw = d.wing_bw[w], s0 = d.wing_sstart[w];
+    const int nq = qpanels(nw);
+    const long long psz = panel32_doubles(bw);
+    const int zlen = (d.nw_max + Q32 + d.bw_max + 1) & ~1;
+    double* P = sm;
+    double* z = sm + d.q32_doubles_max + comp * zlen;
+    double* tb = sm + d.q32_doubles_max + 2 * zlen + comp * Q32;
+    const long long bytes = (long long)nq * psz * 8;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, (uint32_t)bytes);
+        bulk_load_all(P, d.lq + d.wing_qofs[w], bytes, &bar);
+    }
+    const int* perm = d.perm + s0;
+    double* rr = comp == 0 ? d.rx : d.ry;
+    for (int p = lane; p < nw + Q32 + bw; p += 32) z[p] = p < nw ? rr[perm[p]] : 0.0;
+    __syncthreads();
+    const bool ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) solver_status(d, ST_COPY_TIMEOUT);
+        mbar_wait(&bar, 0);   // let a late copy land before the block exits
+        return;
+    }
+    for (int q = 0; q < nq; ++q) {   // L' D v = r
+        const int k0 = q * Q32, np = min(Q32, nw - k0);
+        const double* MT = P + q * psz;
+        const double* R = MT + Q32P * Q32;
+        const double* piv = R + Q32P * bw;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll
+        for (int c = 0; c < Q32; c += 4) {
+            t0 = t0 + MT[c * Q32P + lane] * z[k0 + c];
+            t1 = t1 + MT[(c + 1) * Q32P + lane] * z[k0 + c + 1];
+            t2 = t2 + MT[(c + 2) * Q32P + lane] * z[k0 + c + 2];
+            t3 = t3 + MT[(c + 3) * Q32P + lane] * z[k0 + c + 3];
+        }
+        const double tl = (t0 + t1) + (t2 + t3);
+        tb[lane] = tl;
+        __syncwarp();
+        for (int rb = lane; rb < bw; rb += 32) {
+            const double* Rr = R + rb * Q32P;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+            for (int c = 0; c < Q32; c += 4) {
+                a0 = a0 + Rr[c] * tb[c];
+                a1 = a1 + Rr[c + 1] * tb[c + 1];
+                a2 = a2 + Rr[c + 2] * tb[c + 2];
+                a3 = a3 + Rr[c + 3] * tb[c + 3];
+            }
+            z[k0 + np + rb] -= (a0 + a1) + (a2 + a3);
+        }
+        z[k0 + lane] = tl * piv[lane];   // zero past the last segment
+        __syncwarp();
+    }
+    for (int q = nq - 1; q >= 0; --q) {   // L'^T y = v
+        const int k0 = q * Q32, np = min(Q32, nw - k0);
+        const double* MT = P + q * psz;
+        const double* R = MT + Q32P * Q32;
+        double a0 = 0.0, a1 = 0.0;
+        int rb = 0;
+        for (; rb + 1 < bw; rb += 2) {
+            a0 = a0 + R[rb * Q32P + lane] * z[k0 + np + rb];
+            a1 = a1 + R[(rb + 1) * Q32P + lane] * z[k0 + np + rb + 1];
+        }
+        if (rb < bw) a0 = a0 + R[rb * Q32P + lane] * z[k0 + np + rb];
+        tb[lane] = z[k0 + lane] - (a0 + a1);
+        __syncwarp();
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+#pragma unroll
+        for (int c = 0; c < Q32; c += 4) {
+            y0 = y0 + MT[lane * Q32P + c] * tb[c];
+            y1 = y1 + MT[lane * Q32P + c + 1] * tb[c + 1];
+            y2 = y2 + MT[lane * Q32P + c + 2] * tb[c + 2];
+            y3 = y3 + MT[lane * Q32P + c + 3] * tb[c + 3];
+        }
+        if (lane < np) z[k0 + lane] = (y0 + y1) + (y2 + y3);
+        __syncwarp();
+    }
+    double ym = 0.0;
+#pragma unroll 4
+    for (int p = lane; p < nw; p += 32) {
+        rr[perm[p]] = z[p];
+        ym = fmax(ym, fabs(z[p]));
+    }
+    for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
+    if (lane == 0) d.ymax[2 * w + comp] = ym;
+    if (d.wing_count > 1 && __ldcg(d.ibm_flags) != 0) {
+        __shared__ int last;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) last = atomicAdd(d.solve_count, 1) == d.wing_count - 1;
+        __syncthreads();
+        if (!last) return;
+        __threadfence();
+        if (tid == 0) *d.solve_count = 0;
+        cg_joint_solve(d, z, comp, lane);
+    }
+}
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve32_kernel(DevState d) { ibm_solve32_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve32_kernel_multi(MultiArgs m) {
+    const int e = multi_episode(m, blockIdx.x);
+    ibm_solve32_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
+}
+size_t ibm_solve32_smem(long long q32_doubles_max, int nw_max, int bw_max) {
+    const long long zlen = (nw_max + Q32 + bw_max + 1) & ~1;
+    return (size_t)(q32_doubles_max + 2 * zlen + 2 * Q32) * sizeof(double);
+}
+
 size_t ibm_factor_staging_bytes(int bw_max) {
     const int nt = round_tile(bw_max) / TILE;
     const size_t rows = (size_t)2 * SP * round_tile(bw_max) * sizeof(double);   // a multiple of 16
@@ -795,6 +987,8 @@ cudaError_t ibm_prepare(size_t factor_smem, size_t solve_smem) {
     if (e == cudaSuccess) e = raise_smem_limit(ibm_factor_kernel_multi<false>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<true>, optin);
     if (e == cudaSuccess) e = raise_smem_limit(ibm_solve_kernel_multi<false>, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve32_kernel, optin);
+    if (e == cudaSuccess) e = raise_smem_limit(ibm_solve32_kernel_multi, optin);
     if (e == cudaSuccess && dev < 64) g_prepared_devices |= 1ULL << dev;
     return e;
 }
@@ -819,7 +1013,9 @@ void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_
 
 void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st) {
     if (d.wing_count <= 0) return;
-    if (d.solve_in_smem)
+    if (d.solve32)
+        ibm_solve32_kernel<<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+    else if (d.solve_in_smem)
         ibm_solve_kernel<true><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
     else
         ibm_solve_kernel<false><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
@@ -832,8 +1028,9 @@ int multi_blocks_solver(MultiKernel k, const DevState& d) {
     switch (k) {
     case MK_FACTOR_SMEM: return d.factor_in_smem ? d.wing_count : 0;
     case MK_FACTOR_GLOBAL: return d.factor_in_smem ? 0 : d.wing_count;
-    case MK_SOLVE_SMEM: return d.solve_in_smem ? d.wing_count : 0;
-    case MK_SOLVE_GLOBAL: return d.solve_in_smem ? 0 : d.wing_count;
+    case MK_SOLVE32: return d.solve32 ? d.wing_count : 0;
+    case MK_SOLVE_SMEM: return !d.solve32 && d.solve_in_smem ? d.wing_count : 0;
+    case MK_SOLVE_GLOBAL: return !d.solve32 && !d.solve_in_smem ? d.wing_count : 0;
     default: return -1;
     }
 }
@@ -842,6 +1039,7 @@ bool launch_multi_solver(MultiKernel k, const MultiArgs& m, int nb, size_t smem,
     switch (k) {
     case MK_FACTOR_SMEM: ibm_factor_kernel_multi<true><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
     case MK_FACTOR_GLOBAL: ibm_factor_kernel_multi<false><<<nb, FACTOR_THREADS, smem, st>>>(m); return true;
+    case MK_SOLVE32: ibm_solve32_kernel_multi<<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
     case MK_SOLVE_SMEM: ibm_solve_kernel_multi<true><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
     case MK_SOLVE_GLOBAL: ibm_solve_kernel_multi<false><<<nb, SOLVE_THREADS, smem, st>>>(m); return true;
     default: return false;

@@ -152,7 +152,13 @@ __global__ void __launch_bounds__(BULK_TX) fused_bulk_kernel(const float* __rest
 // so the immersed-boundary chain's blocks, at higher priority, are
 // dispatched as bulk blocks retire.  Measured alone at 4001 x 2001: 96.7 us
 // against 103.2 us for the one-node-per-thread form with global pulls.
-constexpr int TMA_TX = 128, TMA_TY = 4, TMA_THREADS = 256;
+#ifndef LBM_BULK_TILE_ROWS
+#define LBM_BULK_TILE_ROWS 4
+#endif
+#ifndef LBM_BULK_TILE_THREADS
+#define LBM_BULK_TILE_THREADS 256
+#endif
+constexpr int TMA_TX = 128, TMA_TY = LBM_BULK_TILE_ROWS, TMA_THREADS = LBM_BULK_TILE_THREADS;
 constexpr int TMA_BOXW = TMA_TX + 8;
 constexpr int TMA_CH = (TMA_TY * TMA_BOXW + 31) & ~31;   // floats per plane chunk, 128-byte multiple
 constexpr size_t TMA_SMEM = 9 * TMA_CH * sizeof(float) + 128;

@@ -125,7 +125,7 @@ struct GeoSet {
     int *box = nullptr, *claim_cnt = nullptr, *pb = nullptr, *band_claimer = nullptr, *band_n = nullptr;
     int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
     unsigned* band_bits = nullptr;
-    double *lband = nullptr, *linv = nullptr;
+    double *lband = nullptr, *linv = nullptr, *lq = nullptr;
 };
 
 static GeoSet geo_of(const DevState& d) {
@@ -134,7 +134,7 @@ static GeoSet geo_of(const DevState& d) {
     g.box = d.box; g.claim_cnt = d.claim_cnt; g.pb = d.pb; g.band_claimer = d.band_claimer;
     g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
     g.band_bits = d.band_bits;
-    g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv;
+    g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv; g.lq = d.lq;
     return g;
 }
 
@@ -143,7 +143,7 @@ static void use_geo(DevState& d, const GeoSet& g) {
     d.box = g.box; d.claim_cnt = g.claim_cnt; d.pb = g.pb; d.band_claimer = g.band_claimer;
     d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
     d.band_bits = g.band_bits;
-    d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv;
+    d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv; d.lq = g.lq;
 }
 
 struct LbmHandle {
@@ -834,8 +834,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     // RCM order and half bandwidth per wing
     std::vector<int> perm(ns), bw(W), rpos(ns);
-    std::vector<long long> lofs(W), iofs(W);
-    long long ltot = 0, itot = 0;
+    std::vector<long long> lofs(W), iofs(W), qofs(W);
+    long long ltot = 0, itot = 0, qtot = 0, qmax = 0;
     for (int w = 0; w < W; ++w) {
         const int nw = npts[w] - 1;
         std::vector<double> mx(nw), my(nw);
@@ -854,6 +854,9 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         ltot += ibm_wing_storage(nw, bw[w]);
         iofs[w] = itot;
         itot += ibm_linv_storage(nw);
+        qofs[w] = qtot;   // the wing's 32-row panel data
+        qtot += ibm_panel32_storage(nw, bw[w]);
+        qmax = std::max(qmax, ibm_panel32_storage(nw, bw[w]));
     }
 
     // allocations
@@ -881,7 +884,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.band_n = band_n;
     int *pst = nullptr, *sst = nullptr, *npw = nullptr, *sgw = nullptr, *dperm = nullptr, *dbw = nullptr,
         *drpos = nullptr;
-    long long *dlofs = nullptr, *diofs = nullptr;
+    long long *dlofs = nullptr, *diofs = nullptr, *dqofs = nullptr;
     double *xb0 = nullptr, *yb0 = nullptr;
     const size_t nsz = std::max(1, ns), npz = std::max(1, np), wz = std::max(1, W);
     if (dalloc(h, &pst, wz) || dalloc(h, &sst, wz) || dalloc(h, &npw, wz) || dalloc(h, &sgw, nsz) ||
@@ -894,6 +897,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         dalloc(h, &dperm, nsz) || dalloc(h, &dbw, wz) || dalloc(h, &dlofs, wz) ||
         dalloc(h, &d.lband, (size_t)std::max<long long>(1, ltot)) || dalloc(h, &diofs, wz) ||
         dalloc(h, &d.linv, (size_t)std::max<long long>(1, itot)) || dalloc(h, &d.wm, wz) ||
+        dalloc(h, &d.lq, (size_t)std::max<long long>(1, qtot)) || dalloc(h, &dqofs, wz) ||
         dalloc(h, &d.rel_pos, wz) || dalloc(h, &d.cycle, 1) || dalloc(h, &d.row_index, 1) ||
         dalloc(h, &d.gcycle, 1) || dalloc(h, &d.fin_count, 1) ||
         dalloc(h, &d.sum_row, (size_t)h->row_len) || dalloc(h, &d.sample_count, 1) || dalloc(h, &d.status, 1) ||
@@ -913,10 +917,13 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         CK(cudaMemcpy(dbw, bw.data(), W * sizeof(int), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(dlofs, lofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(diofs, iofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dqofs, qofs.data(), W * sizeof(long long), cudaMemcpyHostToDevice));
     }
     d.wing_pstart = pst; d.wing_sstart = sst; d.wing_npts = npw; d.seg_wing = sgw;
     d.xb0 = xb0; d.yb0 = yb0; d.perm = dperm; d.wing_bw = dbw; d.wing_lofs = dlofs; d.rpos = drpos;
     d.wing_linv_ofs = diofs;
+    d.wing_qofs = dqofs;
+    d.q32_doubles_max = qmax;
     h->ppw.assign(npts.begin(), npts.end());
     // dynamic shared memory of the factorisation kernel (one block per wing):
     // [staged panel rows][pair table][the wing's banded factor, if it fits]
@@ -948,6 +955,10 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.solve_stream = !d.solve_in_smem && ibm_solve_ring_fits(bwmax) &&
                      ibm_solve_smem(nwmax, bwmax, wmax, false) + ibm_solve_ring_bytes(bwmax) <= smem_cap;
     if (d.solve_stream) d.solve_smem += (long long)ibm_solve_ring_bytes(bwmax);
+    // substitution in 32-row panels when every wing's panel data fit in
+    // shared memory (the factorisation then also builds them)
+    d.solve32 = W > 0 && !(c.flags & LBM_FLAG_SOLVE_STREAM) && ibm_solve32_smem(qmax, nwmax, bwmax) <= smem_cap;
+    if (d.solve32) d.solve_smem = (long long)ibm_solve32_smem(qmax, nwmax, bwmax);
     CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||
         dalloc(h, &d.force_part, (size_t)ibm_finish_blocks(d) * wz * 3))
@@ -964,7 +975,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             dalloc(h, &g.band_ij, 2 * (size_t)cap) || dalloc(h, &g.band_wing, cap) || dalloc(h, &g.band_map, N) ||
             dalloc(h, &g.band_bits, band_bits_words(d)) ||
             dalloc(h, &g.ibm_flags, 4) || dalloc(h, &g.lband, (size_t)std::max<long long>(1, ltot)) ||
-            dalloc(h, &g.linv, (size_t)std::max<long long>(1, itot)))
+            dalloc(h, &g.linv, (size_t)std::max<long long>(1, itot)) ||
+            dalloc(h, &g.lq, (size_t)std::max<long long>(1, qtot)))
             return -1;
     }
     if (ensure_rows(h, 1024)) return -1;
@@ -996,7 +1008,10 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     h->pinned_n = 4096;
     if (c.precision != LBM_PRECISION_FP64) {
         h->fc = h->d.fc = fused_consts(d);
-        h->tmap_ok = fused_tensor_map(d, h->planes[0], &h->tmap[0]) == 0 &&
+#ifndef LBM_BULK_TILED
+#define LBM_BULK_TILED 1
+#endif
+        h->tmap_ok = LBM_BULK_TILED && fused_tensor_map(d, h->planes[0], &h->tmap[0]) == 0 &&
                      fused_tensor_map(d, h->planes[1], &h->tmap[1]) == 0;
     }
     if (init_state(h)) return -1;
@@ -1370,7 +1385,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         }
         launch(MK_BC, t.cur, t.a_cur, b->s_bc);
         cudaEventRecord(b->ev_bc, b->s_bc);
-        for (MultiKernel k2 : {MK_RHS, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
+        for (MultiKernel k2 : {MK_RHS, MK_SOLVE32, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL, MK_SPREAD, MK_FINISH})
             launch(k2, t.cur, t.a_cur, b->s_ibm);
         cudaEventRecord(b->ev_ibm, b->s_ibm);
         launch((MultiKernel)kind, t.cur, t.a_cur, b->s_bulk);

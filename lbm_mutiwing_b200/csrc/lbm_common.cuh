@@ -147,6 +147,10 @@ struct DevState {
     long long factor_smem_off;   // its byte offset in the factor kernel's shared memory
     double* linv;                // inverses of the factor's diagonal blocks, per wing and panel
     const long long* wing_linv_ofs;  // W offsets into linv
+    int solve32;                 // the substitution runs in 32-row panels from the panel data in lq
+    double* lq;                  // per wing and 32-row panel: MT, R, pivots (built by the factorisation)
+    const long long* wing_qofs;  // W offsets into lq
+    long long q32_doubles_max;   // largest wing's panel data (doubles)
     int solve_in_smem;           // the substitution copies the wing's factor to shared memory
     int solve_stream;            // otherwise it streams the factor through a ring of rows in shared memory
     long long solve_smem;        // dynamic shared memory of the substitution kernel (bytes)

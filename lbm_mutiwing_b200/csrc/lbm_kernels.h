@@ -62,6 +62,10 @@ bool ibm_solve_ring_fits(int bw);
 size_t ibm_factor_staging_bytes(int bw_max);
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st);
 void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st);
+// 32-row panel substitution: doubles of a wing's panel data, and the
+// kernel's dynamic shared memory for the largest wing's panel data
+long long ibm_panel32_storage(int nw, int bw);
+size_t ibm_solve32_smem(long long q32_doubles_max, int nw_max, int bw_max);
 constexpr int IBM_PANEL = 8;            // columns per factorisation panel
 constexpr int IBM_MAX_BANDWIDTH = 160;  // staged panel rows and pair table stay within shared memory
 // Banded storage of a wing's G: row p holds G(p, p - dd) at dd = 0..bw.
@@ -91,7 +95,7 @@ void launch_step_advance(const DevState& d, cudaStream_t st);        // cycle +=
 enum MultiKernel : int {
     MK_GEOMETRY, MK_CLAIM, MK_COUNT, MK_SCAN, MK_LIST, MK_ASSEMBLE,   // geometry of a step
     MK_RHS, MK_SPREAD, MK_FINISH,                                      // immersed boundary
-    MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
+    MK_FACTOR_SMEM, MK_FACTOR_GLOBAL, MK_SOLVE32, MK_SOLVE_SMEM, MK_SOLVE_GLOBAL,  // banded solver
     MK_BULK1, MK_BULK2, MK_BULK4, MK_BC,   // lattice (bulk: 1, 2 or 4 node runs per block)
     MK_KINDS
 };
