@@ -44,7 +44,10 @@ extern "C" {
 /* LbmConfig.flags */
 #define LBM_FLAG_NO_GRAPHS 1   /* launch every kernel directly (no CUDA graph replay) */
 #define LBM_FLAG_SOLVE_STREAM 2  /* stream each wing's factor through shared memory in an 8-row substitution
-                                    even when the wing fits whole or in 32-row panels (for testing) */
+                                    even when the wing fits whole (for testing) */
+#define LBM_FLAG_SOLVE_PANELS32 4  /* substitute in 32-row panels built by the factorisation, where every
+                                      wing's panel data fit in shared memory (fewer dependent steps on the
+                                      step's chain, a longer factorisation) */
 
 /* lbm_step flags */
 #define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */

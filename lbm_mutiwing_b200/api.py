@@ -28,6 +28,7 @@ STEP_FIELDS = 1
 STEP_ERR = 2
 FLAG_NO_GRAPHS = 1
 FLAG_SOLVE_STREAM = 2
+FLAG_SOLVE_PANELS32 = 4
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}
@@ -93,11 +94,13 @@ class LbmError(RuntimeError):
     pass
 
 
-def load_library(path: str = LIB_PATH):
-    """Load the CUDA library; raises if it is absent (no fallback)."""
+def load_library(path: Optional[str] = None):
+    """Load the CUDA library (``path``, else the module's ``LIB_PATH`` at the
+    first call); raises if it is absent (no fallback)."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or LIB_PATH
     if not os.path.exists(path):
         raise LbmError(f"{path} is missing: build it with `python -m lbm_mutiwing_b200.build`")
     lib = C.CDLL(path)

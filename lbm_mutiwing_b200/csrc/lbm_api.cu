@@ -115,10 +115,17 @@ constexpr int NPHASE = 6;
 // kernel values, band list and map, and the factorised G.  It depends only
 // on the motion, so the fused path builds it GEO_AHEAD steps in advance, on
 // side streams, into one of GEO_SETS sets while earlier steps read theirs.
-constexpr int GEO_SETS = 2, GEO_AHEAD = 1;
+#ifndef LBM_GEO_AHEAD
+#define LBM_GEO_AHEAD 1
+#endif
+constexpr int GEO_AHEAD = LBM_GEO_AHEAD, GEO_SETS = GEO_AHEAD + 1;
 // steps per CUDA graph: a multiple of 2 (plane parity) and of GEO_SETS, so
 // a graph ends in the state it started from
-constexpr int GRAPH_STEPS = 2;
+#ifndef LBM_GRAPH_STEPS
+#define LBM_GRAPH_STEPS (GEO_SETS % 2 ? 2 * GEO_SETS : GEO_SETS)
+#endif
+constexpr int GRAPH_STEPS = LBM_GRAPH_STEPS;
+static_assert(GRAPH_STEPS % 2 == 0 && GRAPH_STEPS % GEO_SETS == 0, "a graph returns to its parity and set");
 struct GeoSet {
     WingMotion* wm = nullptr;
     double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
@@ -554,6 +561,9 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         if (prefetch) {
             cudaStream_t sa = h->s_aux[h->parity], sb = h->s_aux2[h->parity];
             cudaStreamWaitEvent(sa, h->ev_main, 0);
+            // builds read and advance the geometry's cycle counter in order
+            const int sp = (sn + GEO_SETS - 1) % GEO_SETS;
+            if (GEO_AHEAD > 1 && h->pending[sp]) cudaStreamWaitEvent(sa, h->ev_list[sp], 0);
             {
                 PhaseMark pm(h, 0, sa);
                 launch_ibm_band(dn, sa, h->ev_geom[h->parity]);
@@ -955,9 +965,10 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     d.solve_stream = !d.solve_in_smem && ibm_solve_ring_fits(bwmax) &&
                      ibm_solve_smem(nwmax, bwmax, wmax, false) + ibm_solve_ring_bytes(bwmax) <= smem_cap;
     if (d.solve_stream) d.solve_smem += (long long)ibm_solve_ring_bytes(bwmax);
-    // substitution in 32-row panels when every wing's panel data fit in
-    // shared memory (the factorisation then also builds them)
-    d.solve32 = W > 0 && !(c.flags & LBM_FLAG_SOLVE_STREAM) && ibm_solve32_smem(qmax, nwmax, bwmax) <= smem_cap;
+    // substitution in 32-row panels on request, when every wing's panel
+    // data fit in shared memory (the factorisation then also builds them)
+    d.solve32 = (c.flags & LBM_FLAG_SOLVE_PANELS32) && W > 0 && !(c.flags & LBM_FLAG_SOLVE_STREAM) &&
+                ibm_solve32_smem(qmax, nwmax, bwmax) <= smem_cap;
     if (d.solve32) d.solve_smem = (long long)ibm_solve32_smem(qmax, nwmax, bwmax);
     CK(ibm_prepare(h->factor_smem, (size_t)d.solve_smem));
     if (dalloc(h, &d.piv_floor, wz) || dalloc(h, &d.ymax, 2 * wz) || dalloc(h, &d.ibm_flags, 4) ||

@@ -113,28 +113,32 @@ def test_batch_rejects_bad_input(gpu_lib):
 
 
 def test_substitution_forms_agree(gpu_lib):
-    """The substitution in 32-row panels (the default where the panel data
-    fit in shared memory) and the 8-row substitution streaming the factor
-    through a ring of rows (the form of wings too large for shared memory)
-    solve the same system: on the FP64 path, force rows within 1e-10
-    relative; the streamed form gives the same bits alone and packed."""
+    """The three substitutions solve the same system: the 8-row form with
+    the wing's factor whole in shared memory (the default), the 8-row form
+    streaming the factor through a ring of rows (wings too large for shared
+    memory) and the 32-row panels built by the factorisation: on the FP64
+    path, force rows within 1e-10 relative; on the FP32 path each form gives
+    the same bits alone and packed."""
     ep = small("s", 2, (5.0, 2.5), markers=160)
-    with api.Simulation(ep, api.PRECISION_FP64) as a, \
-            api.Simulation(ep, api.PRECISION_FP64, flags=api.FLAG_SOLVE_STREAM) as b:
-        ra, rb = a.step(12), b.step(12)
+    forms = (api.FLAG_SOLVE_STREAM, api.FLAG_SOLVE_PANELS32)
+    with api.Simulation(ep, api.PRECISION_FP64) as a:
+        ra = a.step(12)
     scale = np.abs(ra[:, 1:7]).max()
-    assert np.abs(rb[:, 1:7] - ra[:, 1:7]).max() <= 1e-10 * scale
-    ref = api.Simulation(ep, api.PRECISION_FP32)
-    st = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
-    st2 = api.Simulation(ep, api.PRECISION_FP32, flags=api.FLAG_SOLVE_STREAM)
-    try:
-        rows_st = st.step(12)
-        with api.Batch(0) as batch:
-            _same(rows_st, batch.step([st2], 12)[0])
-        _same(st.f(), st2.f())
-    finally:
-        for s_ in (ref, st, st2):
-            s_.close()
+    for fl in forms:
+        with api.Simulation(ep, api.PRECISION_FP64, flags=fl) as b:
+            rb = b.step(12)
+        assert np.abs(rb[:, 1:7] - ra[:, 1:7]).max() <= 1e-10 * scale, fl
+    for fl in forms:
+        st = api.Simulation(ep, api.PRECISION_FP32, flags=fl)
+        st2 = api.Simulation(ep, api.PRECISION_FP32, flags=fl)
+        try:
+            rows_st = st.step(12)
+            with api.Batch(0) as batch:
+                _same(rows_st, batch.step([st2], 12)[0])
+            _same(st.f(), st2.f())
+        finally:
+            st.close()
+            st2.close()
 
 
 def test_wing_too_large_for_shared_memory_matches_oracle(gpu_lib, oracle_lib):
