@@ -45,6 +45,8 @@ extern "C" {
 #define LBM_FLAG_NO_GRAPHS 1   /* launch every kernel directly (no CUDA graph replay) */
 #define LBM_FLAG_SOLVE_STREAM 2  /* stream each wing's factor through shared memory in an 8-row substitution
                                     even when the wing fits whole (for testing) */
+#define LBM_FLAG_SINGLE_STEPS 8   /* fused path: advance one step at a time instead of in two-step passes
+                                     (the same results; for testing and comparison) */
 #define LBM_FLAG_SOLVE_PANELS32 4  /* substitute in 32-row panels built by the factorisation, where every
                                       wing's panel data fit in shared memory (fewer dependent steps on the
                                       step's chain, a longer factorisation) */

@@ -240,6 +240,10 @@ __device__ __forceinline__ void ibm_geometry_kernel_body(const DevState& d, cons
         if (d.band_bits) atomicAnd(d.band_bits + (p >> 5), ~(1u << (p & 31)));
         if (d.precision == 0) { d.gfx[p] = 0.0; d.gfy[p] = 0.0; }
     }
+    if (d.tile_flags) {   // set again by the count kernel
+        const int nwords = (d.pass_ntx * d.pass_nty + 3) >> 2;
+        for (int b = t; b < nwords; b += stride) reinterpret_cast<unsigned*>(d.tile_flags)[b] = 0u;
+    }
     if (t == 0 && d.wing_count > 0 && d.motion_source == 1 && d.step_rows <= 0) set_status(d, ST_MOTION);
     if (t == 0) d.ibm_flags[0] = 0;   // set again by the count kernel when supports share nodes
 }
@@ -269,12 +273,23 @@ __global__ void ibm_claim_kernel_multi(MultiArgs m) {
     ibm_claim_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
 }
 
+// Flags the pass tiles whose R1 (the tile and one ring) holds node (i, j)
+// (0-based): tx with x0 - 1 <= i <= x0 + PASS_TX, ty with y0 - 1 <= j <=
+// y0 + PASS_TY (x0 = PASS_TX tx, y0 = 1 + PASS_TY ty).
+__device__ inline void flag_pass_tiles(const DevState& d, int i, int j) {
+    const int tx0 = max(0, (i + PASS_TX - 1) / PASS_TX - 1), tx1 = min(d.pass_ntx - 1, (i + 1) / PASS_TX);
+    const int ty0 = max(0, (j + PASS_TY - 2) / PASS_TY - 1), ty1 = min(d.pass_nty - 1, j / PASS_TY);
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) d.tile_flags[ty * d.pass_ntx + tx] = 1;
+}
+
 // Claims per segment, and the coupling test: a box node claimed by a
 // segment of another wing lies in the supports of both wings, so G has
 // entries between them and the wings are solved jointly (the lowest segment
 // index claims a node, hence every shared node is seen from the higher
 // wing's side).  One warp per segment, a box slot per lane: every node's
-// claimer is loaded at once and counted by a ballot.
+// claimer is loaded at once and counted by a ballot.  Each claimed node
+// flags the pass tiles around it.
 __device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const int bid_) {
     const int s = (bid_ * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (s >= d.nseg) return;
@@ -290,6 +305,7 @@ __device__ __forceinline__ void ibm_count_kernel_body(const DevState& d, const i
                 const int bm = d.band_map[pidx(d, i - 1, j - 1)];
                 mine = bm == s;
                 shared |= bm != s && bm >= 0 && bm < d.nseg && d.seg_wing[bm] != w;
+                if (mine && d.tile_flags) flag_pass_tiles(d, i - 1, j - 1);
             }
             c += __popc(__ballot_sync(0xffffffffu, mine));
         }
@@ -339,6 +355,29 @@ __device__ __forceinline__ void ibm_scan_kernel_body(const DevState& d, const in
         d.band_n[0] = nb;
         d.claim_cnt[d.nseg] = nb;
     }
+    if (!d.tile_flags) return;
+    // the flagged pass tiles in index order (the same scan over the flags)
+    const int ntl = d.pass_ntx * d.pass_nty, tper = (ntl + nt - 1) / nt;
+    const int t0 = min(ntl, tid * tper), t1 = min(ntl, t0 + tper);
+    int tl = 0;
+    for (int u = t0; u < t1; ++u) tl += d.tile_flags[u];
+    x = tl;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();   // wsum is free again
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int tb = 0, ttot = 0;
+    for (int k = 0; k < (nt >> 5); ++k) {
+        if (k < warp) tb += wsum[k];
+        ttot += wsum[k];
+    }
+    int at = tb + x - tl;
+    for (int u = t0; u < t1; ++u)
+        if (d.tile_flags[u]) d.tile_list[at++] = u;
+    if (tid == 0) d.tile_n[0] = ttot;
 }
 __global__ void __launch_bounds__(1024) ibm_scan_kernel(DevState d) { ibm_scan_kernel_body(d, blockIdx.x); }
 __global__ void __launch_bounds__(1024) ibm_scan_kernel_multi(MultiArgs m) {

@@ -200,7 +200,9 @@ __global__ void __launch_bounds__(TMA_THREADS) fused_bulk_tma_kernel(const __gri
     }
 }
 
-int fused_tensor_map(const DevState& d, const float* base, void* out) {
+// Tensor map of the nine planes at base (x: columns of the pitched rows, y:
+// rows, z: planes) with the given box; 0 on success.
+static int encode_plane_map(const DevState& d, const float* base, const cuuint32_t box[3], void* out) {
     static std::once_flag once;
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     std::call_once(once, [] {
@@ -213,13 +215,195 @@ int fused_tensor_map(const DevState& d, const float* base, void* out) {
     if (!enc) return -1;
     const cuuint64_t dims[3] = {(cuuint64_t)d.pitch, (cuuint64_t)d.ny, 9};
     const cuuint64_t strides[2] = {(cuuint64_t)d.pitch * sizeof(float), (cuuint64_t)d.plane * sizeof(float)};
-    const cuuint32_t box[3] = {TMA_BOXW, TMA_TY, 1};
     const cuuint32_t es[3] = {1, 1, 1};
     const CUresult r = enc(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
                            const_cast<float*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : -1;
+}
+
+int fused_tensor_map(const DevState& d, const float* base, void* out) {
+    const cuuint32_t box[3] = {TMA_BOXW, TMA_TY, 1};
+    return encode_plane_map(d, base, box, out);
+}
+
+// ------------------------------------------------------------ two-step passes
+// One pass advances the interior n -> n + 2 with one read of step n's planes
+// P and one write of step n + 2's planes Q (temporal blocking: half the HBM
+// traffic of two steps).  A block takes a tile of PASS_TX x PASS_TY nodes:
+// one thread issues nine tiled tensor loads of the tile and two rings of
+// neighbours (box of PASS_TX + 8 columns from x0 - 4, 16-byte aligned, and
+// PASS_TY + 4 rows from y0 - 2; out-of-range parts read as zero), the block
+// computes step n + 1 on the tile and one ring (R1) into shared memory, then
+// step n + 2 on the tile from there.  Step n + 1 values that are not plain
+// collisions -- band nodes of step n (immersed boundary) and the border (far
+// field) -- come from O, where the band re-collision and the far field of
+// step n put them; tiles whose R1 holds such nodes are the near tiles, run
+// after those writers, every other tile (the far tiles) from the start of
+// the pass.  Band nodes of step n + 1 and the border are left out of Q: the
+// second step's band re-collision and far field write them.  Every node is
+// computed by fused_collide, as in the one-step kernels, so a pass gives the
+// bits of two steps.
+constexpr int PASS_THREADS = 256;
+constexpr int PASS_BOXW = PASS_TX + 8, PASS_BOXH = PASS_TY + 4;
+constexpr int PASS_CH = (PASS_BOXH * PASS_BOXW + 31) & ~31;   // floats per input plane, 128-byte multiple
+constexpr int PASS_MW = PASS_TX + 2, PASS_MH = PASS_TY + 2;   // R1
+constexpr int PASS_MCH = PASS_MH * PASS_MW;
+constexpr size_t PASS_SMEM = (size_t)(9 * PASS_CH + 9 * PASS_MCH) * sizeof(float) + 128;
+static_assert(PASS_TX % 4 == 0, "tile columns start on 16-byte boundaries");
+static_assert(PASS_BOXW <= 256 && PASS_BOXH <= 256, "tensor-map box extents");
+
+template <bool NEAR>
+__device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin, float* Smid,
+                                          uint64_t* bar) {
+    const int tx = t % a.ntx, ty = t / a.ntx;
+    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, (uint32_t)(9 * PASS_BOXH * PASS_BOXW * sizeof(float)));
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * PASS_CH, tm, x0 - 4, y0 - 2, k, bar);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
+        mbar_wait(bar, 0);   // let a late copy land before the block exits
+        return;
+    }
+    // step n + 1 on R1: node (x0 - 1 + mc, y0 - 1 + mr), box cell (mr + 1, mc + 3)
+    for (int n = threadIdx.x; n < PASS_MH * PASS_MW; n += PASS_THREADS) {
+        const int mr = n / PASS_MW, mc = n % PASS_MW;
+        float o[9];
+        if (NEAR) {
+            const int i = x0 - 1 + mc, j = y0 - 1 + mr;
+            if (i < 0 || i > a.nx - 1 || j < 0 || j > a.ny - 1) continue;   // outside: never pulled
+            const long long p = (long long)j * a.pitch + i;
+            const bool border = i == 0 || j == 0 || i == a.nx - 1 || j == a.ny - 1;
+            if (border || ((__ldg(a.bits0 + (p >> 5)) >> (p & 31)) & 1u)) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) Smid[k * PASS_MCH + n] = __ldcg(a.O + k * a.plane + p);
+                continue;
+            }
+        }
+        float g[9], drho, jx, jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g[k] = Sin[k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc + 3 - ex(k)];
+        fused_collide(g, a.c, o, drho, jx, jy);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Smid[k * PASS_MCH + n] = o[k];
+    }
+    __syncthreads();
+    // step n + 2 on the tile: node (x0 + cc, y0 + rr), R1 cell (rr + 1, cc + 1)
+    for (int n = threadIdx.x; n < PASS_TY * PASS_TX; n += PASS_THREADS) {
+        const int rr = n / PASS_TX, cc = n % PASS_TX, i = x0 + cc, j = y0 + rr;
+        if (NEAR && (i < 1 || i > a.nx - 2 || j > a.ny - 2)) continue;
+        const long long p = (long long)j * a.pitch + i;
+        if ((__ldg(a.bits1 + (p >> 5)) >> (p & 31)) & 1u) continue;   // band nodes of step n + 1
+        float g[9], o[9], drho, jx, jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g[k] = Smid[k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc + 1 - ex(k)];
+        fused_collide(g, a.c, o, drho, jx, jy);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a.Q[k * a.plane + p] = o[k];
+    }
+}
+
+__global__ void __launch_bounds__(PASS_THREADS, 4) pass_far_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                   const PassArgs a) {
+    extern __shared__ unsigned char pass_raw[];
+    __shared__ uint64_t bar;
+    const int t = blockIdx.x;
+    if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) || __ldg(a.flags0 + t)) return;   // a near tile
+    float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
+    pass_tile<false>(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
+}
+
+__global__ void __launch_bounds__(PASS_THREADS, 4) pass_near_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                    const PassArgs a) {
+    extern __shared__ unsigned char pass_raw[];
+    __shared__ uint64_t bar;
+    const int b = blockIdx.x;
+    int t;
+    if (b < a.nborder) {
+        t = __ldg(a.border_list + b);
+    } else {
+        if (b - a.nborder >= min(__ldcg(a.band_n), a.band_cap)) return;
+        t = __ldcg(a.band_list + (b - a.nborder));
+        if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny)) return;   // taken by its border block
+    }
+    float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
+    pass_tile<true>(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
+}
+
+int pass_tensor_map(const DevState& d, const float* base, void* out) {
+    const cuuint32_t box[3] = {PASS_BOXW, PASS_BOXH, 1};
+    return encode_plane_map(d, base, box, out);
+}
+
+void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st) {
+    pass_far_kernel<<<a.ntx * a.nty, PASS_THREADS, PASS_SMEM, st>>>(*reinterpret_cast<const CUtensorMap*>(tmap), a);
+}
+
+void launch_pass_near(const PassArgs& a, const void* tmap, cudaStream_t st) {
+    pass_near_kernel<<<a.nborder + a.band_cap, PASS_THREADS, PASS_SMEM, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(tmap), a);
+}
+
+cudaError_t pass_prepare() {
+    cudaError_t e = cudaFuncSetAttribute(pass_far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PASS_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pass_near_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PASS_SMEM);
+    return e;
+}
+
+bool is_pass_far_kernel(const void* func) { return func == reinterpret_cast<const void*>(pass_far_kernel); }
+bool is_pass_near_kernel(const void* func) { return func == reinterpret_cast<const void*>(pass_near_kernel); }
+
+// Step n + 1 values for the second step's immersed boundary and far field:
+// item t < 64 nseg is slot t % 64 of the 8 x 8 square around segment
+// t / 64's support box (the box and one ring), then the columns 1..3,
+// nx-4..nx-2 (rows 1..ny-2) and the rows 1, 2, ny-3, ny-2 (columns
+// 4..nx-5).  Band nodes of step n are skipped (the band re-collision writes
+// them), and so are nodes outside a segment's square.
+__global__ void __launch_bounds__(256) pass_ring_kernel(const DevState d, const float* __restrict__ P,
+                                                        float* __restrict__ O, const unsigned* __restrict__ bits0) {
+    const long long nbox = 64LL * d.nseg, ncol = 6LL * (d.ny - 2), nrow = 4LL * (d.nx - 8);
+    for (long long t = (long long)blockIdx.x * 256 + threadIdx.x; t < nbox + ncol + nrow;
+         t += (long long)gridDim.x * 256) {
+        int i, j;
+        if (t < nbox) {
+            const int s = (int)(t >> 6), a = (int)(t & 63) >> 3, c = (int)(t & 7);
+            const int i1 = d.box[4 * s], i2 = d.box[4 * s + 1], j1 = d.box[4 * s + 2], j2 = d.box[4 * s + 3];
+            if (i2 < i1 || j2 < j1 || a > i2 - i1 + 2 || c > j2 - j1 + 2) continue;
+            i = i1 - 2 + a;   // box columns i1 - 1 .. i2 - 1 (0-based) and one ring
+            j = j1 - 2 + c;
+        } else if (t < nbox + ncol) {
+            const int u = (int)(t - nbox), col = u / (d.ny - 2);
+            i = col < 3 ? 1 + col : d.nx - 7 + col;   // 1, 2, 3, nx-4, nx-3, nx-2
+            j = 1 + u % (d.ny - 2);
+        } else {
+            const int u = (int)(t - nbox - ncol), row = u / (d.nx - 8);
+            j = row < 2 ? 1 + row : d.ny - 5 + row;   // 1, 2, ny-3, ny-2
+            i = 4 + u % (d.nx - 8);
+        }
+        if (i < 1 || i > d.nx - 2 || j < 1 || j > d.ny - 2) continue;
+        const long long p = (long long)j * d.pitch + i;
+        if ((__ldg(bits0 + (p >> 5)) >> (p & 31)) & 1u) continue;
+        float g[9], o[9], drho, jx, jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g[k] = __ldg(P + k * d.plane + p - ex(k) - (long long)ey(k) * d.pitch);
+        fused_collide(g, d.fc, o, drho, jx, jy);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) O[k * d.plane + p] = o[k];
+    }
+}
+
+void launch_pass_ring(const DevState& d, const float* P, float* O, const unsigned* bits0, cudaStream_t st) {
+    const long long n = 64LL * d.nseg + 6LL * (d.ny - 2) + 4LL * (d.nx - 8);
+    const int grid = (int)std::min<long long>(1184, std::max<long long>(1, (n + 255) / 256));
+    pass_ring_kernel<<<grid, 256, 0, st>>>(d, P, O, bits0);
 }
 
 // Packed form: an episode's interior nodes, row by row without the border

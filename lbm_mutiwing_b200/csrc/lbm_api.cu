@@ -114,18 +114,20 @@ constexpr int NPHASE = 6;
 // Immersed-boundary geometry of one step: motion, markers, support boxes,
 // kernel values, band list and map, and the factorised G.  It depends only
 // on the motion, so the fused path builds it GEO_AHEAD steps in advance, on
-// side streams, into one of GEO_SETS sets while earlier steps read theirs.
+// side streams, into one of GEO_SETS sets while earlier steps read theirs:
+// a two-step pass reads the sets of its two steps and builds the next two.
 #ifndef LBM_GEO_AHEAD
-#define LBM_GEO_AHEAD 1
+#define LBM_GEO_AHEAD 2
 #endif
-constexpr int GEO_AHEAD = LBM_GEO_AHEAD, GEO_SETS = GEO_AHEAD + 1;
-// steps per CUDA graph: a multiple of 2 (plane parity) and of GEO_SETS, so
-// a graph ends in the state it started from
+constexpr int GEO_AHEAD = LBM_GEO_AHEAD, GEO_SETS = 2 * GEO_AHEAD;
+// steps per CUDA graph of single steps: a multiple of 2 (the two plane
+// copies alternate) and of GEO_SETS, so a graph ends in the state it started
+// from (graphs of passes hold one pass)
 #ifndef LBM_GRAPH_STEPS
 #define LBM_GRAPH_STEPS (GEO_SETS % 2 ? 2 * GEO_SETS : GEO_SETS)
 #endif
 constexpr int GRAPH_STEPS = LBM_GRAPH_STEPS;
-static_assert(GRAPH_STEPS % 2 == 0 && GRAPH_STEPS % GEO_SETS == 0, "a graph returns to its parity and set");
+static_assert(GRAPH_STEPS % 2 == 0 && GRAPH_STEPS % GEO_SETS == 0, "a graph returns to its planes and set");
 struct GeoSet {
     WingMotion* wm = nullptr;
     double *xb1 = nullptr, *yb1 = nullptr, *xb2 = nullptr, *yb2 = nullptr, *kx = nullptr, *ky = nullptr;
@@ -133,6 +135,8 @@ struct GeoSet {
     int *band_ij = nullptr, *band_wing = nullptr, *band_map = nullptr, *ibm_flags = nullptr;
     unsigned* band_bits = nullptr;
     double *lband = nullptr, *linv = nullptr, *lq = nullptr;
+    unsigned char* tile_flags = nullptr;
+    int *tile_list = nullptr, *tile_n = nullptr;
 };
 
 static GeoSet geo_of(const DevState& d) {
@@ -142,6 +146,7 @@ static GeoSet geo_of(const DevState& d) {
     g.band_n = d.band_n; g.band_ij = d.band_ij; g.band_wing = d.band_wing; g.band_map = d.band_map;
     g.band_bits = d.band_bits;
     g.ibm_flags = d.ibm_flags; g.lband = d.lband; g.linv = d.linv; g.lq = d.lq;
+    g.tile_flags = d.tile_flags; g.tile_list = d.tile_list; g.tile_n = d.tile_n;
     return g;
 }
 
@@ -151,6 +156,7 @@ static void use_geo(DevState& d, const GeoSet& g) {
     d.band_n = g.band_n; d.band_ij = g.band_ij; d.band_wing = g.band_wing; d.band_map = g.band_map;
     d.band_bits = g.band_bits;
     d.ibm_flags = g.ibm_flags; d.lband = g.lband; d.linv = g.linv; d.lq = g.lq;
+    d.tile_flags = g.tile_flags; d.tile_list = g.tile_list; d.tile_n = g.tile_n;
 }
 
 struct LbmHandle {
@@ -158,8 +164,12 @@ struct LbmHandle {
     std::string err;
     DevState d{};
     FusedConsts fc{};
-    int parity = 0;                 // fused path: 0 -> current planes in gA
-    float* planes[2] = {nullptr, nullptr};
+    // fused path: three plane copies; a step goes from planes[cur] to
+    // planes[alt] and swaps them, a pass writes its second step to the third
+    // copy (its first step's band and border values to planes[alt]), which
+    // becomes cur
+    int cur = 0, alt = 1;
+    float* planes[3] = {nullptr, nullptr, nullptr};
     GeoSet geo[GEO_SETS];           // geometry sets (the plain path uses set 0)
     int gset = 0;                   // fused path: set of the next step
     int prio_lo = 0, prio_hi = 0;   // stream priority range of the device
@@ -171,8 +181,12 @@ struct LbmHandle {
     // pairs of geometry streams used by alternate steps, so that the
     // geometry builds of consecutive steps run side by side: aux (motion,
     // markers, band list), aux2 (assembly and factorisation of G)
-    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_bc = nullptr, s_aux[2] = {}, s_aux2[2] = {};
-    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_bc = nullptr, ev_geom[2] = {};
+    // near: the near tiles of a pass
+    cudaStream_t s_main = nullptr, s_ibm = nullptr, s_bc = nullptr, s_aux[2] = {}, s_aux2[2] = {}, s_near = nullptr;
+    cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_bc = nullptr, ev_geom[GEO_SETS] = {};
+    // a pass: first step's chain and far field done, step n + 1 ring
+    // values written, near tiles done
+    cudaEvent_t ev_chain1 = nullptr, ev_bc1 = nullptr, ev_ring = nullptr, ev_near = nullptr;
     cudaEvent_t ev_list[GEO_SETS] = {}, ev_fact[GEO_SETS] = {};   // a set's band list / factor done
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
@@ -202,15 +216,20 @@ struct LbmHandle {
     std::vector<std::pair<int, std::pair<size_t, size_t>>> marks;   // phase, (start ev, stop ev)
     double phase_ms[NPHASE] = {0, 0, 0, 0, 0, 0};
     long long timed_steps = 0;
-    // CUDA graphs of two consecutive steps, one per starting parity; any
-    // change of a pointer or value baked into DevState drops them
-    cudaGraphExec_t gexec[2][GEO_SETS] = {};
-    // tensor maps of the two plane copies (fused path), for the tiled bulk
-    // kernel; tmap_ok false keeps the kernel with global pulls
-    CUtensorMap tmap[2];
-    bool tmap_ok = false;
+    // CUDA graphs of GRAPH_STEPS single steps, and of one pass, by starting
+    // planes (cur, alt) and geometry set; any change of a pointer or value
+    // baked into DevState drops them
+    cudaGraphExec_t gexec[3][3][GEO_SETS] = {};
+    cudaGraphExec_t pexec[3][3][GEO_SETS] = {};
+    // tensor maps of the three plane copies (fused path), for the tiled bulk
+    // kernel (tmap_ok false keeps the kernel with global pulls) and the
+    // pass kernels (passes run when pass_ok)
+    CUtensorMap tmap[3], ptmap[3];
+    bool tmap_ok = false, pass_ok = false;
+    int* border_tiles = nullptr;    // pass tiles whose R1 meets the border
+    int nborder = 0;
     double* d_out = nullptr;        // strided output fields (SAVE)
-    size_t out_cap = 0;   // by starting plane parity and geometry set
+    size_t out_cap = 0;
     // Continuation state: the cycle the device counters hold after the last
     // call (-1: unknown), and, on the fused path, the cycle whose geometry
     // the last step of that call built into set gset (-1: none, or made
@@ -290,12 +309,13 @@ int dalloc(LbmHandle* h, T** p, size_t count) {
 DevState current(const LbmHandle* h) {
     DevState d = h->d;
     if (d.precision != 0) {
-        d.gA = h->planes[h->parity];
-        d.gB = h->planes[1 - h->parity];
+        d.gA = h->planes[h->cur];
+        d.gB = h->planes[h->alt];
         use_geo(d, h->geo[h->gset]);
     }
     return d;
 }
+int third_planes(const LbmHandle* h) { return 3 - h->cur - h->alt; }
 
 // The geometry of the last completed step (band list, markers).
 DevState last_geometry(const LbmHandle* h) {
@@ -393,7 +413,8 @@ int init_state(LbmHandle* h) {
             fill(d.pre, 1.0 / 3.0) || fill(d.gfx, 0.0) || fill(d.gfy, 0.0))
             return -1;
     } else {
-        h->parity = 0;
+        h->cur = 0;
+        h->alt = 1;
         d = current(h);
         launch_fused_init(d, h->s_main);
         CK(cudaGetLastError());
@@ -498,8 +519,8 @@ void collect_phase_times(LbmHandle* h) {
 // Fused path: the geometry (motion, markers, band list and factorised G) of
 // the first GEO_AHEAD steps of a call, each in its own set; every later
 // step's geometry is built GEO_AHEAD steps ahead while earlier steps run.
-void prime_geometry(LbmHandle* h, int64_t n_steps) {
-    for (int a = 0; a < GEO_AHEAD && a < n_steps; ++a) {
+void prime_geometry(LbmHandle* h) {
+    for (int a = 0; a < GEO_AHEAD; ++a) {
         DevState d = current(h);
         use_geo(d, h->geo[(h->gset + a) % GEO_SETS]);
         launch_ibm_band(d, h->s_main, nullptr);
@@ -508,7 +529,42 @@ void prime_geometry(LbmHandle* h, int64_t n_steps) {
     for (bool& p : h->pending) p = false;
 }
 
-// One evolution step (solution.f90:272-422) on the current parity.  On the
+// Makes the main stream wait for every geometry set still building.
+void wait_pending(LbmHandle* h) {
+    for (int s = 0; s < GEO_SETS; ++s)
+        if (h->pending[s]) {
+            cudaStreamWaitEvent(h->s_main, h->ev_list[s], 0);
+            cudaStreamWaitEvent(h->s_main, h->ev_fact[s], 0);
+            h->pending[s] = false;
+        }
+}
+
+// The geometry of set sn on the side streams (pair k), GEO_AHEAD steps ahead
+// of the step that starts it; its band list and factor events let later
+// steps wait for it.  Builds read and advance the geometry's cycle counter,
+// so a build starts after the previous build's band list.
+void build_geometry(LbmHandle* h, int sn, int k) {
+    DevState dn = h->d;
+    use_geo(dn, h->geo[sn]);
+    cudaStream_t sa = h->s_aux[k], sb = h->s_aux2[k];
+    cudaStreamWaitEvent(sa, h->ev_main, 0);
+    const int sp = (sn + GEO_SETS - 1) % GEO_SETS;
+    if (h->pending[sp]) cudaStreamWaitEvent(sa, h->ev_list[sp], 0);
+    {
+        PhaseMark pm(h, 0, sa);
+        launch_ibm_band(dn, sa, h->ev_geom[sn]);
+    }
+    cudaEventRecord(h->ev_list[sn], sa);
+    cudaStreamWaitEvent(sb, h->ev_geom[sn], 0);
+    {
+        PhaseMark pm(h, 5, sb);
+        launch_ibm_factor(dn, h->factor_smem, sb);
+    }
+    cudaEventRecord(h->ev_fact[sn], sb);
+    h->pending[sn] = true;
+}
+
+// One evolution step (solution.f90:272-422) on the current planes.  On the
 // fused path, prefetch builds the geometry of the step GEO_AHEAD ahead, and
 // drain makes this step wait for it as well (graph boundaries).
 void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drain) {
@@ -553,30 +609,10 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         // prime); the one built now goes to the set whose last reader was
         // the previous step.
         const int sn = (h->gset + GEO_AHEAD) % GEO_SETS, s1 = (h->gset + 1) % GEO_SETS;
-        DevState dn = d;
-        use_geo(dn, h->geo[sn]);
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
         cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
-        if (prefetch) {
-            cudaStream_t sa = h->s_aux[h->parity], sb = h->s_aux2[h->parity];
-            cudaStreamWaitEvent(sa, h->ev_main, 0);
-            // builds read and advance the geometry's cycle counter in order
-            const int sp = (sn + GEO_SETS - 1) % GEO_SETS;
-            if (GEO_AHEAD > 1 && h->pending[sp]) cudaStreamWaitEvent(sa, h->ev_list[sp], 0);
-            {
-                PhaseMark pm(h, 0, sa);
-                launch_ibm_band(dn, sa, h->ev_geom[h->parity]);
-            }
-            cudaEventRecord(h->ev_list[sn], sa);
-            cudaStreamWaitEvent(sb, h->ev_geom[h->parity], 0);
-            {
-                PhaseMark pm(h, 5, sb);
-                launch_ibm_factor(dn, h->factor_smem, sb);
-            }
-            cudaEventRecord(h->ev_fact[sn], sb);
-            h->pending[sn] = true;
-        }
+        if (prefetch) build_geometry(h, sn, h->gset & 1);
         {
             PhaseMark pm(h, 3, h->s_bc);
             launch_outer_bc(d, h->s_bc);
@@ -593,7 +629,7 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         cudaEventRecord(h->ev_ibm, h->s_ibm);
         {
             PhaseMark pm(h, 1, h->s_main);
-            launch_fused_bulk(d, h->fc, fields, h->tmap_ok ? &h->tmap[h->parity] : nullptr, h->s_main);
+            launch_fused_bulk(d, h->fc, fields, h->tmap_ok ? &h->tmap[h->cur] : nullptr, h->s_main);
         }
         cudaStreamWaitEvent(h->s_main, h->ev_ibm, 0);
         cudaStreamWaitEvent(h->s_main, h->ev_bc, 0);
@@ -604,41 +640,150 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
             cudaStreamWaitEvent(h->s_main, h->ev_fact[s], 0);
             h->pending[s] = false;
         }
-        h->parity = 1 - h->parity;
+        std::swap(h->cur, h->alt);
         h->last_gset = h->gset;
         h->gset = s1;
     }
     if (h->timing) h->timed_steps += 1;
 }
 
-void drop_graphs(LbmHandle* h) {
-    for (auto& row : h->gexec)
-        for (auto& g : row)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
+// Two steps n -> n + 2 of the fused path in one pass (no fields, no
+// diagnostics): P = planes[cur] (step n), O = planes[alt] (step n + 1 where
+// the second step's immersed boundary and far field and the near tiles read
+// it), Q = the third copy (step n + 2).
+//   s_ibm   chain of step n (P -> O at its band nodes), then, after the
+//           ring, the chain of step n + 1 (O -> Q at its band nodes)
+//   s_bc    far field of step n (P -> O border), the ring (P -> O: the
+//           support boxes of step n + 1 and one ring around them, the
+//           columns and rows the far field reads), then, after the first
+//           chain (a band node may sit in column 3), the far field of
+//           step n + 1 (O -> Q border)
+//   s_main  far tiles (P -> Q), from the start
+//   s_near  near tiles (P and O -> Q), after the first chain and far field
+//   aux     the geometry of steps n + 2 and n + 3
+// The pass ends when all are done (the next pass reads all of them).
+void enqueue_pass(LbmHandle* h) {
+    wait_pending(h);   // both steps' geometry is complete before the pass starts
+    const int g0 = h->gset, g1 = (g0 + 1) % GEO_SETS, g2 = (g0 + 2) % GEO_SETS, g3 = (g0 + 3) % GEO_SETS;
+    const int third = third_planes(h);
+    float *P = h->planes[h->cur], *O = h->planes[h->alt], *Q = h->planes[third];
+    DevState dA = h->d, dB = h->d;
+    dA.diag = dB.diag = 0;
+    dA.write_fields = dB.write_fields = 0;
+    dA.gA = P;
+    dA.gB = O;
+    use_geo(dA, h->geo[g0]);
+    dB.gA = O;
+    dB.gB = Q;
+    use_geo(dB, h->geo[g1]);
+    PassArgs pa;
+    pa.P = P;
+    pa.O = O;
+    pa.Q = Q;
+    pa.bits0 = h->geo[g0].band_bits;
+    pa.bits1 = h->geo[g1].band_bits;
+    pa.flags0 = h->geo[g0].tile_flags;
+    pa.border_list = h->border_tiles;
+    pa.band_list = h->geo[g0].tile_list;
+    pa.band_n = h->geo[g0].tile_n;
+    pa.nborder = h->nborder;
+    pa.band_cap = std::min(h->d.pass_ntx * h->d.pass_nty, 4 * std::max(1, h->d.nseg));
+    pa.nx = h->d.nx;
+    pa.ny = h->d.ny;
+    pa.pitch = h->d.pitch;
+    pa.ntx = h->d.pass_ntx;
+    pa.nty = h->d.pass_nty;
+    pa.plane = h->d.plane;
+    pa.c = h->fc;
+    pa.status = h->d.status;
+    cudaEventRecord(h->ev_main, h->s_main);
+    for (cudaStream_t st : {h->s_ibm, h->s_bc, h->s_near}) cudaStreamWaitEvent(st, h->ev_main, 0);
+    build_geometry(h, g2, 0);
+    build_geometry(h, g3, 1);
+    {
+        PhaseMark pm(h, 3, h->s_bc);
+        launch_outer_bc(dA, h->s_bc);
+    }
+    cudaEventRecord(h->ev_bc1, h->s_bc);
+    {
+        PhaseMark pm(h, 2, h->s_bc);
+        launch_pass_ring(dB, P, O, pa.bits0, h->s_bc);
+    }
+    cudaEventRecord(h->ev_ring, h->s_bc);
+    {
+        PhaseMark pm(h, 4, h->s_ibm);
+        launch_ibm_rhs(dA, true, h->s_ibm);
+        launch_ibm_solve(dA, true, false, h->s_ibm);
+    }
+    cudaEventRecord(h->ev_chain1, h->s_ibm);
+    cudaStreamWaitEvent(h->s_ibm, h->ev_ring, 0);
+    {
+        PhaseMark pm(h, 4, h->s_ibm);
+        launch_ibm_rhs(dB, true, h->s_ibm);
+        launch_ibm_solve(dB, true, false, h->s_ibm);
+    }
+    cudaEventRecord(h->ev_ibm, h->s_ibm);
+    cudaStreamWaitEvent(h->s_bc, h->ev_chain1, 0);
+    {
+        PhaseMark pm(h, 3, h->s_bc);
+        launch_outer_bc(dB, h->s_bc);
+    }
+    cudaEventRecord(h->ev_bc, h->s_bc);
+    cudaStreamWaitEvent(h->s_near, h->ev_chain1, 0);
+    cudaStreamWaitEvent(h->s_near, h->ev_bc1, 0);
+    {
+        PhaseMark pm(h, 2, h->s_near);
+        launch_pass_near(pa, &h->ptmap[h->cur], h->s_near);
+    }
+    cudaEventRecord(h->ev_near, h->s_near);
+    {
+        PhaseMark pm(h, 1, h->s_main);
+        launch_pass_far(pa, &h->ptmap[h->cur], h->s_main);
+    }
+    for (cudaEvent_t e : {h->ev_ibm, h->ev_bc, h->ev_near, h->ev_list[g2], h->ev_fact[g2], h->ev_list[g3],
+                          h->ev_fact[g3]})
+        cudaStreamWaitEvent(h->s_main, e, 0);
+    for (bool& q : h->pending) q = false;
+    h->cur = third;   // O stays the overlay of the next pass; P is free
+    h->last_gset = g1;
+    h->gset = g2;
+    if (h->timing) h->timed_steps += 2;
 }
 
-// Two steps starting at parity p, captured from both streams (the second
-// stream joins and leaves through events, as in eager launches).
-// GRAPH_STEPS steps from plane parity p and geometry set gs.  The graph is
-// self-contained: it starts with the geometry of its first GEO_AHEAD steps
-// complete and its last step waits for the geometry it built for the steps
-// after the graph.
-int build_graph(LbmHandle* h, int p, int gs) {
+void drop_graphs(LbmHandle* h) {
+    for (auto* tab : {&h->gexec, &h->pexec})
+        for (auto& plane : *tab)
+            for (auto& row : plane)
+                for (auto& g : row)
+                    if (g) {
+                        cudaGraphExecDestroy(g);
+                        g = nullptr;
+                    }
+}
+
+// GRAPH_STEPS single steps, or one pass, from planes (c, a) and geometry
+// set gs, captured from all streams (the side streams join and leave
+// through events, as in eager launches).  The graph is self-contained: it
+// starts with the geometry of its first GEO_AHEAD steps complete and its
+// last step waits for the geometry it built for the steps after the graph.
+int build_graph(LbmHandle* h, int c, int a, int gs, bool pass) {
     DeviceLock lock(g_device_mutex);
-    const int saved = h->parity, saved_g = h->gset, saved_last = h->last_gset;
+    const int saved_c = h->cur, saved_a = h->alt, saved_g = h->gset, saved_last = h->last_gset;
     bool saved_pending[GEO_SETS];
     std::copy(h->pending, h->pending + GEO_SETS, saved_pending);
-    h->parity = p;
+    h->cur = c;
+    h->alt = a;
     h->gset = gs;
     for (bool& q : h->pending) q = false;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->s_main, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < GRAPH_STEPS; ++k) enqueue_step(h, false, false, true, k == GRAPH_STEPS - 1);
+    if (pass)
+        enqueue_pass(h);
+    else
+        for (int k = 0; k < GRAPH_STEPS; ++k) enqueue_step(h, false, false, true, k == GRAPH_STEPS - 1);
     cudaError_t e = cudaStreamEndCapture(h->s_main, &g);
-    h->parity = saved;
+    h->cur = saved_c;
+    h->alt = saved_a;
     h->gset = saved_g;
     h->last_gset = saved_last;
     std::copy(saved_pending, saved_pending + GEO_SETS, h->pending);
@@ -661,12 +806,14 @@ int build_graph(LbmHandle* h, int p, int gs) {
         if (e != cudaSuccess) break;
         cudaKernelNodeAttrValue v;
         std::memset(&v, 0, sizeof(v));
-        v.priority = is_bulk_kernel(kp.func)                                      ? h->prio_lo
-                     : (is_geometry_kernel(kp.func) || is_far_field_kernel(kp.func)) ? h->prio_mid
-                                                                                      : h->prio_hi;
+        v.priority = (is_bulk_kernel(kp.func) || is_pass_far_kernel(kp.func)) ? h->prio_lo
+                     : (is_geometry_kernel(kp.func) || is_far_field_kernel(kp.func) || is_pass_near_kernel(kp.func))
+                         ? h->prio_mid
+                         : h->prio_hi;
         e = cudaGraphKernelNodeSetAttribute(nodes[k], cudaKernelNodeAttributePriority, &v);
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->gexec[p][gs], g, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphExec_t& slot = pass ? h->pexec[c][a][gs] : h->gexec[c][a][gs];
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&slot, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
     return 0;
@@ -730,13 +877,19 @@ constexpr int BV_PLAIN = 0, BV_SECOND_LAST = 2, BV_LAST = 4, BV_AHEAD = 6, BV_CO
 constexpr int BATCH_SLOT_ITEMS = 4;   // per-slot items per thread in packed launches
 constexpr int64_t GRAPH_PAIR_MIN = 8;  // steady steps ahead before a step pair is captured
 
+// Packed steps alternate between the handle's two plane copies (cur, alt)
+// and two of its geometry sets (gset, gset + 1), each step building the next
+// step's geometry into the other set.
+int batch_set(const LbmHandle* h, int ph) { return (h->gset + (ph & 1)) % GEO_SETS; }
+
 void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out) {
     for (int ph = 0; ph < 2; ++ph) {
         DevState d = h->d;
-        const int p = h->parity ^ ph, g = (h->gset + ph) % GEO_SETS;
-        d.gA = h->planes[p];
-        d.gB = h->planes[1 - p];
+        const int g = batch_set(h, ph);
+        d.gA = h->planes[ph ? h->alt : h->cur];
+        d.gB = h->planes[ph ? h->cur : h->alt];
         use_geo(d, h->geo[g]);
+        d.tile_flags = nullptr;   // no passes in packed steps
         d.diag = 0;
         d.write_fields = 0;
         d.slot_items = BATCH_SLOT_ITEMS;
@@ -753,7 +906,8 @@ void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out
         }
         out[BV_LAST + ph] = l;
         DevState a = d;
-        use_geo(a, h->geo[(g + GEO_AHEAD) % GEO_SETS]);
+        use_geo(a, h->geo[batch_set(h, ph + 1)]);
+        a.tile_flags = nullptr;
         out[BV_AHEAD + ph] = a;
     }
 }
@@ -878,7 +1032,7 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             return -1;
     } else {
         if (dalloc(h, &h->planes[0], 9 * N) || dalloc(h, &h->planes[1], 9 * N) ||
-            dalloc(h, &d.edge_f0, 9 * (size_t)(2 * c.nx + 2 * c.ny)))
+            dalloc(h, &h->planes[2], 9 * N) || dalloc(h, &d.edge_f0, 9 * (size_t)(2 * c.nx + 2 * c.ny)))
             return -1;
     }
     if (dalloc(h, &d.band_map, N)) return -1;
@@ -990,6 +1144,30 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
             dalloc(h, &g.lq, (size_t)std::max<long long>(1, qtot)))
             return -1;
     }
+    if (c.precision != LBM_PRECISION_FP64) {
+        // pass tiles: flags and flagged-tile lists per geometry set, and the
+        // tiles whose R1 meets the border
+        const int ntx = pass_tiles_x(c.nx), nty = pass_tiles_y(c.ny), ntl = ntx * nty;
+        for (int s = 0; s < GEO_SETS; ++s) {
+            GeoSet& g = h->geo[s];
+            if (dalloc(h, &g.tile_flags, (size_t)(ntl + 3) / 4 * 4) || dalloc(h, &g.tile_list, (size_t)ntl) ||
+                dalloc(h, &g.tile_n, 1))
+                return -1;
+            CK(cudaMemset(g.tile_flags, 0, (size_t)(ntl + 3) / 4 * 4));
+            CK(cudaMemset(g.tile_n, 0, sizeof(int)));
+        }
+        h->d.tile_flags = h->geo[0].tile_flags;
+        h->d.tile_list = h->geo[0].tile_list;
+        h->d.tile_n = h->geo[0].tile_n;
+        h->d.pass_ntx = ntx;
+        h->d.pass_nty = nty;
+        std::vector<int> bt;
+        for (int t = 0; t < ntl; ++t)
+            if (pass_border_tile(t % ntx, t / ntx, c.nx, c.ny)) bt.push_back(t);
+        if (dalloc(h, &h->border_tiles, bt.size())) return -1;
+        CK(cudaMemcpy(h->border_tiles, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
+        h->nborder = (int)bt.size();
+    }
     if (ensure_rows(h, 1024)) return -1;
     // the immersed-boundary chain is latency-bound and on the critical path:
     // its stream gets the highest priority so its blocks are scheduled ahead
@@ -1006,10 +1184,11 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     for (int k = 0; k < 2; ++k) {
         CK(cudaStreamCreateWithPriority(&h->s_aux[k], cudaStreamNonBlocking, h->prio_mid));
         CK(cudaStreamCreateWithPriority(&h->s_aux2[k], cudaStreamNonBlocking, h->prio_mid));
-        CK(cudaEventCreateWithFlags(&h->ev_geom[k], cudaEventDisableTiming));
     }
+    for (int s = 0; s < GEO_SETS; ++s) CK(cudaEventCreateWithFlags(&h->ev_geom[s], cudaEventDisableTiming));
     CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, h->prio_mid));
-    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_bc})
+    CK(cudaStreamCreateWithPriority(&h->s_near, cudaStreamNonBlocking, h->prio_mid));
+    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_bc, &h->ev_chain1, &h->ev_bc1, &h->ev_ring, &h->ev_near})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     for (int s = 0; s < GEO_SETS; ++s) {
         CK(cudaEventCreateWithFlags(&h->ev_list[s], cudaEventDisableTiming));
@@ -1022,8 +1201,11 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
 #ifndef LBM_BULK_TILED
 #define LBM_BULK_TILED 1
 #endif
-        h->tmap_ok = LBM_BULK_TILED && fused_tensor_map(d, h->planes[0], &h->tmap[0]) == 0 &&
-                     fused_tensor_map(d, h->planes[1], &h->tmap[1]) == 0;
+        h->tmap_ok = LBM_BULK_TILED != 0;
+        for (int k = 0; k < 3; ++k) h->tmap_ok = h->tmap_ok && fused_tensor_map(d, h->planes[k], &h->tmap[k]) == 0;
+        // two-step passes need the tiled loads and a lattice of a few tiles
+        h->pass_ok = c.nx >= 16 && c.ny >= 16 && pass_prepare() == cudaSuccess;
+        for (int k = 0; k < 3; ++k) h->pass_ok = h->pass_ok && pass_tensor_map(d, h->planes[k], &h->ptmap[k]) == 0;
     }
     if (init_state(h)) return -1;
     return 0;
@@ -1133,24 +1315,34 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     if (n_steps > 0) h->next_cycle = h->geo_ready = -1;   // until the steps are enqueued
     const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
     const bool want_err = (flags & LBM_STEP_ERR) != 0;
-    // all but the last two steps replay a two-step CUDA graph; the last two
-    // may write fields or diagnostics and are launched directly
+    // all but the last two steps run as two-step passes (or, without
+    // passes, GRAPH_STEPS single steps) replayed from CUDA graphs; the last
+    // two may write fields or diagnostics and are launched directly
     const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
-    if (fused && n_steps > 0 && !have_geo) prime_geometry(h, n_steps);
+    const bool passes = fused && h->pass_ok && !(h->cfg.flags & LBM_FLAG_SINGLE_STEPS);
+    if (fused && n_steps > 0 && !have_geo) prime_geometry(h);
     int64_t n = 0;
-    if (graphs && fused && n + GRAPH_STEPS <= n_steps - 2) {
-        // Both graphs a run can meet (plane parity and geometry set advance
-        // together, so after an odd step count the next call starts from the
-        // other pair) are built by the first call that replays one, so later
-        // calls capture nothing.
-        for (int q = 0; q < 2; ++q) {
-            const int p = h->parity ^ q, g = (h->gset + q) % GEO_SETS;
-            if (!h->gexec[p][g] && build_graph(h, p, g)) return -1;
+    if (passes) {
+        for (; n + 2 <= n_steps - 2; n += 2) {
+            if (!graphs) {
+                enqueue_pass(h);
+                CK(cudaGetLastError());
+                continue;
+            }
+            wait_pending(h);
+            cudaGraphExec_t& ge = h->pexec[h->cur][h->alt][h->gset];
+            if (!ge && build_graph(h, h->cur, h->alt, h->gset, true)) return -1;
+            CK(cudaGraphLaunch(ge, h->s_main));
+            h->cur = third_planes(h);   // as enqueue_pass leaves the state
+            h->last_gset = (h->gset + 1) % GEO_SETS;
+            h->gset = (h->gset + 2) % GEO_SETS;
         }
+    } else if (graphs && fused) {
         // whole graphs while the last two steps stay outside
         for (; n + GRAPH_STEPS <= n_steps - 2; n += GRAPH_STEPS) {
-            cudaGraphExec_t& ge = h->gexec[h->parity][h->gset];
-            if (!ge && build_graph(h, h->parity, h->gset)) return -1;
+            wait_pending(h);
+            cudaGraphExec_t& ge = h->gexec[h->cur][h->alt][h->gset];
+            if (!ge && build_graph(h, h->cur, h->alt, h->gset, false)) return -1;
             CK(cudaGraphLaunch(ge, h->s_main));
             h->last_gset = (h->gset + GEO_SETS - 1) % GEO_SETS;
         }
@@ -1298,7 +1490,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
     };
     for (int64_t k = 0, a = active(0); k < K; ++k) {
         const int ph = (int)(k & 1);
-        const int an = (k + GEO_AHEAD < K) ? active(k + GEO_AHEAD) : 0;
+        const int an = (k + 1 < K) ? active(k + 1) : 0;
         sig.assign((size_t)a, 0);
         for (int e = 0; e < a; ++e) {
             const int i = order[e];
@@ -1488,9 +1680,9 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         h->geo_ready = -1;
         int rc = 0;
         if (ns > 0) {
-            h->parity ^= (int)(ns & 1);
-            h->last_gset = (int)((h->gset + ns - 1) % GEO_SETS);
-            h->gset = (int)((h->gset + ns) % GEO_SETS);
+            if (ns & 1) std::swap(h->cur, h->alt);
+            h->last_gset = batch_set(h, (int)((ns - 1) & 1));
+            h->gset = batch_set(h, (int)(ns & 1));
             if (want_err) {
                 std::swap(h->d.fo_u, h->d.fo_u0);
                 std::swap(h->d.fo_v, h->d.fo_v0);
@@ -1781,7 +1973,7 @@ int lbm_move_mesh(LbmHandle* h, int32_t dr) {
         launch_plain_shift(h->d, dr, h->s_main);
     } else {
         launch_fused_shift(current(h), dr, h->s_main);
-        h->parity = 1 - h->parity;
+        std::swap(h->cur, h->alt);
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s_main));
@@ -1859,13 +2051,15 @@ void lbm_destroy(LbmHandle* h) {
     drop_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->pinned) cudaFreeHost(h->pinned);
-    for (cudaStream_t s : {h->s_main, h->s_ibm, h->s_aux[0], h->s_aux[1], h->s_aux2[0], h->s_aux2[1], h->s_bc})
+    for (cudaStream_t s :
+         {h->s_main, h->s_ibm, h->s_aux[0], h->s_aux[1], h->s_aux2[0], h->s_aux2[1], h->s_bc, h->s_near})
         if (s) cudaStreamDestroy(s);
-    for (cudaEvent_t e : {h->ev_geom[0], h->ev_geom[1], h->ev_bc, h->ev_ibm, h->ev_main})
+    for (cudaEvent_t e : {h->ev_bc, h->ev_ibm, h->ev_main, h->ev_chain1, h->ev_bc1, h->ev_ring, h->ev_near})
         if (e) cudaEventDestroy(e);
     for (int s = 0; s < GEO_SETS; ++s) {
         if (h->ev_list[s]) cudaEventDestroy(h->ev_list[s]);
         if (h->ev_fact[s]) cudaEventDestroy(h->ev_fact[s]);
+        if (h->ev_geom[s]) cudaEventDestroy(h->ev_geom[s]);
     }
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
     delete h;

@@ -33,6 +33,52 @@ void launch_fused_shift(const DevState& d, int dr, cudaStream_t st);
 void launch_fused_export(const DevState& d, const float* g, double* f, cudaStream_t st);
 void launch_fused_import(const DevState& d, const double* f, float* g, cudaStream_t st);
 
+// Two-step pass n -> n + 2 of the fused path (kernels_fp32.cu).  Tile (tx,
+// ty) covers the interior nodes [PASS_TX tx, PASS_TX tx + PASS_TX - 1] x
+// [1 + PASS_TY ty, PASS_TY (ty + 1)]; its first step needs the tile and one
+// ring of neighbours (R1), its pulls a second ring.
+constexpr int PASS_TX = 64, PASS_TY = 8;
+inline int pass_tiles_x(int nx) { return (nx + PASS_TX - 1) / PASS_TX; }
+inline int pass_tiles_y(int ny) { return (ny - 2 + PASS_TY - 1) / PASS_TY; }
+// whether R1 of tile (tx, ty) holds a node of the lattice border
+inline __host__ __device__ bool pass_border_tile(int tx, int ty, int nx, int ny) {
+    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+    return x0 - 1 <= 0 || x0 + PASS_TX >= nx - 1 || y0 - 1 <= 0 || y0 + PASS_TY >= ny - 1;
+}
+struct PassArgs {
+    const float* P;              // planes of step n (read by the tensor map)
+    const float* O;              // planes of step n + 1: band nodes of step n and the border
+    float* Q;                    // planes of step n + 2
+    const unsigned* bits0;       // band bits of step n's geometry
+    const unsigned* bits1;       // band bits of step n + 1's geometry
+    const unsigned char* flags0; // tile flags of step n's geometry
+    const int* border_list;      // tiles whose R1 meets the border
+    const int* band_list;        // flagged tiles of step n's geometry
+    const int* band_n;           // their count
+    int nborder, band_cap;       // border tiles; capacity of the flagged-tile list
+    int nx, ny, pitch, ntx, nty;
+    long long plane;
+    FusedConsts c;
+    int* status;
+};
+// Tensor map of the nine planes at base for the pass kernel's boxes.
+int pass_tensor_map(const DevState& d, const float* base, void* out);
+// far tiles (every tile not flagged and off the border), from P alone
+void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st);
+// the border tiles and the flagged tiles, after the band and the far field
+// of step n have written their step n + 1 values to O
+void launch_pass_near(const PassArgs& a, const void* tmap, cudaStream_t st);
+// Step n + 1 values (from P) in O where the second step's immersed boundary
+// and far field read them: the support boxes of step n + 1's geometry and
+// one ring around them (d: that geometry), and the columns 1..3, nx-4..nx-2
+// and rows 1, 2, ny-3, ny-2; band nodes of step n (bits0) are left to the
+// band re-collision.
+void launch_pass_ring(const DevState& d, const float* P, float* O, const unsigned* bits0, cudaStream_t st);
+// raises the pass kernels' shared-memory limit (the calling thread's device)
+cudaError_t pass_prepare();
+bool is_pass_far_kernel(const void* func);
+bool is_pass_near_kernel(const void* func);
+
 // immersed boundary (ibm.cu)
 // move_boundary: motion, markers, boxes, band list; geometry_done (may be
 // null) is recorded once the boxes and kernel values exist
