@@ -18,9 +18,12 @@ e2e    = the same metric through the online STEP path of the C ABI: per
          segment of 50 steps, the segment's two motion rows go host -> device
          and every step's force row comes back device -> host, both inside the
          timed region.
-roofline: the fused collide-stream kernel's algorithmic traffic (9 reads +
-         9 writes of 4 bytes per interior node) over its mean CUDA-event time,
-         against the measured HBM copy bandwidth.
+roofline: the dominant kernel's algorithmic traffic over its mean CUDA-event
+         time, against the measured HBM copy bandwidth.  FP32 path: the
+         two-step pass's far-tile kernel, 9 reads of step n + 9 writes of
+         step n + 2, 4 bytes each, per node of the far tiles it processed
+         (64 x 8 nodes a tile); whole_step_frac counts 36 bytes per node and
+         step (a pass moves each node's distributions once for two steps).
 The distribution planes (2 x 288 MB) exceed the 126 MB L2, so no separate L2
 flush is needed between steps.
 
@@ -186,12 +189,12 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(workload_name):
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "fused_bulk_traffic.json")
+def ncu_traffic(workload_name, kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         d = json.load(open(p))
-        return d.get(workload_name)
+        return d.get(kernel, {}).get(workload_name)
     except Exception:
         return None
 
@@ -504,17 +507,24 @@ def run_ours(args):
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peak()
-    bytes_per_node = 72 if prec == api.PRECISION_FP32 else 144
     interior = (ep.nx - 2) * (ep.ny - 2)
-    alg_bytes = bytes_per_node * interior
-    bulk_ms = phases["collide_stream_ms"] / max(1, phases["steps"])
-    achieved = alg_bytes / (bulk_ms / 1e3) / 1e9
-    roof = {"kernel": "fused_bulk_kernel" if prec == api.PRECISION_FP32 else "plain stream+moments+collide",
-            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    if prec == api.PRECISION_FP32 and phases.get("passes", 0) > 0:
+        kernel = "pass_far_kernel"
+        launches = phases["passes"]
+        kernel_ms = phases["pass_far_ms"] / launches
+        alg_bytes = 72 * 512 * phases["far_tiles"] / launches
+        step_bytes = 36 * interior
+    else:
+        kernel = "fused_bulk_tma_kernel" if prec == api.PRECISION_FP32 else "plain stream+moments+collide"
+        kernel_ms = phases["collide_stream_ms"] / max(1, phases["steps"])
+        alg_bytes = (72 if prec == api.PRECISION_FP32 else 144) * interior
+        step_bytes = alg_bytes
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    roof = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind,
-            "traffic": ncu_traffic(ep.name) if prec == api.PRECISION_FP32 else None,
-            "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": bulk_ms,
-            "whole_step_frac": alg_bytes * K / (ms / 1e3) / 1e9 / peak}
+            "traffic": ncu_traffic(ep.name, kernel) if prec == api.PRECISION_FP32 else None,
+            "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": kernel_ms,
+            "whole_step_frac": step_bytes * K / (ms / 1e3) / 1e9 / peak}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms / K, "timed_repeats": len(reps),

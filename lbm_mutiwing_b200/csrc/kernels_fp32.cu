@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 4) pass_far_kernel(const __grid_
     __shared__ uint64_t bar;
     const int t = blockIdx.x;
     if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) || __ldg(a.flags0 + t)) return;   // a near tile
+    if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
     pass_tile<false>(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
 }

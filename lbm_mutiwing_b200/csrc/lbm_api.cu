@@ -108,8 +108,8 @@ static int rcm_order(const std::vector<double>& mx, const std::vector<double>& m
 using namespace lbm;
 
 // phase timers: move_boundary, collide-stream, band re-collision, far field,
-// immersed-boundary solve
-constexpr int NPHASE = 6;
+// immersed-boundary solve, factorisation, far tiles of passes
+constexpr int NPHASE = 7;
 
 // Immersed-boundary geometry of one step: motion, markers, support boxes,
 // kernel values, band list and map, and the factorised G.  It depends only
@@ -214,8 +214,9 @@ struct LbmHandle {
     std::vector<cudaEvent_t> evpool;
     size_t evused = 0;
     std::vector<std::pair<int, std::pair<size_t, size_t>>> marks;   // phase, (start ev, stop ev)
-    double phase_ms[NPHASE] = {0, 0, 0, 0, 0, 0};
-    long long timed_steps = 0;
+    double phase_ms[NPHASE] = {0, 0, 0, 0, 0, 0, 0};
+    long long timed_steps = 0, timed_passes = 0;
+    int* d_far_tiles = nullptr;     // far tiles processed while timing
     // CUDA graphs of GRAPH_STEPS single steps, and of one pass, by starting
     // planes (cur, alt) and geometry set; any change of a pointer or value
     // baked into DevState drops them
@@ -696,6 +697,7 @@ void enqueue_pass(LbmHandle* h) {
     pa.plane = h->d.plane;
     pa.c = h->fc;
     pa.status = h->d.status;
+    pa.far_tiles = h->timing ? h->d_far_tiles : nullptr;
     cudaEventRecord(h->ev_main, h->s_main);
     for (cudaStream_t st : {h->s_ibm, h->s_bc, h->s_near}) cudaStreamWaitEvent(st, h->ev_main, 0);
     build_geometry(h, g2, 0);
@@ -737,7 +739,7 @@ void enqueue_pass(LbmHandle* h) {
     }
     cudaEventRecord(h->ev_near, h->s_near);
     {
-        PhaseMark pm(h, 1, h->s_main);
+        PhaseMark pm(h, 1, h->s_main), pf(h, 6, h->s_main);
         launch_pass_far(pa, &h->ptmap[h->cur], h->s_main);
     }
     for (cudaEvent_t e : {h->ev_ibm, h->ev_bc, h->ev_near, h->ev_list[g2], h->ev_fact[g2], h->ev_list[g3],
@@ -747,7 +749,10 @@ void enqueue_pass(LbmHandle* h) {
     h->cur = third;   // O stays the overlay of the next pass; P is free
     h->last_gset = g1;
     h->gset = g2;
-    if (h->timing) h->timed_steps += 2;
+    if (h->timing) {
+        h->timed_steps += 2;
+        h->timed_passes += 1;
+    }
 }
 
 void drop_graphs(LbmHandle* h) {
@@ -1164,7 +1169,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         std::vector<int> bt;
         for (int t = 0; t < ntl; ++t)
             if (pass_border_tile(t % ntx, t / ntx, c.nx, c.ny)) bt.push_back(t);
-        if (dalloc(h, &h->border_tiles, bt.size())) return -1;
+        if (dalloc(h, &h->border_tiles, bt.size()) || dalloc(h, &h->d_far_tiles, 1)) return -1;
+        CK(cudaMemset(h->d_far_tiles, 0, sizeof(int)));
         CK(cudaMemcpy(h->border_tiles, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
         h->nborder = (int)bt.size();
     }
@@ -1323,6 +1329,15 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     if (fused && n_steps > 0 && !have_geo) prime_geometry(h);
     int64_t n = 0;
     if (passes) {
+        // the pass graphs this state can reach (the current planes move to
+        // the third copy and back, the sets by two, the overlay copy stays)
+        // are built by the first call that replays one, so later calls
+        // capture nothing
+        if (graphs && n + 2 <= n_steps - 2)
+            for (int q = 0; q < 4; ++q) {
+                const int c = (q & 1) ? third_planes(h) : h->cur, g = (h->gset + (q & 2)) % GEO_SETS;
+                if (!h->pexec[c][h->alt][g] && build_graph(h, c, h->alt, g, true)) return -1;
+            }
         for (; n + 2 <= n_steps - 2; n += 2) {
             if (!graphs) {
                 enqueue_pass(h);
@@ -2010,6 +2025,12 @@ int lbm_set_timing(LbmHandle* h, int32_t enable) {
     h->timing = enable != 0;
     for (double& v : h->phase_ms) v = 0.0;
     h->timed_steps = 0;
+    h->timed_passes = 0;
+    if (h->d_far_tiles) {
+        CK(cudaSetDevice(h->cfg.device));
+        CK(cudaMemsetAsync(h->d_far_tiles, 0, sizeof(int), h->s_main));
+        CK(cudaStreamSynchronize(h->s_main));
+    }
     h->marks.clear();
     h->evused = 0;
     return 0;
@@ -2017,10 +2038,18 @@ int lbm_set_timing(LbmHandle* h, int32_t enable) {
 
 int lbm_get_phase_times(LbmHandle* h, double* out, int32_t n) {
     if (!h || !out) return -1;
-    double v[NPHASE + 1] = {0};
-    for (int k = 0; k < NPHASE; ++k) v[k] = h->phase_ms[k];
-    v[NPHASE] = (double)h->timed_steps;
-    for (int k = 0; k < n && k <= NPHASE; ++k) out[k] = v[k];
+    double v[10] = {0};
+    for (int k = 0; k < 6; ++k) v[k] = h->phase_ms[k];
+    v[6] = (double)h->timed_steps;
+    v[7] = h->phase_ms[6];
+    v[8] = (double)h->timed_passes;
+    if (h->d_far_tiles) {
+        int ft = 0;
+        CK(cudaSetDevice(h->cfg.device));
+        CK(cudaMemcpy(&ft, h->d_far_tiles, sizeof(int), cudaMemcpyDeviceToHost));
+        v[9] = (double)ft;
+    }
+    for (int k = 0; k < n && k < 10; ++k) out[k] = v[k];
     return 0;
 }
 

@@ -60,6 +60,7 @@ struct PassArgs {
     long long plane;
     FusedConsts c;
     int* status;
+    int* far_tiles;              // counts the far tiles processed (null: not counted)
 };
 // Tensor map of the nine planes at base for the pass kernel's boxes.
 int pass_tensor_map(const DevState& d, const float* base, void* out);
