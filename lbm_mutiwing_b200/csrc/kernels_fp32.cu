@@ -44,55 +44,84 @@ FusedConsts fused_consts(const DevState& d) {
     return c;
 }
 
-// MRT collision of one node on its pulled deviations g (moments of the
-// deviation, relaxation toward the equilibrium moments, back to
-// populations); drho and (jx, jy) are the node's density deviation and
-// momentum.  Every bulk kernel calls this one function, so all give the
-// same bits.
+// MRT collision on pulled deviations g (moments of the deviation,
+// relaxation toward the equilibrium moments, back to populations); drho and
+// (jx, jy) are the density deviation and momentum.  Every operation is an
+// explicitly rounded IEEE add, multiply or fused multiply-add (a - b as
+// fma(-1, b, a)), so the result does not depend on how the compiler would
+// contract expressions: the lane type V is float (one node) or float2 (two
+// nodes through the paired FP32 instructions of sm_100, each lane rounded
+// as the float form), and every kernel gives the same bits.
+template <class V>
+struct Lanes;
+template <>
+struct Lanes<float> {
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float k(float x) { return x; }
+};
+template <>
+struct Lanes<float2> {
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+    static __device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+    static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+    static __device__ __forceinline__ float2 k(float x) { return make_float2(x, x); }
+};
+template <class V>
+__device__ __forceinline__ void collide_lanes(const V g[9], const FusedConsts& c, V o[9], V& drho, V& jx, V& jy) {
+    using L = Lanes<V>;
+    const V m1k = L::k(-1.0f);
+    auto sub = [&](V a, V b) { return L::fma(m1k, b, a); };
+    // moments of the deviation
+    const V p13 = L::add(g[1], g[3]), p24 = L::add(g[2], g[4]);
+    const V p57 = L::add(g[5], g[7]), p68 = L::add(g[6], g[8]);
+    const V s14 = L::add(p13, p24), s58 = L::add(p57, p68);
+    const V m0 = L::add(L::add(g[0], s14), s58);
+    const V m1 = L::fma(L::k(2.0f), s58, sub(L::mul(L::k(-4.0f), g[0]), s14));
+    const V m2 = L::fma(L::k(4.0f), g[0], L::fma(L::k(-2.0f), s14, s58));
+    const V d13 = sub(g[1], g[3]), d24 = sub(g[2], g[4]);
+    const V a5 = sub(g[5], g[7]), a6 = sub(g[6], g[8]);
+    jx = sub(L::add(d13, a5), a6);
+    const V m4 = sub(L::fma(L::k(-2.0f), d13, a5), a6);
+    jy = L::add(L::add(d24, a5), a6);
+    const V m6 = L::add(L::fma(L::k(-2.0f), d24, a5), a6);
+    const V m7 = sub(p13, p24);
+    const V m8 = sub(p57, p68);
+    // relaxation toward the equilibrium moments (solution.f90:616-646)
+    drho = L::add(m0, L::k(c.wm1));
+    const V jxx = L::mul(jx, jx), jyy = L::mul(jy, jy), q = L::add(jxx, jyy);
+    const V t1 = L::fma(L::k(3.0f), q, L::fma(L::k(-2.0f), drho, L::k(-c.k1)));
+    const V e1 = L::fma(L::k(c.s1), sub(t1, m1), m1);
+    const V t2 = L::fma(L::k(-3.0f), q, L::add(drho, L::k(c.k2)));
+    const V e2 = L::fma(L::k(c.s2), sub(t2, m2), m2);
+    const V e4 = L::fma(L::k(-c.s4), L::add(jx, m4), m4);
+    const V e6 = L::fma(L::k(-c.s6), L::add(jy, m6), m6);
+    const V e7 = L::fma(L::k(c.s7), sub(sub(jxx, jyy), m7), m7);
+    const V e8 = L::fma(L::k(c.s8), sub(L::mul(jx, jy), m8), m8);
+    // back to populations: M^-1 = M^T diag(1/9, 1/36, 1/36, 1/6, 1/12, 1/6, 1/12, 1/4, 1/4)
+    const V b0 = L::mul(m0, L::k(1.0f / 9.0f));
+    const V b1 = L::mul(e1, L::k(1.0f / 36.0f)), b2 = L::mul(e2, L::k(1.0f / 36.0f));
+    const V b3 = L::mul(jx, L::k(1.0f / 6.0f)), b4 = L::mul(e4, L::k(1.0f / 12.0f));
+    const V b5 = L::mul(jy, L::k(1.0f / 6.0f)), b6 = L::mul(e6, L::k(1.0f / 12.0f));
+    const V b7 = L::mul(e7, L::k(0.25f)), b8 = L::mul(e8, L::k(0.25f));
+    const V rA = L::fma(L::k(-2.0f), b2, sub(b0, b1));   // axis populations, common part
+    const V rD = L::add(L::fma(L::k(2.0f), b1, b0), b2);  // diagonal populations, common part
+    const V x34 = L::fma(L::k(-2.0f), b4, b3), y56 = L::fma(L::k(-2.0f), b6, b5);
+    const V xd = L::add(b3, b4), yd = L::add(b5, b6);
+    o[0] = L::fma(L::k(4.0f), b2, L::fma(L::k(-4.0f), b1, b0));
+    o[1] = L::add(L::add(rA, x34), b7);
+    o[2] = sub(L::add(rA, y56), b7);
+    o[3] = L::add(sub(rA, x34), b7);
+    o[4] = sub(sub(rA, y56), b7);
+    o[5] = L::add(L::add(L::add(rD, xd), yd), b8);
+    o[6] = sub(L::add(sub(rD, xd), yd), b8);
+    o[7] = L::add(sub(sub(rD, xd), yd), b8);
+    o[8] = sub(sub(L::add(rD, xd), yd), b8);
+}
 __device__ __forceinline__ void fused_collide(const float g[9], const FusedConsts& c, float o[9], float& drho,
                                               float& jx, float& jy) {
-    // moments of the deviation
-    const float s14 = (g[1] + g[3]) + (g[2] + g[4]);
-    const float s58 = (g[5] + g[7]) + (g[6] + g[8]);
-    const float m0 = (g[0] + s14) + s58;
-    const float m1 = -4.0f * g[0] - s14 + 2.0f * s58;
-    const float m2 = 4.0f * g[0] - 2.0f * s14 + s58;
-    const float d13 = g[1] - g[3], d24 = g[2] - g[4];
-    const float a5 = g[5] - g[7], a6 = g[6] - g[8];
-    jx = d13 + a5 - a6;
-    const float m4 = -2.0f * d13 + a5 - a6;
-    jy = d24 + a5 + a6;
-    const float m6 = -2.0f * d24 + a5 + a6;
-    const float m7 = (g[1] + g[3]) - (g[2] + g[4]);
-    const float m8 = (g[5] + g[7]) - (g[6] + g[8]);
-    // relaxation toward the equilibrium moments (solution.f90:616-646)
-    drho = m0 + c.wm1;
-    const float jxx = jx * jx, jyy = jy * jy;
-    const float e1 = m1 + c.s1 * ((-2.0f * drho + 3.0f * (jxx + jyy) - c.k1) - m1);
-    const float e2 = m2 + c.s2 * ((drho - 3.0f * (jxx + jyy) + c.k2) - m2);
-    const float e4 = m4 + c.s4 * (-jx - m4);
-    const float e6 = m6 + c.s6 * (-jy - m6);
-    const float e7 = m7 + c.s7 * ((jxx - jyy) - m7);
-    const float e8 = m8 + c.s8 * (jx * jy - m8);
-    // back to populations: M^-1 = M^T diag(1/9, 1/36, 1/36, 1/6, 1/12, 1/6, 1/12, 1/4, 1/4)
-    const float b0 = m0 * (1.0f / 9.0f);
-    const float b1 = e1 * (1.0f / 36.0f), b2 = e2 * (1.0f / 36.0f);
-    const float b3 = jx * (1.0f / 6.0f), b4 = e4 * (1.0f / 12.0f);
-    const float b5 = jy * (1.0f / 6.0f), b6 = e6 * (1.0f / 12.0f);
-    const float b7 = e7 * 0.25f, b8 = e8 * 0.25f;
-    const float rA = b0 - b1 - 2.0f * b2;       // axis populations, common part
-    const float rD = b0 + 2.0f * b1 + b2;       // diagonal populations, common part
-    const float x34 = b3 - 2.0f * b4, y56 = b5 - 2.0f * b6;
-    const float xd = b3 + b4, yd = b5 + b6;
-    o[0] = b0 - 4.0f * b1 + 4.0f * b2;
-    o[1] = rA + x34 + b7;
-    o[2] = rA + y56 - b7;
-    o[3] = rA - x34 + b7;
-    o[4] = rA - y56 - b7;
-    o[5] = rD + xd + yd + b8;
-    o[6] = rD - xd + yd - b8;
-    o[7] = rD - xd - yd + b8;
-    o[8] = rD + xd - yd - b8;
+    collide_lanes<float>(g, c, o, drho, jx, jy);
 }
 
 // One interior node (i, j); nodes of the band list are left to the band
@@ -251,7 +280,7 @@ constexpr int PASS_CH = (PASS_BOXH * PASS_BOXW + 31) & ~31;   // floats per inpu
 constexpr int PASS_MW = PASS_TX + 2, PASS_MH = PASS_TY + 2;   // R1
 constexpr int PASS_MCH = PASS_MH * PASS_MW;
 constexpr size_t PASS_SMEM = (size_t)(9 * PASS_CH + 9 * PASS_MCH) * sizeof(float) + 128;
-static_assert(PASS_TX % 4 == 0, "tile columns start on 16-byte boundaries");
+static_assert(PASS_TX % 64 == 0, "tiles start on 16-byte boundaries and on band-bit words");
 static_assert(PASS_BOXW <= 256 && PASS_BOXH <= 256, "tensor-map box extents");
 
 template <bool NEAR>
@@ -310,15 +339,103 @@ __device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs&
     }
 }
 
+// A pair of horizontally adjacent values from shared memory at an even
+// base index plus OFF: one 8-byte load when OFF is even, two otherwise.
+template <int OFF>
+__device__ __forceinline__ float2 lds_pair(const float* S, int even_base) {
+    if (OFF % 2 == 0) return *reinterpret_cast<const float2*>(S + even_base + OFF);
+    return make_float2(S[even_base + OFF], S[even_base + OFF + 1]);
+}
+
+// Far tile, two nodes per thread through the paired FP32 instructions:
+// every R1 node is interior and off step n's band, every tile node interior.
+// Column pairs start at even offsets, so the pulls of the six directions
+// with ex != 0, the step n + 1 stores and the step n + 2 stores are 8-byte
+// accesses.  The tile's band bits of step n + 1 (8 rows x 2 words) are
+// staged in shared memory while the tensor loads are in flight.
+__device__ __forceinline__ void pass_tile_far2(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin,
+                                               float* Smid, uint64_t* bar, unsigned* sbits) {
+    const int tx = t % a.ntx, ty = t / a.ntx;
+    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, (uint32_t)(9 * PASS_BOXH * PASS_BOXW * sizeof(float)));
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * PASS_CH, tm, x0 - 4, y0 - 2, k, bar);
+    }
+    if (threadIdx.x < 2 * PASS_TY) {
+        const long long w = ((long long)(y0 + (threadIdx.x >> 1)) * a.pitch + x0) >> 5;
+        sbits[threadIdx.x] = __ldg(a.bits1 + w + (threadIdx.x & 1));
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
+        mbar_wait(bar, 0);   // let a late copy land before the block exits
+        return;
+    }
+    const FusedConsts c = a.c;
+    // step n + 1 on R1: pair u = (mr, mc / 2), nodes (x0 - 1 + mc, y0 - 1 + mr)
+    // and the next column; box cell (mr + 1, mc + 3)
+    for (int u = threadIdx.x; u < PASS_MH * PASS_MW / 2; u += PASS_THREADS) {
+        const int mr = u / (PASS_MW / 2), mc = 2 * (u % (PASS_MW / 2));
+        float2 g[9], o[9], drho, jx, jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const int base = k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc;
+            switch (ex(k)) {   // ex is a constant per unrolled k
+            case 1: g[k] = lds_pair<2>(Sin, base); break;
+            case -1: g[k] = lds_pair<4>(Sin, base); break;
+            default: g[k] = lds_pair<3>(Sin, base); break;
+            }
+        }
+        collide_lanes<float2>(g, c, o, drho, jx, jy);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * PASS_MCH + mr * PASS_MW + mc) = o[k];
+    }
+    __syncthreads();
+    // step n + 2 on the tile: pair (rr, cc / 2), nodes (x0 + cc, y0 + rr) and
+    // the next column; R1 cell (rr + 1, cc + 1)
+    for (int u = threadIdx.x; u < PASS_TY * PASS_TX / 2; u += PASS_THREADS) {
+        const int rr = u / (PASS_TX / 2), cc = 2 * (u % (PASS_TX / 2));
+        const unsigned word = sbits[rr * 2 + (cc >> 5)];
+        const unsigned b0 = (word >> (cc & 31)) & 1u, b1 = (word >> ((cc & 31) + 1)) & 1u;
+        if (b0 & b1) continue;   // both band nodes of step n + 1
+        float2 g[9], o[9], drho, jx, jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const int base = k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc;
+            switch (ex(k)) {
+            case 1: g[k] = lds_pair<0>(Smid, base); break;
+            case -1: g[k] = lds_pair<2>(Smid, base); break;
+            default: g[k] = lds_pair<1>(Smid, base); break;
+            }
+        }
+        collide_lanes<float2>(g, c, o, drho, jx, jy);
+        float* q = a.Q + (long long)(y0 + rr) * a.pitch + x0 + cc;
+        if (!(b0 | b1)) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(q + k * a.plane) = o[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                if (!b0) q[k * a.plane] = o[k].x;
+                if (!b1) q[k * a.plane + 1] = o[k].y;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(PASS_THREADS, 4) pass_far_kernel(const __grid_constant__ CUtensorMap tm,
                                                                    const PassArgs a) {
     extern __shared__ unsigned char pass_raw[];
     __shared__ uint64_t bar;
+    __shared__ unsigned sbits[2 * PASS_TY];
     const int t = blockIdx.x;
     if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) || __ldg(a.flags0 + t)) return;   // a near tile
     if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
-    pass_tile<false>(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
+    pass_tile_far2(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar, sbits);
 }
 
 __global__ void __launch_bounds__(PASS_THREADS, 4) pass_near_kernel(const __grid_constant__ CUtensorMap tm,

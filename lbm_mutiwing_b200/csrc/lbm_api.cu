@@ -773,6 +773,9 @@ void drop_graphs(LbmHandle* h) {
 // last step waits for the geometry it built for the steps after the graph.
 int build_graph(LbmHandle* h, int c, int a, int gs, bool pass) {
     DeviceLock lock(g_device_mutex);
+    // the capture re-records the geometry events: wait for pending builds
+    // now, while the events still name them
+    wait_pending(h);
     const int saved_c = h->cur, saved_a = h->alt, saved_g = h->gset, saved_last = h->last_gset;
     bool saved_pending[GEO_SETS];
     std::copy(h->pending, h->pending + GEO_SETS, saved_pending);
