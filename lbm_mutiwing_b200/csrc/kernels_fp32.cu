@@ -274,7 +274,7 @@ int fused_tensor_map(const DevState& d, const float* base, void* out) {
 // second step's band re-collision and far field write them.  Every node is
 // computed by fused_collide, as in the one-step kernels, so a pass gives the
 // bits of two steps.
-constexpr int PASS_THREADS = 256;
+constexpr int PASS_THREADS = 352;   // one column pair of R1 per thread (10 x 33 pairs)
 constexpr int PASS_BOXW = PASS_TX + 8, PASS_BOXH = PASS_TY + 4;
 constexpr int PASS_CH = (PASS_BOXH * PASS_BOXW + 31) & ~31;   // floats per input plane, 128-byte multiple
 constexpr int PASS_MW = PASS_TX + 2, PASS_MH = PASS_TY + 2;   // R1

@@ -164,10 +164,10 @@ struct LbmHandle {
     std::string err;
     DevState d{};
     FusedConsts fc{};
-    // fused path: three plane copies; a step goes from planes[cur] to
-    // planes[alt] and swaps them, a pass writes its second step to the third
-    // copy (its first step's band and border values to planes[alt]), which
-    // becomes cur
+    // fused path: three plane copies; a step or a pass goes from planes[cur]
+    // to the third copy, which becomes cur (a pass writes its first step's
+    // band and border values to planes[alt], which never changes), so cur
+    // alternates between two copies
     int cur = 0, alt = 1;
     float* planes[3] = {nullptr, nullptr, nullptr};
     GeoSet geo[GEO_SETS];           // geometry sets (the plain path uses set 0)
@@ -311,7 +311,7 @@ DevState current(const LbmHandle* h) {
     DevState d = h->d;
     if (d.precision != 0) {
         d.gA = h->planes[h->cur];
-        d.gB = h->planes[h->alt];
+        d.gB = h->planes[3 - h->cur - h->alt];
         use_geo(d, h->geo[h->gset]);
     }
     return d;
@@ -641,7 +641,7 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
             cudaStreamWaitEvent(h->s_main, h->ev_fact[s], 0);
             h->pending[s] = false;
         }
-        std::swap(h->cur, h->alt);
+        h->cur = third_planes(h);
         h->last_gset = h->gset;
         h->gset = s1;
     }
@@ -885,17 +885,19 @@ constexpr int BV_PLAIN = 0, BV_SECOND_LAST = 2, BV_LAST = 4, BV_AHEAD = 6, BV_CO
 constexpr int BATCH_SLOT_ITEMS = 4;   // per-slot items per thread in packed launches
 constexpr int64_t GRAPH_PAIR_MIN = 8;  // steady steps ahead before a step pair is captured
 
-// Packed steps alternate between the handle's two plane copies (cur, alt)
-// and two of its geometry sets (gset, gset + 1), each step building the next
-// step's geometry into the other set.
+// Packed steps alternate between the handle's current plane copy and its
+// third copy (as single steps do) and between two of its geometry sets
+// (gset, gset + 1), each step building the next step's geometry into the
+// other set.
 int batch_set(const LbmHandle* h, int ph) { return (h->gset + (ph & 1)) % GEO_SETS; }
 
 void batch_variants(LbmHandle* h, bool want_fields, bool want_err, DevState* out) {
     for (int ph = 0; ph < 2; ++ph) {
         DevState d = h->d;
         const int g = batch_set(h, ph);
-        d.gA = h->planes[ph ? h->alt : h->cur];
-        d.gB = h->planes[ph ? h->cur : h->alt];
+        const int third = third_planes(h);
+        d.gA = h->planes[ph ? third : h->cur];
+        d.gB = h->planes[ph ? h->cur : third];
         use_geo(d, h->geo[g]);
         d.tile_flags = nullptr;   // no passes in packed steps
         d.diag = 0;
@@ -1332,13 +1334,13 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     if (fused && n_steps > 0 && !have_geo) prime_geometry(h);
     int64_t n = 0;
     if (passes) {
-        // the pass graphs this state can reach (the current planes move to
-        // the third copy and back, the sets by two, the overlay copy stays)
-        // are built by the first call that replays one, so later calls
-        // capture nothing
+        // every pass graph a handle can meet (the current planes alternate
+        // between two copies, the overlay copy stays, four geometry sets) is
+        // built by the first call that replays one, so later calls capture
+        // nothing
         if (graphs && n + 2 <= n_steps - 2)
-            for (int q = 0; q < 4; ++q) {
-                const int c = (q & 1) ? third_planes(h) : h->cur, g = (h->gset + (q & 2)) % GEO_SETS;
+            for (int q = 0; q < 2 * GEO_SETS; ++q) {
+                const int c = (q & 1) ? third_planes(h) : h->cur, g = (h->gset + q / 2) % GEO_SETS;
                 if (!h->pexec[c][h->alt][g] && build_graph(h, c, h->alt, g, true)) return -1;
             }
         for (; n + 2 <= n_steps - 2; n += 2) {
@@ -1698,7 +1700,7 @@ int lbm_batch_step(LbmBatch* b, int32_t n, LbmHandle* const* hs, const int64_t* 
         h->geo_ready = -1;
         int rc = 0;
         if (ns > 0) {
-            if (ns & 1) std::swap(h->cur, h->alt);
+            if (ns & 1) h->cur = third_planes(h);
             h->last_gset = batch_set(h, (int)((ns - 1) & 1));
             h->gset = batch_set(h, (int)(ns & 1));
             if (want_err) {
@@ -1991,7 +1993,7 @@ int lbm_move_mesh(LbmHandle* h, int32_t dr) {
         launch_plain_shift(h->d, dr, h->s_main);
     } else {
         launch_fused_shift(current(h), dr, h->s_main);
-        std::swap(h->cur, h->alt);
+        h->cur = third_planes(h);
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s_main));
