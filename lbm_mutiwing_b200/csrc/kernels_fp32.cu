@@ -274,14 +274,19 @@ int fused_tensor_map(const DevState& d, const float* base, void* out) {
 // second step's band re-collision and far field write them.  Every node is
 // computed by fused_collide, as in the one-step kernels, so a pass gives the
 // bits of two steps.
-constexpr int PASS_THREADS = 352;   // one column pair of R1 per thread (10 x 33 pairs)
+// one column pair of R1 per thread, in whole warps
+constexpr int PASS_THREADS = ((PASS_TY + 2) * (PASS_TX + 2) / 2 + 31) / 32 * 32;
+constexpr int PASS_WORDS = PASS_TX / 32;   // band-bit words of a tile row
 constexpr int PASS_BOXW = PASS_TX + 8, PASS_BOXH = PASS_TY + 4;
 constexpr int PASS_CH = (PASS_BOXH * PASS_BOXW + 31) & ~31;   // floats per input plane, 128-byte multiple
 constexpr int PASS_MW = PASS_TX + 2, PASS_MH = PASS_TY + 2;   // R1
 constexpr int PASS_MCH = PASS_MH * PASS_MW;
 constexpr size_t PASS_SMEM = (size_t)(9 * PASS_CH + 9 * PASS_MCH) * sizeof(float) + 128;
-static_assert(PASS_TX % 64 == 0, "tiles start on 16-byte boundaries and on band-bit words");
+static_assert(PASS_TX % 32 == 0, "tiles start on 16-byte boundaries and on band-bit words");
 static_assert(PASS_BOXW <= 256 && PASS_BOXH <= 256, "tensor-map box extents");
+// resident blocks per SM that the shared memory allows (the launch bounds
+// then keep the registers within the same count)
+constexpr int PASS_MINB = (227 * 1024) / (int)(PASS_SMEM + 1024) < 8 ? (227 * 1024) / (int)(PASS_SMEM + 1024) : 8;
 
 template <bool NEAR>
 __device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin, float* Smid,
@@ -347,98 +352,127 @@ __device__ __forceinline__ float2 lds_pair(const float* S, int even_base) {
     return make_float2(S[even_base + OFF], S[even_base + OFF + 1]);
 }
 
-// Far tile, two nodes per thread through the paired FP32 instructions:
+// Far tiles, two nodes per thread through the paired FP32 instructions:
 // every R1 node is interior and off step n's band, every tile node interior.
 // Column pairs start at even offsets, so the pulls of the six directions
 // with ex != 0, the step n + 1 stores and the step n + 2 stores are 8-byte
-// accesses.  The tile's band bits of step n + 1 (8 rows x 2 words) are
-// staged in shared memory while the tensor loads are in flight.
-__device__ __forceinline__ void pass_tile_far2(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin,
-                                               float* Smid, uint64_t* bar, unsigned* sbits) {
-    const int tx = t % a.ntx, ty = t / a.ntx;
-    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+// accesses.  A block takes PASS_TPC consecutive tiles (near tiles among them
+// are skipped): once the first step of a tile has read the staged planes,
+// thread 0 issues the next tile's tensor loads into the same buffer, so they
+// fly while the second step runs.  The band bits of step n + 1 of each tile
+// (PASS_TY rows x PASS_WORDS words) are staged beside its loads.
+#ifndef LBM_PASS_TPC
+#define LBM_PASS_TPC 2
+#endif
+constexpr int PASS_TPC = LBM_PASS_TPC;
+
+__device__ __forceinline__ bool pass_far_tile(const PassArgs& a, int t) {
+    return t < a.ntx * a.nty && !pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) && !__ldg(a.flags0 + t);
+}
+
+// Thread 0 arms the barrier and issues tile t's loads; the first
+// PASS_WORDS * PASS_TY threads stage its band bits.
+__device__ __forceinline__ void pass_issue_far(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin,
+                                               uint64_t* bar, unsigned* sbits) {
+    const int x0 = (t % a.ntx) * PASS_TX, y0 = 1 + (t / a.ntx) * PASS_TY;
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
         mbar_arrive_expect_tx(bar, (uint32_t)(9 * PASS_BOXH * PASS_BOXW * sizeof(float)));
 #pragma unroll
         for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * PASS_CH, tm, x0 - 4, y0 - 2, k, bar);
     }
-    if (threadIdx.x < 2 * PASS_TY) {
-        const long long w = ((long long)(y0 + (threadIdx.x >> 1)) * a.pitch + x0) >> 5;
-        sbits[threadIdx.x] = __ldg(a.bits1 + w + (threadIdx.x & 1));
-    }
-    __syncthreads();
-    const bool ok = mbar_wait(bar, 0);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
-        mbar_wait(bar, 0);   // let a late copy land before the block exits
-        return;
-    }
-    const FusedConsts c = a.c;
-    // step n + 1 on R1: pair u = (mr, mc / 2), nodes (x0 - 1 + mc, y0 - 1 + mr)
-    // and the next column; box cell (mr + 1, mc + 3)
-    for (int u = threadIdx.x; u < PASS_MH * PASS_MW / 2; u += PASS_THREADS) {
-        const int mr = u / (PASS_MW / 2), mc = 2 * (u % (PASS_MW / 2));
-        float2 g[9], o[9], drho, jx, jy;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const int base = k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc;
-            switch (ex(k)) {   // ex is a constant per unrolled k
-            case 1: g[k] = lds_pair<2>(Sin, base); break;
-            case -1: g[k] = lds_pair<4>(Sin, base); break;
-            default: g[k] = lds_pair<3>(Sin, base); break;
-            }
-        }
-        collide_lanes<float2>(g, c, o, drho, jx, jy);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * PASS_MCH + mr * PASS_MW + mc) = o[k];
-    }
-    __syncthreads();
-    // step n + 2 on the tile: pair (rr, cc / 2), nodes (x0 + cc, y0 + rr) and
-    // the next column; R1 cell (rr + 1, cc + 1)
-    for (int u = threadIdx.x; u < PASS_TY * PASS_TX / 2; u += PASS_THREADS) {
-        const int rr = u / (PASS_TX / 2), cc = 2 * (u % (PASS_TX / 2));
-        const unsigned word = sbits[rr * 2 + (cc >> 5)];
-        const unsigned b0 = (word >> (cc & 31)) & 1u, b1 = (word >> ((cc & 31) + 1)) & 1u;
-        if (b0 & b1) continue;   // both band nodes of step n + 1
-        float2 g[9], o[9], drho, jx, jy;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const int base = k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc;
-            switch (ex(k)) {
-            case 1: g[k] = lds_pair<0>(Smid, base); break;
-            case -1: g[k] = lds_pair<2>(Smid, base); break;
-            default: g[k] = lds_pair<1>(Smid, base); break;
-            }
-        }
-        collide_lanes<float2>(g, c, o, drho, jx, jy);
-        float* q = a.Q + (long long)(y0 + rr) * a.pitch + x0 + cc;
-        if (!(b0 | b1)) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(q + k * a.plane) = o[k];
-        } else {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                if (!b0) q[k * a.plane] = o[k].x;
-                if (!b1) q[k * a.plane + 1] = o[k].y;
-            }
-        }
+    if (threadIdx.x < PASS_WORDS * PASS_TY) {
+        const long long w = ((long long)(y0 + threadIdx.x / PASS_WORDS) * a.pitch + x0) >> 5;
+        sbits[threadIdx.x] = __ldg(a.bits1 + w + threadIdx.x % PASS_WORDS);
     }
 }
 
-__global__ void __launch_bounds__(PASS_THREADS, 4) pass_far_kernel(const __grid_constant__ CUtensorMap tm,
-                                                                   const PassArgs a) {
+__global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                            const PassArgs a) {
     extern __shared__ unsigned char pass_raw[];
     __shared__ uint64_t bar;
-    __shared__ unsigned sbits[2 * PASS_TY];
-    const int t = blockIdx.x;
-    if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) || __ldg(a.flags0 + t)) return;   // a near tile
-    if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
+    __shared__ unsigned sbits[2][PASS_WORDS * PASS_TY];
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
-    pass_tile_far2(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar, sbits);
+    float* Smid = Sin + 9 * PASS_CH;
+    const int first = blockIdx.x * PASS_TPC, last = first + PASS_TPC;
+    int t = first;
+    while (t < last && !pass_far_tile(a, t)) ++t;
+    if (t >= last) return;   // near tiles only
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    pass_issue_far(&tm, a, t, Sin, &bar, sbits[0]);
+    __syncthreads();
+    const FusedConsts& c = a.c;
+    for (int it = 0; t < last; ++it) {
+        if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
+        const int tx = t % a.ntx, ty = t / a.ntx;
+        const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+        int tn = t + 1;   // the block's next far tile (its flag loads overlap the wait)
+        while (tn < last && !pass_far_tile(a, tn)) ++tn;
+        const bool ok = mbar_wait(&bar, it & 1);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
+            mbar_wait(&bar, it & 1);   // let a late copy land before the block exits
+            return;
+        }
+        // step n + 1 on R1: pair u = (mr, mc / 2), nodes (x0 - 1 + mc, y0 - 1 + mr)
+        // and the next column; box cell (mr + 1, mc + 3)
+        for (int u = threadIdx.x; u < PASS_MH * PASS_MW / 2; u += PASS_THREADS) {
+            const int mr = u / (PASS_MW / 2), mc = 2 * (u % (PASS_MW / 2));
+            float2 g[9], o[9], drho, jx, jy;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const int base = k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc;
+                switch (ex(k)) {   // ex is a constant per unrolled k
+                case 1: g[k] = lds_pair<2>(Sin, base); break;
+                case -1: g[k] = lds_pair<4>(Sin, base); break;
+                default: g[k] = lds_pair<3>(Sin, base); break;
+                }
+            }
+            collide_lanes<float2>(g, c, o, drho, jx, jy);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * PASS_MCH + mr * PASS_MW + mc) = o[k];
+        }
+        __syncthreads();   // the staged planes are read: the next tile's loads may land
+        if (tn < last) {
+            if (threadIdx.x == 0) fence_async_smem();
+            pass_issue_far(&tm, a, tn, Sin, &bar, sbits[(it + 1) & 1]);
+        }
+        // step n + 2 on the tile: pair (rr, cc / 2), nodes (x0 + cc, y0 + rr)
+        // and the next column; R1 cell (rr + 1, cc + 1)
+        const unsigned* bits = sbits[it & 1];
+        for (int u = threadIdx.x; u < PASS_TY * PASS_TX / 2; u += PASS_THREADS) {
+            const int rr = u / (PASS_TX / 2), cc = 2 * (u % (PASS_TX / 2));
+            const unsigned word = bits[rr * PASS_WORDS + (cc >> 5)];
+            const unsigned b0 = (word >> (cc & 31)) & 1u, b1 = (word >> ((cc & 31) + 1)) & 1u;
+            if (b0 & b1) continue;   // both band nodes of step n + 1
+            float2 g[9], o[9], drho, jx, jy;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const int base = k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc;
+                switch (ex(k)) {
+                case 1: g[k] = lds_pair<0>(Smid, base); break;
+                case -1: g[k] = lds_pair<2>(Smid, base); break;
+                default: g[k] = lds_pair<1>(Smid, base); break;
+                }
+            }
+            collide_lanes<float2>(g, c, o, drho, jx, jy);
+            float* q = a.Q + (long long)(y0 + rr) * a.pitch + x0 + cc;
+            if (!(b0 | b1)) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(q + k * a.plane) = o[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    if (!b0) q[k * a.plane] = o[k].x;
+                    if (!b1) q[k * a.plane + 1] = o[k].y;
+                }
+            }
+        }
+        __syncthreads();   // R1 values read: the next tile's first step may overwrite them
+        t = tn;
+    }
 }
 
-__global__ void __launch_bounds__(PASS_THREADS, 4) pass_near_kernel(const __grid_constant__ CUtensorMap tm,
+__global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_near_kernel(const __grid_constant__ CUtensorMap tm,
                                                                     const PassArgs a) {
     extern __shared__ unsigned char pass_raw[];
     __shared__ uint64_t bar;
@@ -461,7 +495,8 @@ int pass_tensor_map(const DevState& d, const float* base, void* out) {
 }
 
 void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st) {
-    pass_far_kernel<<<a.ntx * a.nty, PASS_THREADS, PASS_SMEM, st>>>(*reinterpret_cast<const CUtensorMap*>(tmap), a);
+    pass_far_kernel<<<(a.ntx * a.nty + PASS_TPC - 1) / PASS_TPC, PASS_THREADS, PASS_SMEM, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(tmap), a);
 }
 
 void launch_pass_near(const PassArgs& a, const void* tmap, cudaStream_t st) {

@@ -688,7 +688,7 @@ void enqueue_pass(LbmHandle* h) {
     pa.band_list = h->geo[g0].tile_list;
     pa.band_n = h->geo[g0].tile_n;
     pa.nborder = h->nborder;
-    pa.band_cap = std::min(h->d.pass_ntx * h->d.pass_nty, 4 * std::max(1, h->d.nseg));
+    pa.band_cap = std::min(h->d.pass_ntx * h->d.pass_nty, PASS_TILES_PER_SEGMENT * std::max(1, h->d.nseg));
     pa.nx = h->d.nx;
     pa.ny = h->d.ny;
     pa.pitch = h->d.pitch;

@@ -37,7 +37,16 @@ void launch_fused_import(const DevState& d, const double* f, float* g, cudaStrea
 // ty) covers the interior nodes [PASS_TX tx, PASS_TX tx + PASS_TX - 1] x
 // [1 + PASS_TY ty, PASS_TY (ty + 1)]; its first step needs the tile and one
 // ring of neighbours (R1), its pulls a second ring.
-constexpr int PASS_TX = 64, PASS_TY = 8;
+#ifndef LBM_PASS_TX
+#define LBM_PASS_TX 64
+#endif
+#ifndef LBM_PASS_TY
+#define LBM_PASS_TY 8
+#endif
+constexpr int PASS_TX = LBM_PASS_TX, PASS_TY = LBM_PASS_TY;
+// flagged tiles a support box can touch: its 6 nodes and the ring either
+// side span 8 nodes in each direction
+constexpr int PASS_TILES_PER_SEGMENT = ((8 + PASS_TX - 1) / PASS_TX + 1) * ((8 + PASS_TY - 1) / PASS_TY + 1);
 inline int pass_tiles_x(int nx) { return (nx + PASS_TX - 1) / PASS_TX; }
 inline int pass_tiles_y(int ny) { return (ny - 2 + PASS_TY - 1) / PASS_TY; }
 // whether R1 of tile (tx, ty) holds a node of the lattice border
