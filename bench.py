@@ -200,12 +200,25 @@ def ncu_traffic(workload_name, kernel):
 
 
 # Kernels of one step with wings:
-#   fused FP32: geometry, claim, count, scan, list, assemble, factor (the next
-#               step's geometry) | rhs, solve, spread, close | bulk | far field
+#   fused FP32 single step: geometry, claim, count, scan, list, assemble,
+#               factor (a later step's geometry) | rhs, solve, spread, close |
+#               bulk | far field
+#   fused FP32 two-step pass: the geometry of two later steps (2 x 7) | two
+#               chains (2 x 4) | two far fields | ring | near tiles | far tiles
 #   plain FP64: geometry, claim, count, scan, list, assemble, factor, stream,
 #               moments, ustar, rhs, solve, spread, finish, forces, collide,
 #               far field, advance
 KERNELS_PER_STEP = {"fp32": 13, "fp64": 18}
+KERNELS_PER_PASS = 27
+
+
+def kernels_in_call(k, precision):
+    """Kernels one lbm_step call of k steps launches: on the FP32 path all
+    but the last two steps run as passes."""
+    if precision != "fp32":
+        return k * KERNELS_PER_STEP["fp64"]
+    passes = max(0, (k - 2) // 2)
+    return passes * KERNELS_PER_PASS + (k - 2 * passes) * KERNELS_PER_STEP["fp32"]
 
 
 def config_of(ep, storage, world):
@@ -539,7 +552,7 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "segment_steps": SEG},
             "clocks": clk.summary(),
-            "gpu_launches": K * len(reps) * KERNELS_PER_STEP[args.precision]}
+            "gpu_launches": len(reps) * kernels_in_call(K, args.precision)}
     if plain:
         line["plain_fp64"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
