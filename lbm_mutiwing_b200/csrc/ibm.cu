@@ -711,16 +711,29 @@ __global__ void __launch_bounds__(FINISH_THREADS) ibm_finish_kernel(DevState d) 
 // through L2.
 __device__ __forceinline__ void force_row_body(const DevState& d) {
     const int nblocks = (int)max(1LL, ((long long)d.band_cap + FINISH_THREADS - 1) / FINISH_THREADS);
-    constexpr int CHUNK = 16;   // block partials staged per pass
+    constexpr int STAGE = 1536;   // partial sums staged per pass (12 KB)
     __shared__ double fm[MAX_WINGS][3];
     __shared__ double red[8][2];
-    __shared__ double part[CHUNK * MAX_WINGS * 3];
+    __shared__ double part[STAGE];
     const int tid = threadIdx.x, W = d.wing_count;
-    // partials are loaded in parallel, then added in block order
+    // partials are loaded in parallel (every load of a pass issued before
+    // any is used), then added in block order
+    const int per = W > 0 ? STAGE / (3 * W) : nblocks;   // blocks per pass (at least 32: W <= 16)
     double v = 0.0;
-    for (int k0 = 0; k0 < nblocks; k0 += CHUNK) {
-        const int nk = min(CHUNK, nblocks - k0);
-        for (int t = tid; t < nk * 3 * W; t += blockDim.x) part[t] = __ldcg(d.force_part + (long long)k0 * W * 3 + t);
+    for (int k0 = 0; k0 < nblocks; k0 += per) {
+        const int nk = min(per, nblocks - k0), n = nk * 3 * W;
+        const double* src = d.force_part + (long long)k0 * W * 3;
+        double r[STAGE / 256];
+#pragma unroll
+        for (int q = 0; q < STAGE / 256; ++q) {
+            const int t = tid + q * 256;
+            r[q] = t < n ? __ldcg(src + t) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < STAGE / 256; ++q) {
+            const int t = tid + q * 256;
+            if (t < n) part[t] = r[q];
+        }
         __syncthreads();
         if (tid < 3 * W)
             for (int k = 0; k < nk; ++k) v += part[k * 3 * W + tid];
