@@ -23,7 +23,9 @@ roofline: the dominant kernel's algorithmic traffic over its mean CUDA-event
          two-step pass's far-tile kernel, 9 reads of step n + 9 writes of
          step n + 2, 4 bytes each, per node of the far tiles it processed
          (64 x 8 nodes a tile); whole_step_frac counts 36 bytes per node and
-         step (a pass moves each node's distributions once for two steps).
+         step (a pass moves each node's distributions once for two steps),
+         one_step_equivalent_frac 72 (the bytes a one-step scheme moves at
+         the same step rate).
 The distribution planes (2 x 288 MB) exceed the 126 MB L2, so no separate L2
 flush is needed between steps.
 
@@ -213,11 +215,11 @@ KERNELS_PER_PASS = 27
 
 
 def kernels_in_call(k, precision):
-    """Kernels one lbm_step call of k steps launches: on the FP32 path all
-    but the last two steps run as passes."""
+    """Kernels one lbm_step call of k steps (no field request) launches: on
+    the FP32 path every step runs in a pass but one of an odd count."""
     if precision != "fp32":
         return k * KERNELS_PER_STEP["fp64"]
-    passes = max(0, (k - 2) // 2)
+    passes = k // 2
     return passes * KERNELS_PER_PASS + (k - 2 * passes) * KERNELS_PER_STEP["fp32"]
 
 
@@ -537,7 +539,9 @@ def run_ours(args):
             "frac": achieved / peak, "peak_source": peak_kind,
             "traffic": ncu_traffic(ep.name, kernel) if prec == api.PRECISION_FP32 else None,
             "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": kernel_ms,
-            "whole_step_frac": step_bytes * K / (ms / 1e3) / 1e9 / peak}
+            "whole_step_frac": step_bytes * K / (ms / 1e3) / 1e9 / peak,
+            "one_step_equivalent_frac": (72 if prec == api.PRECISION_FP32 else 144) * interior * K
+                                        / (ms / 1e3) / 1e9 / peak}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms / K, "timed_repeats": len(reps),

@@ -663,13 +663,16 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
 //   s_near  near tiles (P and O -> Q), after the first chain and far field
 //   aux     the geometry of steps n + 2 and n + 3
 // The pass ends when all are done (the next pass reads all of them).
-void enqueue_pass(LbmHandle* h) {
+// diag_last: the pass ends the call, so its second step computes the
+// no-slip residual diagnostic (lbm_ibm_residual).
+void enqueue_pass(LbmHandle* h, bool diag_last = false) {
     wait_pending(h);   // both steps' geometry is complete before the pass starts
     const int g0 = h->gset, g1 = (g0 + 1) % GEO_SETS, g2 = (g0 + 2) % GEO_SETS, g3 = (g0 + 3) % GEO_SETS;
     const int third = third_planes(h);
     float *P = h->planes[h->cur], *O = h->planes[h->alt], *Q = h->planes[third];
     DevState dA = h->d, dB = h->d;
-    dA.diag = dB.diag = 0;
+    dA.diag = 0;
+    dB.diag = diag_last ? 1 : 0;
     dA.write_fields = dB.write_fields = 0;
     dA.gA = P;
     dA.gB = O;
@@ -1326,26 +1329,30 @@ int lbm_step(LbmHandle* h, int64_t first_cycle, int64_t n_steps, double* force_r
     if (n_steps > 0) h->next_cycle = h->geo_ready = -1;   // until the steps are enqueued
     const bool want_fields = (flags & LBM_STEP_FIELDS) != 0;
     const bool want_err = (flags & LBM_STEP_ERR) != 0;
-    // all but the last two steps run as two-step passes (or, without
-    // passes, GRAPH_STEPS single steps) replayed from CUDA graphs; the last
-    // two may write fields or diagnostics and are launched directly
+    // steps run as two-step passes replayed from CUDA graphs, the last pass
+    // launched directly (it computes the residual diagnostic); single steps
+    // remain for an odd count and, when the call writes fields or the
+    // erranalysis pair, for its last two steps.  Without passes, all but
+    // the last two steps replay graphs of GRAPH_STEPS single steps.
     const bool graphs = !h->timing && !(h->cfg.flags & LBM_FLAG_NO_GRAPHS);
     const bool passes = fused && h->pass_ok && !(h->cfg.flags & LBM_FLAG_SINGLE_STEPS);
     if (fused && n_steps > 0 && !have_geo) prime_geometry(h);
     int64_t n = 0;
     if (passes) {
+        const int64_t tail = (want_fields || want_err) ? 2 : (n_steps & 1);   // single steps at the end
         // every pass graph a handle can meet (the current planes alternate
         // between two copies, the overlay copy stays, four geometry sets) is
         // built by the first call that replays one, so later calls capture
         // nothing
-        if (graphs && n + 2 <= n_steps - 2)
+        if (graphs && n_steps - tail >= 4)
             for (int q = 0; q < 2 * GEO_SETS; ++q) {
                 const int c = (q & 1) ? third_planes(h) : h->cur, g = (h->gset + q / 2) % GEO_SETS;
                 if (!h->pexec[c][h->alt][g] && build_graph(h, c, h->alt, g, true)) return -1;
             }
-        for (; n + 2 <= n_steps - 2; n += 2) {
-            if (!graphs) {
-                enqueue_pass(h);
+        for (; n + 2 <= n_steps - tail; n += 2) {
+            const bool last = n + 2 == n_steps;
+            if (!graphs || last) {
+                enqueue_pass(h, last);
                 CK(cudaGetLastError());
                 continue;
             }

@@ -6,9 +6,11 @@ the first step's immersed boundary and far field, every other node of step
 n + 1 is recomputed where it is needed.  Each node is computed by the same
 collision code, so stepping in passes must give, bit for bit, the force
 rows, distributions, running sums and output fields of stepping one step at
-a time (LBM_FLAG_SINGLE_STEPS), for odd and even step counts, calls that
-continue one another, eager launches and CUDA graph replay, wings close to
-tile edges, coupled wings and a lattice made only of border tiles.
+a time (LBM_FLAG_SINGLE_STEPS), and the no-slip residual of each call's last
+step (a call without field requests ends in a pass, which computes it), for
+odd and even step counts, calls that continue one another, eager launches
+and CUDA graph replay, wings close to tile edges, coupled wings and a
+lattice made only of border tiles.
 """
 import numpy as np
 import pytest
@@ -36,7 +38,7 @@ def _run(ep, calls, flags=0, graphs=True, step_flags=0):
         for n in calls:
             rows.append(s.step(n, first_cycle=cyc, flags=step_flags))
             cyc += n
-        out = {"rows": np.concatenate(rows), "f": s.f(), "sums": s.sums()}
+        out = {"rows": np.concatenate(rows), "f": s.f(), "sums": s.sums(), "resid": s.ibm_residual()}
         if step_flags & api.STEP_FIELDS:
             out["fields"] = s.fields()
     return out
@@ -49,6 +51,7 @@ def _compare(a, b):
     rb, cb, _ = b["sums"]
     assert ca == cb
     _same(ra, rb)
+    assert a["resid"] == b["resid"]   # the no-slip residual of the call's last step
     for x, y in zip(a.get("fields", ()), b.get("fields", ())):
         _same(x, y)
 
