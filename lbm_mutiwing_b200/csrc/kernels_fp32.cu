@@ -288,8 +288,9 @@ static_assert(PASS_BOXW <= 256 && PASS_BOXH <= 256, "tensor-map box extents");
 // then keep the registers within the same count)
 constexpr int PASS_MINB = (227 * 1024) / (int)(PASS_SMEM + 1024) < 8 ? (227 * 1024) / (int)(PASS_SMEM + 1024) : 8;
 
-template <bool NEAR>
-__device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin, float* Smid,
+// A near tile, one node per thread: step n + 1 values of border nodes and of
+// step n's band nodes come from O, nodes outside the lattice are skipped.
+__device__ __forceinline__ void pass_tile_near(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin, float* Smid,
                                           uint64_t* bar) {
     const int tx = t % a.ntx, ty = t / a.ntx;
     const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
@@ -310,7 +311,7 @@ __device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs&
     for (int n = threadIdx.x; n < PASS_MH * PASS_MW; n += PASS_THREADS) {
         const int mr = n / PASS_MW, mc = n % PASS_MW;
         float o[9];
-        if (NEAR) {
+        {
             const int i = x0 - 1 + mc, j = y0 - 1 + mr;
             if (i < 0 || i > a.nx - 1 || j < 0 || j > a.ny - 1) continue;   // outside: never pulled
             const long long p = (long long)j * a.pitch + i;
@@ -332,7 +333,7 @@ __device__ __forceinline__ void pass_tile(const CUtensorMap* tm, const PassArgs&
     // step n + 2 on the tile: node (x0 + cc, y0 + rr), R1 cell (rr + 1, cc + 1)
     for (int n = threadIdx.x; n < PASS_TY * PASS_TX; n += PASS_THREADS) {
         const int rr = n / PASS_TX, cc = n % PASS_TX, i = x0 + cc, j = y0 + rr;
-        if (NEAR && (i < 1 || i > a.nx - 2 || j > a.ny - 2)) continue;
+        if (i < 1 || i > a.nx - 2 || j > a.ny - 2) continue;
         const long long p = (long long)j * a.pitch + i;
         if ((__ldg(a.bits1 + (p >> 5)) >> (p & 31)) & 1u) continue;   // band nodes of step n + 1
         float g[9], o[9], drho, jx, jy;
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_near_kernel(cons
         if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny)) return;   // taken by its border block
     }
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
-    pass_tile<true>(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
+    pass_tile_near(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
 }
 
 int pass_tensor_map(const DevState& d, const float* base, void* out) {
