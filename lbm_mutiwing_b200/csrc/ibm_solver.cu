@@ -697,26 +697,17 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
         double wc[PANEL];
 #pragma unroll
         for (int c = 0; c < PANEL; ++c) wc[c] = __shfl_sync(0xffffffffu, wl, c);
-        for (int rb0 = 0; rb0 < bw; rb0 += 64) {
-            double acc[2];
+        for (int rb0 = 0; rb0 < bw; rb0 += 32) {   // one row below the panel per lane
+            const int rb = min(rb0 + lane, bw - 1);
+            const int i = k0 + np + rb;
+            const double* row = rowp(i) + (i - k0);
+            double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int rb = min(rb0 + lane + 32 * h, bw - 1);
-                const int i = k0 + np + rb;
-                const double* row = rowp(i) + (i - k0);
-                double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-                for (int c = 0; c < PANEL / 2; ++c) {
-                    a0 = a0 + row[-c] * wc[c];
-                    a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
-                }
-                acc[h] = a0 + a1;
+            for (int c = 0; c < PANEL / 2; ++c) {
+                a0 = a0 + row[-c] * wc[c];
+                a1 = a1 + row[-(c + PANEL / 2)] * wc[c + PANEL / 2];
             }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int rb = rb0 + lane + 32 * h;
-                if (rb < bw) z[k0 + np + rb] -= acc[h];
-            }
+            if (rb0 + lane < bw) z[k0 + np + rb] -= a0 + a1;
         }
         if (lane < np) z[k0 + lane] = wl * Li[PANEL * PANEL + lane];
         __syncwarp();
@@ -764,26 +755,17 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
 #pragma unroll
         for (int c = 0; c < PANEL; ++c) yc[c] = __shfl_sync(0xffffffffu, yl, c);
         const int above = min(bw, k0);   // rows k0 - above .. k0 - 1
-        for (int r0 = 0; r0 < above; r0 += 64) {
-            double acc[2];
+        for (int r0 = 0; r0 < above; r0 += 32) {   // one row above the panel per lane
+            const int r = min(r0 + lane, above - 1);
+            const int j = k0 - 1 - r;
+            const double* col = rowp(k0) + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
+            double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = min(r0 + lane + 32 * h, above - 1);
-                const int j = k0 - 1 - r;
-                const double* col = rowp(k0) + (k0 - j);   // L'(k0 + c, j) at col[c * (ld + 1)]
-                double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-                for (int c = 0; c < PANEL / 2; ++c) {
-                    a0 = a0 + col[c * (ld + 1)] * yc[c];
-                    a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
-                }
-                acc[h] = a0 + a1;
+            for (int c = 0; c < PANEL / 2; ++c) {
+                a0 = a0 + col[c * (ld + 1)] * yc[c];
+                a1 = a1 + col[(c + PANEL / 2) * (ld + 1)] * yc[c + PANEL / 2];
             }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = r0 + lane + 32 * h;
-                if (r < above) z[k0 - 1 - r] -= acc[h];
-            }
+            if (r0 + lane < above) z[k0 - 1 - r] -= a0 + a1;
         }
         if (lane < PANEL) z[k0 + lane] = yl;
         __syncwarp();
