@@ -4,18 +4,18 @@
 // g_k = f_k - w_k (rho0 = 1, w_k the FP32-rounded weights of D2Q9model.f90).
 //
 // Layout in HBM: nine planes g[k][y][x] with a padded row pitch (multiple of
-// 32 floats), two copies (ping-pong A -> B).  A thread owns one x column and
-// walks BULK_ROWS consecutive rows; the nine loads of a row are warp-coalesced
-// (shifted by the lattice velocity) and each stored value is read exactly once
-// by the next step, so HBM traffic is 9 reads + 9 writes of 4 bytes per node.
+// 32 floats), three copies (a step reads one and writes another; a two-step
+// pass also writes its first step's band and border values to the third).
+// One step moves 9 reads + 9 writes of 4 bytes per node; a pass moves the
+// same for two steps.
 //
 // Deviation form of the collision: with c = M w (only c0, c1, c2 are
 // non-zero), m_dev = M g and rho = 1 + (m_dev,0 + W - 1), the post-collision
 // deviation is m'_dev = m_dev + S (m_eq(rho, j) - c - m_dev), g' = M^-1 m'_dev.
 // Bulk nodes carry no body force (the immersed-boundary force is non-zero
 // only on band nodes), so j = (m_dev,3, m_dev,5) and m_eq needs no division.
-// Band nodes are re-collided afterwards in FP64 by fused_band_kernel with the
-// corrected velocity and the Guo forcing term.
+// Band nodes are re-collided in FP64 by the immersed boundary's closing
+// kernel with the corrected velocity and the Guo forcing term.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -408,10 +408,15 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
         const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
         int tn = t + 1;   // the block's next far tile (its flag loads overlap the wait)
         while (tn < last && !pass_far_tile(a, tn)) ++tn;
-        const bool ok = mbar_wait(&bar, it & 1);
+        // thread 0 waits for the loads; the others hold at the block barrier,
+        // which orders the staged planes for them, without taking issue slots
+        bool ok = true;
+        if (threadIdx.x == 0) ok = mbar_wait(&bar, it & 1);
         if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(a.status, ST_COPY_TIMEOUT);
-            mbar_wait(&bar, it & 1);   // let a late copy land before the block exits
+            if (threadIdx.x == 0) {
+                atomicOr(a.status, ST_COPY_TIMEOUT);
+                mbar_wait(&bar, it & 1);   // let a late copy land before the block exits
+            }
             return;
         }
         // step n + 1 on R1: pair u = (mr, mc / 2), nodes (x0 - 1 + mc, y0 - 1 + mr)
