@@ -68,48 +68,47 @@ struct Lanes<float2> {
     static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
     static __device__ __forceinline__ float2 k(float x) { return make_float2(x, x); }
 };
-template <class V>
-__device__ __forceinline__ void collide_lanes(const V g[9], const FusedConsts& c, V o[9], V& drho, V& jx, V& jy) {
+template <class V, class K>
+__device__ __forceinline__ void collide_lanes(const V g[9], const K& k, V o[9], V& drho, V& jx, V& jy) {
     using L = Lanes<V>;
-    const V m1k = L::k(-1.0f);
-    auto sub = [&](V a, V b) { return L::fma(m1k, b, a); };
+    auto sub = [&](V a, V b) { return L::fma(k.m1(), b, a); };
     // moments of the deviation
     const V p13 = L::add(g[1], g[3]), p24 = L::add(g[2], g[4]);
     const V p57 = L::add(g[5], g[7]), p68 = L::add(g[6], g[8]);
     const V s14 = L::add(p13, p24), s58 = L::add(p57, p68);
     const V m0 = L::add(L::add(g[0], s14), s58);
-    const V m1 = L::fma(L::k(2.0f), s58, sub(L::mul(L::k(-4.0f), g[0]), s14));
-    const V m2 = L::fma(L::k(4.0f), g[0], L::fma(L::k(-2.0f), s14, s58));
+    const V m1 = L::fma(k.p2(), s58, sub(L::mul(k.m4(), g[0]), s14));
+    const V m2 = L::fma(k.p4(), g[0], L::fma(k.m2(), s14, s58));
     const V d13 = sub(g[1], g[3]), d24 = sub(g[2], g[4]);
     const V a5 = sub(g[5], g[7]), a6 = sub(g[6], g[8]);
     jx = sub(L::add(d13, a5), a6);
-    const V m4 = sub(L::fma(L::k(-2.0f), d13, a5), a6);
+    const V m4 = sub(L::fma(k.m2(), d13, a5), a6);
     jy = L::add(L::add(d24, a5), a6);
-    const V m6 = L::add(L::fma(L::k(-2.0f), d24, a5), a6);
+    const V m6 = L::add(L::fma(k.m2(), d24, a5), a6);
     const V m7 = sub(p13, p24);
     const V m8 = sub(p57, p68);
     // relaxation toward the equilibrium moments (solution.f90:616-646)
-    drho = L::add(m0, L::k(c.wm1));
+    drho = L::add(m0, k.wm1());
     const V jxx = L::mul(jx, jx), jyy = L::mul(jy, jy), q = L::add(jxx, jyy);
-    const V t1 = L::fma(L::k(3.0f), q, L::fma(L::k(-2.0f), drho, L::k(-c.k1)));
-    const V e1 = L::fma(L::k(c.s1), sub(t1, m1), m1);
-    const V t2 = L::fma(L::k(-3.0f), q, L::add(drho, L::k(c.k2)));
-    const V e2 = L::fma(L::k(c.s2), sub(t2, m2), m2);
-    const V e4 = L::fma(L::k(-c.s4), L::add(jx, m4), m4);
-    const V e6 = L::fma(L::k(-c.s6), L::add(jy, m6), m6);
-    const V e7 = L::fma(L::k(c.s7), sub(sub(jxx, jyy), m7), m7);
-    const V e8 = L::fma(L::k(c.s8), sub(L::mul(jx, jy), m8), m8);
+    const V t1 = L::fma(k.p3(), q, L::fma(k.m2(), drho, k.mk1()));
+    const V e1 = L::fma(k.s1(), sub(t1, m1), m1);
+    const V t2 = L::fma(k.m3(), q, L::add(drho, k.k2()));
+    const V e2 = L::fma(k.s2(), sub(t2, m2), m2);
+    const V e4 = L::fma(k.ms4(), L::add(jx, m4), m4);
+    const V e6 = L::fma(k.ms6(), L::add(jy, m6), m6);
+    const V e7 = L::fma(k.s7(), sub(sub(jxx, jyy), m7), m7);
+    const V e8 = L::fma(k.s8(), sub(L::mul(jx, jy), m8), m8);
     // back to populations: M^-1 = M^T diag(1/9, 1/36, 1/36, 1/6, 1/12, 1/6, 1/12, 1/4, 1/4)
-    const V b0 = L::mul(m0, L::k(1.0f / 9.0f));
-    const V b1 = L::mul(e1, L::k(1.0f / 36.0f)), b2 = L::mul(e2, L::k(1.0f / 36.0f));
-    const V b3 = L::mul(jx, L::k(1.0f / 6.0f)), b4 = L::mul(e4, L::k(1.0f / 12.0f));
-    const V b5 = L::mul(jy, L::k(1.0f / 6.0f)), b6 = L::mul(e6, L::k(1.0f / 12.0f));
-    const V b7 = L::mul(e7, L::k(0.25f)), b8 = L::mul(e8, L::k(0.25f));
-    const V rA = L::fma(L::k(-2.0f), b2, sub(b0, b1));   // axis populations, common part
-    const V rD = L::add(L::fma(L::k(2.0f), b1, b0), b2);  // diagonal populations, common part
-    const V x34 = L::fma(L::k(-2.0f), b4, b3), y56 = L::fma(L::k(-2.0f), b6, b5);
+    const V b0 = L::mul(m0, k.r9());
+    const V b1 = L::mul(e1, k.r36()), b2 = L::mul(e2, k.r36());
+    const V b3 = L::mul(jx, k.r6()), b4 = L::mul(e4, k.r12());
+    const V b5 = L::mul(jy, k.r6()), b6 = L::mul(e6, k.r12());
+    const V b7 = L::mul(e7, k.r4()), b8 = L::mul(e8, k.r4());
+    const V rA = L::fma(k.m2(), b2, sub(b0, b1));   // axis populations, common part
+    const V rD = L::add(L::fma(k.p2(), b1, b0), b2);  // diagonal populations, common part
+    const V x34 = L::fma(k.m2(), b4, b3), y56 = L::fma(k.m2(), b6, b5);
     const V xd = L::add(b3, b4), yd = L::add(b5, b6);
-    o[0] = L::fma(L::k(4.0f), b2, L::fma(L::k(-4.0f), b1, b0));
+    o[0] = L::fma(k.p4(), b2, L::fma(k.m4(), b1, b0));
     o[1] = L::add(L::add(rA, x34), b7);
     o[2] = sub(L::add(rA, y56), b7);
     o[3] = L::add(sub(rA, x34), b7);
@@ -119,9 +118,72 @@ __device__ __forceinline__ void collide_lanes(const V g[9], const FusedConsts& c
     o[7] = L::add(sub(sub(rD, xd), yd), b8);
     o[8] = sub(sub(L::add(rD, xd), yd), b8);
 }
+// The constants of the collision for two nodes, from the kernel's parameters.
+struct PairK {
+    const PassPairs& k;
+    __device__ float2 m1() const { return k.m1; }
+    __device__ float2 p2() const { return k.p2; }
+    __device__ float2 m2() const { return k.m2; }
+    __device__ float2 p3() const { return k.p3; }
+    __device__ float2 m3() const { return k.m3; }
+    __device__ float2 p4() const { return k.p4; }
+    __device__ float2 m4() const { return k.m4; }
+    __device__ float2 r4() const { return k.r4; }
+    __device__ float2 r6() const { return k.r6; }
+    __device__ float2 r9() const { return k.r9; }
+    __device__ float2 r12() const { return k.r12; }
+    __device__ float2 r36() const { return k.r36; }
+    __device__ float2 wm1() const { return k.wm1; }
+    __device__ float2 mk1() const { return k.mk1; }
+    __device__ float2 k2() const { return k.k2; }
+    __device__ float2 s1() const { return k.s1; }
+    __device__ float2 s2() const { return k.s2; }
+    __device__ float2 ms4() const { return k.ms4; }
+    __device__ float2 ms6() const { return k.ms6; }
+    __device__ float2 s7() const { return k.s7; }
+    __device__ float2 s8() const { return k.s8; }
+};
+
+PassPairs pass_pairs(const FusedConsts& c) {
+    auto two = [](float x) { return make_float2(x, x); };
+    PassPairs k;
+    k.m1 = two(-1.0f); k.p2 = two(2.0f); k.m2 = two(-2.0f); k.p3 = two(3.0f); k.m3 = two(-3.0f);
+    k.p4 = two(4.0f); k.m4 = two(-4.0f); k.r4 = two(0.25f); k.r6 = two(1.0f / 6.0f); k.r9 = two(1.0f / 9.0f);
+    k.r12 = two(1.0f / 12.0f); k.r36 = two(1.0f / 36.0f); k.wm1 = two(c.wm1); k.mk1 = two(-c.k1);
+    k.k2 = two(c.k2); k.s1 = two(c.s1); k.s2 = two(c.s2); k.ms4 = two(-c.s4); k.ms6 = two(-c.s6);
+    k.s7 = two(c.s7); k.s8 = two(c.s8);
+    return k;
+}
+
+// The constants of the collision for one node: literals and the rates of c.
+struct ScalarK {
+    const FusedConsts& c;
+    __device__ float m1() const { return -1.0f; }
+    __device__ float p2() const { return 2.0f; }
+    __device__ float m2() const { return -2.0f; }
+    __device__ float p3() const { return 3.0f; }
+    __device__ float m3() const { return -3.0f; }
+    __device__ float p4() const { return 4.0f; }
+    __device__ float m4() const { return -4.0f; }
+    __device__ float r4() const { return 0.25f; }
+    __device__ float r6() const { return 1.0f / 6.0f; }
+    __device__ float r9() const { return 1.0f / 9.0f; }
+    __device__ float r12() const { return 1.0f / 12.0f; }
+    __device__ float r36() const { return 1.0f / 36.0f; }
+    __device__ float wm1() const { return c.wm1; }
+    __device__ float mk1() const { return -c.k1; }
+    __device__ float k2() const { return c.k2; }
+    __device__ float s1() const { return c.s1; }
+    __device__ float s2() const { return c.s2; }
+    __device__ float ms4() const { return -c.s4; }
+    __device__ float ms6() const { return -c.s6; }
+    __device__ float s7() const { return c.s7; }
+    __device__ float s8() const { return c.s8; }
+};
+
 __device__ __forceinline__ void fused_collide(const float g[9], const FusedConsts& c, float o[9], float& drho,
                                               float& jx, float& jy) {
-    collide_lanes<float>(g, c, o, drho, jx, jy);
+    collide_lanes<float>(g, ScalarK{c}, o, drho, jx, jy);
 }
 
 // One interior node (i, j); nodes of the band list are left to the band
@@ -401,7 +463,6 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     pass_issue_far(&tm, a, t, Sin, &bar, sbits[0]);
     __syncthreads();
-    const FusedConsts& c = a.c;
     for (int it = 0; t < last; ++it) {
         if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
         const int tx = t % a.ntx, ty = t / a.ntx;
@@ -433,7 +494,7 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
                 default: g[k] = lds_pair<3>(Sin, base); break;
                 }
             }
-            collide_lanes<float2>(g, c, o, drho, jx, jy);
+            collide_lanes<float2>(g, PairK{a.k}, o, drho, jx, jy);
 #pragma unroll
             for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * PASS_MCH + mr * PASS_MW + mc) = o[k];
         }
@@ -460,7 +521,7 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
                 default: g[k] = lds_pair<1>(Smid, base); break;
                 }
             }
-            collide_lanes<float2>(g, c, o, drho, jx, jy);
+            collide_lanes<float2>(g, PairK{a.k}, o, drho, jx, jy);
             float* q = a.Q + (long long)(y0 + rr) * a.pitch + x0 + cc;
             if (!(b0 | b1)) {
 #pragma unroll

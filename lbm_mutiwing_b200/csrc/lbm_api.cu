@@ -699,6 +699,7 @@ void enqueue_pass(LbmHandle* h, bool diag_last = false) {
     pa.nty = h->d.pass_nty;
     pa.plane = h->d.plane;
     pa.c = h->fc;
+    pa.k = pass_pairs(h->fc);
     pa.status = h->d.status;
     pa.far_tiles = h->timing ? h->d_far_tiles : nullptr;
     cudaEventRecord(h->ev_main, h->s_main);

@@ -54,6 +54,13 @@ inline __host__ __device__ bool pass_border_tile(int tx, int ty, int nx, int ny)
     const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
     return x0 - 1 <= 0 || x0 + PASS_TX >= nx - 1 || y0 - 1 <= 0 || y0 + PASS_TY >= ny - 1;
 }
+// The collision's constants as pairs (both lanes equal), for the paired
+// FP32 instructions of the far tiles: in the kernel's parameters they are
+// operands as they stand, instead of pairs rebuilt in registers at each use.
+struct PassPairs {
+    float2 m1, p2, m2, p3, m3, p4, m4, r4, r6, r9, r12, r36, wm1, mk1, k2, s1, s2, ms4, ms6, s7, s8;
+};
+PassPairs pass_pairs(const FusedConsts& c);
 struct PassArgs {
     const float* P;              // planes of step n (read by the tensor map)
     const float* O;              // planes of step n + 1: band nodes of step n and the border
@@ -68,6 +75,7 @@ struct PassArgs {
     int nx, ny, pitch, ntx, nty;
     long long plane;
     FusedConsts c;
+    PassPairs k;
     int* status;
     int* far_tiles;              // counts the far tiles processed (null: not counted)
 };
