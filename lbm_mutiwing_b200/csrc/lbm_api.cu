@@ -520,14 +520,14 @@ void collect_phase_times(LbmHandle* h) {
 // Fused path: the geometry (motion, markers, band list and factorised G) of
 // the first GEO_AHEAD steps of a call, each in its own set; every later
 // step's geometry is built GEO_AHEAD steps ahead while earlier steps run.
+// The builds run on the side streams (each band list after the previous
+// one, the factorisations beside them); the first step or pass waits for
+// them.
+void build_geometry(LbmHandle* h, int sn, int k);
 void prime_geometry(LbmHandle* h) {
-    for (int a = 0; a < GEO_AHEAD; ++a) {
-        DevState d = current(h);
-        use_geo(d, h->geo[(h->gset + a) % GEO_SETS]);
-        launch_ibm_band(d, h->s_main, nullptr);
-        launch_ibm_factor(d, h->factor_smem, h->s_main);
-    }
     for (bool& p : h->pending) p = false;
+    cudaEventRecord(h->ev_main, h->s_main);
+    for (int a = 0; a < GEO_AHEAD; ++a) build_geometry(h, (h->gset + a) % GEO_SETS, a & 1);
 }
 
 // Makes the main stream wait for every geometry set still building.
@@ -610,6 +610,11 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
         // prime); the one built now goes to the set whose last reader was
         // the previous step.
         const int sn = (h->gset + GEO_AHEAD) % GEO_SETS, s1 = (h->gset + 1) % GEO_SETS;
+        if (h->pending[h->gset]) {   // this step's geometry, primed on the side streams
+            cudaStreamWaitEvent(h->s_main, h->ev_list[h->gset], 0);
+            cudaStreamWaitEvent(h->s_main, h->ev_fact[h->gset], 0);
+            h->pending[h->gset] = false;
+        }
         cudaEventRecord(h->ev_main, h->s_main);
         cudaStreamWaitEvent(h->s_ibm, h->ev_main, 0);
         cudaStreamWaitEvent(h->s_bc, h->ev_main, 0);
