@@ -50,6 +50,10 @@ extern "C" {
 #define LBM_FLAG_SOLVE_PANELS32 4  /* substitute in 32-row panels built by the factorisation, where every
                                       wing's panel data fit in shared memory (fewer dependent steps on the
                                       step's chain, a longer factorisation) */
+#define LBM_FLAG_PASS_TALL_TILES 16   /* fused path: two-step passes over 64 x 12 tiles whatever the lattice
+                                         size (by default from 32 Mi nodes on; the same results) */
+#define LBM_FLAG_PASS_SHORT_TILES 32  /* fused path: two-step passes over 64 x 8 tiles whatever the lattice
+                                         size (by default below 32 Mi nodes; the same results) */
 
 /* lbm_step flags */
 #define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */

@@ -30,6 +30,8 @@ FLAG_NO_GRAPHS = 1
 FLAG_SOLVE_STREAM = 2
 FLAG_SOLVE_PANELS32 = 4
 FLAG_SINGLE_STEPS = 8
+FLAG_PASS_TALL_TILES = 16
+FLAG_PASS_SHORT_TILES = 32
 
 STATUS_BITS = {1: "band_overflow", 2: "cover_overflow", 4: "box_outside", 8: "pivot_clamped",
                16: "wings_coupled", 32: "coupled_noconv", 64: "motion"}

@@ -275,10 +275,11 @@ __global__ void ibm_claim_kernel_multi(MultiArgs m) {
 
 // Flags the pass tiles whose R1 (the tile and one ring) holds node (i, j)
 // (0-based): tx with x0 - 1 <= i <= x0 + PASS_TX, ty with y0 - 1 <= j <=
-// y0 + PASS_TY (x0 = PASS_TX tx, y0 = 1 + PASS_TY ty).
+// y0 + R (x0 = PASS_TX tx, y0 = 1 + R ty, R = d.pass_rows).
 __device__ inline void flag_pass_tiles(const DevState& d, int i, int j) {
+    const int R = d.pass_rows;
     const int tx0 = max(0, (i + PASS_TX - 1) / PASS_TX - 1), tx1 = min(d.pass_ntx - 1, (i + 1) / PASS_TX);
-    const int ty0 = max(0, (j + PASS_TY - 2) / PASS_TY - 1), ty1 = min(d.pass_nty - 1, j / PASS_TY);
+    const int ty0 = max(0, (j + R - 2) / R - 1), ty1 = min(d.pass_nty - 1, j / R);
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) d.tile_flags[ty * d.pass_ntx + tx] = 1;
 }

@@ -336,31 +336,39 @@ int fused_tensor_map(const DevState& d, const float* base, void* out) {
 // second step's band re-collision and far field write them.  Every node is
 // computed by fused_collide, as in the one-step kernels, so a pass gives the
 // bits of two steps.
-// one column pair of R1 per thread, in whole warps
-constexpr int PASS_THREADS = ((PASS_TY + 2) * (PASS_TX + 2) / 2 + 31) / 32 * 32;
-constexpr int PASS_WORDS = PASS_TX / 32;   // band-bit words of a tile row
-constexpr int PASS_BOXW = PASS_TX + 8, PASS_BOXH = PASS_TY + 4;
-constexpr int PASS_CH = (PASS_BOXH * PASS_BOXW + 31) & ~31;   // floats per input plane, 128-byte multiple
-constexpr int PASS_MW = PASS_TX + 2, PASS_MH = PASS_TY + 2;   // R1
-constexpr int PASS_MCH = PASS_MH * PASS_MW;
-constexpr size_t PASS_SMEM = (size_t)(9 * PASS_CH + 9 * PASS_MCH) * sizeof(float) + 128;
+// The block's shape for tiles of R rows: one column pair of R1 per thread,
+// in whole warps; band-bit words of a tile row; the staged box (BOXW x BOXH)
+// and its plane stride CH (a 128-byte multiple); R1 (MW x MH); the dynamic
+// shared memory; the resident blocks per SM that it allows (the launch
+// bounds then keep the registers within the same count).
+template <int R>
+struct PassShape {
+    static constexpr int THREADS = ((R + 2) * (PASS_TX + 2) / 2 + 31) / 32 * 32;
+    static constexpr int WORDS = PASS_TX / 32;
+    static constexpr int BOXW = PASS_TX + 8, BOXH = R + 4;
+    static constexpr int CH = (BOXH * BOXW + 31) & ~31;
+    static constexpr int MW = PASS_TX + 2, MH = R + 2;
+    static constexpr int MCH = MH * MW;
+    static constexpr size_t SMEM = (size_t)(9 * CH + 9 * MCH) * sizeof(float) + 128;
+    static constexpr int MINB = (227 * 1024) / (int)(SMEM + 1024) < 8 ? (227 * 1024) / (int)(SMEM + 1024) : 8;
+    static_assert(BOXW <= 256 && BOXH <= 256, "tensor-map box extents");
+    static_assert(WORDS * R <= THREADS, "a tile's band bits are staged one word per thread");
+};
 static_assert(PASS_TX % 32 == 0, "tiles start on 16-byte boundaries and on band-bit words");
-static_assert(PASS_BOXW <= 256 && PASS_BOXH <= 256, "tensor-map box extents");
-// resident blocks per SM that the shared memory allows (the launch bounds
-// then keep the registers within the same count)
-constexpr int PASS_MINB = (227 * 1024) / (int)(PASS_SMEM + 1024) < 8 ? (227 * 1024) / (int)(PASS_SMEM + 1024) : 8;
 
 // A near tile, one node per thread: step n + 1 values of border nodes and of
 // step n's band nodes come from O, nodes outside the lattice are skipped.
+template <int R>
 __device__ __forceinline__ void pass_tile_near(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin, float* Smid,
-                                          uint64_t* bar) {
+                                               uint64_t* bar) {
+    using S = PassShape<R>;
     const int tx = t % a.ntx, ty = t / a.ntx;
-    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+    const int x0 = tx * PASS_TX, y0 = 1 + ty * R;
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        mbar_arrive_expect_tx(bar, (uint32_t)(9 * PASS_BOXH * PASS_BOXW * sizeof(float)));
+        mbar_arrive_expect_tx(bar, (uint32_t)(9 * S::BOXH * S::BOXW * sizeof(float)));
 #pragma unroll
-        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * PASS_CH, tm, x0 - 4, y0 - 2, k, bar);
+        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * S::CH, tm, x0 - 4, y0 - 2, k, bar);
     }
     __syncthreads();
     const bool ok = mbar_wait(bar, 0);
@@ -370,8 +378,8 @@ __device__ __forceinline__ void pass_tile_near(const CUtensorMap* tm, const Pass
         return;
     }
     // step n + 1 on R1: node (x0 - 1 + mc, y0 - 1 + mr), box cell (mr + 1, mc + 3)
-    for (int n = threadIdx.x; n < PASS_MH * PASS_MW; n += PASS_THREADS) {
-        const int mr = n / PASS_MW, mc = n % PASS_MW;
+    for (int n = threadIdx.x; n < S::MH * S::MW; n += S::THREADS) {
+        const int mr = n / S::MW, mc = n % S::MW;
         float o[9];
         {
             const int i = x0 - 1 + mc, j = y0 - 1 + mr;
@@ -380,27 +388,27 @@ __device__ __forceinline__ void pass_tile_near(const CUtensorMap* tm, const Pass
             const bool border = i == 0 || j == 0 || i == a.nx - 1 || j == a.ny - 1;
             if (border || ((__ldg(a.bits0 + (p >> 5)) >> (p & 31)) & 1u)) {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) Smid[k * PASS_MCH + n] = __ldcg(a.O + k * a.plane + p);
+                for (int k = 0; k < 9; ++k) Smid[k * S::MCH + n] = __ldcg(a.O + k * a.plane + p);
                 continue;
             }
         }
         float g[9], drho, jx, jy;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) g[k] = Sin[k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc + 3 - ex(k)];
+        for (int k = 0; k < 9; ++k) g[k] = Sin[k * S::CH + (mr + 1 - ey(k)) * S::BOXW + mc + 3 - ex(k)];
         fused_collide(g, a.c, o, drho, jx, jy);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) Smid[k * PASS_MCH + n] = o[k];
+        for (int k = 0; k < 9; ++k) Smid[k * S::MCH + n] = o[k];
     }
     __syncthreads();
     // step n + 2 on the tile: node (x0 + cc, y0 + rr), R1 cell (rr + 1, cc + 1)
-    for (int n = threadIdx.x; n < PASS_TY * PASS_TX; n += PASS_THREADS) {
+    for (int n = threadIdx.x; n < R * PASS_TX; n += S::THREADS) {
         const int rr = n / PASS_TX, cc = n % PASS_TX, i = x0 + cc, j = y0 + rr;
         if (i < 1 || i > a.nx - 2 || j > a.ny - 2) continue;
         const long long p = (long long)j * a.pitch + i;
         if ((__ldg(a.bits1 + (p >> 5)) >> (p & 31)) & 1u) continue;   // band nodes of step n + 1
         float g[9], o[9], drho, jx, jy;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) g[k] = Smid[k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc + 1 - ex(k)];
+        for (int k = 0; k < 9; ++k) g[k] = Smid[k * S::MCH + (rr + 1 - ey(k)) * S::MW + cc + 1 - ex(k)];
         fused_collide(g, a.c, o, drho, jx, jy);
 #pragma unroll
         for (int k = 0; k < 9; ++k) a.Q[k * a.plane + p] = o[k];
@@ -423,52 +431,57 @@ __device__ __forceinline__ float2 lds_pair(const float* S, int even_base) {
 // are skipped): once the first step of a tile has read the staged planes,
 // thread 0 issues the next tile's tensor loads into the same buffer, so they
 // fly while the second step runs.  The band bits of step n + 1 of each tile
-// (PASS_TY rows x PASS_WORDS words) are staged beside its loads.
+// (R rows x PassShape<R>::WORDS words) are staged beside its loads.
 #ifndef LBM_PASS_TPC
 #define LBM_PASS_TPC 2
 #endif
 constexpr int PASS_TPC = LBM_PASS_TPC;
 
+template <int R>
 __device__ __forceinline__ bool pass_far_tile(const PassArgs& a, int t) {
-    return t < a.ntx * a.nty && !pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny) && !__ldg(a.flags0 + t);
+    return t < a.ntx * a.nty && !pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny, R) && !__ldg(a.flags0 + t);
 }
 
 // Thread 0 arms the barrier and issues tile t's loads; the first
-// PASS_WORDS * PASS_TY threads stage its band bits.
+// WORDS * R threads stage its band bits.
+template <int R>
 __device__ __forceinline__ void pass_issue_far(const CUtensorMap* tm, const PassArgs& a, int t, float* Sin,
                                                uint64_t* bar, unsigned* sbits) {
-    const int x0 = (t % a.ntx) * PASS_TX, y0 = 1 + (t / a.ntx) * PASS_TY;
+    using S = PassShape<R>;
+    const int x0 = (t % a.ntx) * PASS_TX, y0 = 1 + (t / a.ntx) * R;
     if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, (uint32_t)(9 * PASS_BOXH * PASS_BOXW * sizeof(float)));
+        mbar_arrive_expect_tx(bar, (uint32_t)(9 * S::BOXH * S::BOXW * sizeof(float)));
 #pragma unroll
-        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * PASS_CH, tm, x0 - 4, y0 - 2, k, bar);
+        for (int k = 0; k < 9; ++k) tma_load_3d(Sin + k * S::CH, tm, x0 - 4, y0 - 2, k, bar);
     }
-    if (threadIdx.x < PASS_WORDS * PASS_TY) {
-        const long long w = ((long long)(y0 + threadIdx.x / PASS_WORDS) * a.pitch + x0) >> 5;
-        sbits[threadIdx.x] = __ldg(a.bits1 + w + threadIdx.x % PASS_WORDS);
+    if (threadIdx.x < S::WORDS * R) {
+        const long long w = ((long long)(y0 + threadIdx.x / S::WORDS) * a.pitch + x0) >> 5;
+        sbits[threadIdx.x] = __ldg(a.bits1 + w + threadIdx.x % S::WORDS);
     }
 }
 
-__global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const __grid_constant__ CUtensorMap tm,
-                                                                            const PassArgs a) {
+template <int R>
+__global__ void __launch_bounds__(PassShape<R>::THREADS, PassShape<R>::MINB)
+    pass_far_kernel(const __grid_constant__ CUtensorMap tm, const PassArgs a) {
+    using S = PassShape<R>;
     extern __shared__ unsigned char pass_raw[];
     __shared__ uint64_t bar;
-    __shared__ unsigned sbits[2][PASS_WORDS * PASS_TY];
+    __shared__ unsigned sbits[2][S::WORDS * R];
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
-    float* Smid = Sin + 9 * PASS_CH;
+    float* Smid = Sin + 9 * S::CH;
     const int first = blockIdx.x * PASS_TPC, last = first + PASS_TPC;
     int t = first;
-    while (t < last && !pass_far_tile(a, t)) ++t;
+    while (t < last && !pass_far_tile<R>(a, t)) ++t;
     if (t >= last) return;   // near tiles only
     if (threadIdx.x == 0) mbar_init(&bar, 1);
-    pass_issue_far(&tm, a, t, Sin, &bar, sbits[0]);
+    pass_issue_far<R>(&tm, a, t, Sin, &bar, sbits[0]);
     __syncthreads();
     for (int it = 0; t < last; ++it) {
         if (a.far_tiles && threadIdx.x == 0) atomicAdd(a.far_tiles, 1);
         const int tx = t % a.ntx, ty = t / a.ntx;
-        const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
+        const int x0 = tx * PASS_TX, y0 = 1 + ty * R;
         int tn = t + 1;   // the block's next far tile (its flag loads overlap the wait)
-        while (tn < last && !pass_far_tile(a, tn)) ++tn;
+        while (tn < last && !pass_far_tile<R>(a, tn)) ++tn;
         // thread 0 waits for the loads; the others hold at the block barrier,
         // which orders the staged planes for them, without taking issue slots
         bool ok = true;
@@ -482,12 +495,12 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
         }
         // step n + 1 on R1: pair u = (mr, mc / 2), nodes (x0 - 1 + mc, y0 - 1 + mr)
         // and the next column; box cell (mr + 1, mc + 3)
-        for (int u = threadIdx.x; u < PASS_MH * PASS_MW / 2; u += PASS_THREADS) {
-            const int mr = u / (PASS_MW / 2), mc = 2 * (u % (PASS_MW / 2));
+        for (int u = threadIdx.x; u < S::MH * S::MW / 2; u += S::THREADS) {
+            const int mr = u / (S::MW / 2), mc = 2 * (u % (S::MW / 2));
             float2 g[9], o[9], drho, jx, jy;
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-                const int base = k * PASS_CH + (mr + 1 - ey(k)) * PASS_BOXW + mc;
+                const int base = k * S::CH + (mr + 1 - ey(k)) * S::BOXW + mc;
                 switch (ex(k)) {   // ex is a constant per unrolled k
                 case 1: g[k] = lds_pair<2>(Sin, base); break;
                 case -1: g[k] = lds_pair<4>(Sin, base); break;
@@ -496,25 +509,25 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
             }
             collide_lanes<float2>(g, PairK{a.k}, o, drho, jx, jy);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * PASS_MCH + mr * PASS_MW + mc) = o[k];
+            for (int k = 0; k < 9; ++k) *reinterpret_cast<float2*>(Smid + k * S::MCH + mr * S::MW + mc) = o[k];
         }
         __syncthreads();   // the staged planes are read: the next tile's loads may land
         if (tn < last) {
             if (threadIdx.x == 0) fence_async_smem();
-            pass_issue_far(&tm, a, tn, Sin, &bar, sbits[(it + 1) & 1]);
+            pass_issue_far<R>(&tm, a, tn, Sin, &bar, sbits[(it + 1) & 1]);
         }
         // step n + 2 on the tile: pair (rr, cc / 2), nodes (x0 + cc, y0 + rr)
         // and the next column; R1 cell (rr + 1, cc + 1)
         const unsigned* bits = sbits[it & 1];
-        for (int u = threadIdx.x; u < PASS_TY * PASS_TX / 2; u += PASS_THREADS) {
+        for (int u = threadIdx.x; u < R * PASS_TX / 2; u += S::THREADS) {
             const int rr = u / (PASS_TX / 2), cc = 2 * (u % (PASS_TX / 2));
-            const unsigned word = bits[rr * PASS_WORDS + (cc >> 5)];
+            const unsigned word = bits[rr * S::WORDS + (cc >> 5)];
             const unsigned b0 = (word >> (cc & 31)) & 1u, b1 = (word >> ((cc & 31) + 1)) & 1u;
             if (b0 & b1) continue;   // both band nodes of step n + 1
             float2 g[9], o[9], drho, jx, jy;
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-                const int base = k * PASS_MCH + (rr + 1 - ey(k)) * PASS_MW + cc;
+                const int base = k * S::MCH + (rr + 1 - ey(k)) * S::MW + cc;
                 switch (ex(k)) {
                 case 1: g[k] = lds_pair<0>(Smid, base); break;
                 case -1: g[k] = lds_pair<2>(Smid, base); break;
@@ -539,8 +552,9 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_far_kernel(const
     }
 }
 
-__global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_near_kernel(const __grid_constant__ CUtensorMap tm,
-                                                                    const PassArgs a) {
+template <int R>
+__global__ void __launch_bounds__(PassShape<R>::THREADS, PassShape<R>::MINB)
+    pass_near_kernel(const __grid_constant__ CUtensorMap tm, const PassArgs a) {
     extern __shared__ unsigned char pass_raw[];
     __shared__ uint64_t bar;
     const int b = blockIdx.x;
@@ -550,36 +564,63 @@ __global__ void __launch_bounds__(PASS_THREADS, PASS_MINB) pass_near_kernel(cons
     } else {
         if (b - a.nborder >= min(__ldcg(a.band_n), a.band_cap)) return;
         t = __ldcg(a.band_list + (b - a.nborder));
-        if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny)) return;   // taken by its border block
+        if (pass_border_tile(t % a.ntx, t / a.ntx, a.nx, a.ny, R)) return;   // taken by its border block
     }
     float* Sin = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(pass_raw) + 127) & ~(uintptr_t)127);
-    pass_tile_near(&tm, a, t, Sin, Sin + 9 * PASS_CH, &bar);
+    pass_tile_near<R>(&tm, a, t, Sin, Sin + 9 * PassShape<R>::CH, &bar);
 }
 
-int pass_tensor_map(const DevState& d, const float* base, void* out) {
-    const cuuint32_t box[3] = {PASS_BOXW, PASS_BOXH, 1};
+int pass_tensor_map(const DevState& d, const float* base, int rows, void* out) {
+    if (rows != PASS_TY && rows != PASS_TY_TALL) return -1;
+    const cuuint32_t box[3] = {(cuuint32_t)PASS_TX + 8, (cuuint32_t)rows + 4, 1};
     return encode_plane_map(d, base, box, out);
 }
 
-void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st) {
-    pass_far_kernel<<<(a.ntx * a.nty + PASS_TPC - 1) / PASS_TPC, PASS_THREADS, PASS_SMEM, st>>>(
+template <int R>
+void launch_pass_far_rows(const PassArgs& a, const void* tmap, cudaStream_t st) {
+    pass_far_kernel<R><<<(a.ntx * a.nty + PASS_TPC - 1) / PASS_TPC, PassShape<R>::THREADS, PassShape<R>::SMEM, st>>>(
         *reinterpret_cast<const CUtensorMap*>(tmap), a);
+}
+template <int R>
+void launch_pass_near_rows(const PassArgs& a, const void* tmap, cudaStream_t st) {
+    pass_near_kernel<R><<<a.nborder + a.band_cap, PassShape<R>::THREADS, PassShape<R>::SMEM, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(tmap), a);
+}
+
+void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st) {
+    if (a.rows == PASS_TY_TALL)
+        launch_pass_far_rows<PASS_TY_TALL>(a, tmap, st);
+    else
+        launch_pass_far_rows<PASS_TY>(a, tmap, st);
 }
 
 void launch_pass_near(const PassArgs& a, const void* tmap, cudaStream_t st) {
-    pass_near_kernel<<<a.nborder + a.band_cap, PASS_THREADS, PASS_SMEM, st>>>(
-        *reinterpret_cast<const CUtensorMap*>(tmap), a);
+    if (a.rows == PASS_TY_TALL)
+        launch_pass_near_rows<PASS_TY_TALL>(a, tmap, st);
+    else
+        launch_pass_near_rows<PASS_TY>(a, tmap, st);
 }
 
-cudaError_t pass_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(pass_far_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PASS_SMEM);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pass_near_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PASS_SMEM);
+template <int R>
+cudaError_t pass_prepare_rows() {
+    const int smem = (int)PassShape<R>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(pass_far_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pass_near_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     return e;
 }
+cudaError_t pass_prepare() {
+    const cudaError_t e = pass_prepare_rows<PASS_TY>();
+    return e == cudaSuccess ? pass_prepare_rows<PASS_TY_TALL>() : e;
+}
 
-bool is_pass_far_kernel(const void* func) { return func == reinterpret_cast<const void*>(pass_far_kernel); }
-bool is_pass_near_kernel(const void* func) { return func == reinterpret_cast<const void*>(pass_near_kernel); }
+bool is_pass_far_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(pass_far_kernel<PASS_TY>) ||
+           func == reinterpret_cast<const void*>(pass_far_kernel<PASS_TY_TALL>);
+}
+bool is_pass_near_kernel(const void* func) {
+    return func == reinterpret_cast<const void*>(pass_near_kernel<PASS_TY>) ||
+           func == reinterpret_cast<const void*>(pass_near_kernel<PASS_TY_TALL>);
+}
 
 // Step n + 1 values for the second step's immersed boundary and far field:
 // item t < 64 nseg is slot t % 64 of the 8 x 8 square around segment

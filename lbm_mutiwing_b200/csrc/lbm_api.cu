@@ -696,12 +696,14 @@ void enqueue_pass(LbmHandle* h, bool diag_last = false) {
     pa.band_list = h->geo[g0].tile_list;
     pa.band_n = h->geo[g0].tile_n;
     pa.nborder = h->nborder;
-    pa.band_cap = std::min(h->d.pass_ntx * h->d.pass_nty, PASS_TILES_PER_SEGMENT * std::max(1, h->d.nseg));
+    pa.band_cap = std::min(h->d.pass_ntx * h->d.pass_nty,
+                           pass_tiles_per_segment(h->d.pass_rows) * std::max(1, h->d.nseg));
     pa.nx = h->d.nx;
     pa.ny = h->d.ny;
     pa.pitch = h->d.pitch;
     pa.ntx = h->d.pass_ntx;
     pa.nty = h->d.pass_nty;
+    pa.rows = h->d.pass_rows;
     pa.plane = h->d.plane;
     pa.c = h->fc;
     pa.k = pass_pairs(h->fc);
@@ -1165,8 +1167,12 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     }
     if (c.precision != LBM_PRECISION_FP64) {
         // pass tiles: flags and flagged-tile lists per geometry set, and the
-        // tiles whose R1 meets the border
-        const int ntx = pass_tiles_x(c.nx), nty = pass_tiles_y(c.ny), ntl = ntx * nty;
+        // tiles whose R1 meets the border; the tall tiles on large lattices
+        // (or as the flags ask)
+        const bool tall = (c.flags & LBM_FLAG_PASS_TALL_TILES) ||
+                          (!(c.flags & LBM_FLAG_PASS_SHORT_TILES) && (long long)c.nx * c.ny >= PASS_TALL_NODES);
+        const int rows = tall ? PASS_TY_TALL : PASS_TY;
+        const int ntx = pass_tiles_x(c.nx), nty = pass_tiles_y(c.ny, rows), ntl = ntx * nty;
         for (int s = 0; s < GEO_SETS; ++s) {
             GeoSet& g = h->geo[s];
             if (dalloc(h, &g.tile_flags, (size_t)(ntl + 3) / 4 * 4) || dalloc(h, &g.tile_list, (size_t)ntl) ||
@@ -1180,9 +1186,10 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         h->d.tile_n = h->geo[0].tile_n;
         h->d.pass_ntx = ntx;
         h->d.pass_nty = nty;
+        h->d.pass_rows = rows;
         std::vector<int> bt;
         for (int t = 0; t < ntl; ++t)
-            if (pass_border_tile(t % ntx, t / ntx, c.nx, c.ny)) bt.push_back(t);
+            if (pass_border_tile(t % ntx, t / ntx, c.nx, c.ny, rows)) bt.push_back(t);
         if (dalloc(h, &h->border_tiles, bt.size()) || dalloc(h, &h->d_far_tiles, 1)) return -1;
         CK(cudaMemset(h->d_far_tiles, 0, sizeof(int)));
         CK(cudaMemcpy(h->border_tiles, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1225,7 +1232,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
         for (int k = 0; k < 3; ++k) h->tmap_ok = h->tmap_ok && fused_tensor_map(d, h->planes[k], &h->tmap[k]) == 0;
         // two-step passes need the tiled loads and a lattice of a few tiles
         h->pass_ok = c.nx >= 16 && c.ny >= 16 && pass_prepare() == cudaSuccess;
-        for (int k = 0; k < 3; ++k) h->pass_ok = h->pass_ok && pass_tensor_map(d, h->planes[k], &h->ptmap[k]) == 0;
+        for (int k = 0; k < 3; ++k)
+            h->pass_ok = h->pass_ok && pass_tensor_map(d, h->planes[k], h->d.pass_rows, &h->ptmap[k]) == 0;
     }
     if (init_state(h)) return -1;
     return 0;

@@ -182,13 +182,13 @@ struct DevState {
     double* wing_fm;             // 3 W raw per-wing Fx, Fy, M of the last step
     double* ibm_resid;           // [0] |X du - r|^2, [1] |r|^2
     FusedConsts fc;              // fused path: collision constants
-    // two-step passes (fused path): lattice tiles of PASS_TX x PASS_TY
+    // two-step passes (fused path): lattice tiles of PASS_TX x pass_rows
     // nodes; a tile is flagged when it or a neighbour of it holds a band
     // node of this geometry set (its first step then needs the band's values)
     unsigned char* tile_flags;   // pass_ntx * pass_nty (null: not tracked)
     int* tile_list;              // the flagged tiles, compacted by the scan kernel
     int* tile_n;                 // [0] flagged tiles
-    int pass_ntx, pass_nty;
+    int pass_ntx, pass_nty, pass_rows;
 };
 
 __host__ __device__ inline long long pidx(const DevState& d, int i, int j) {

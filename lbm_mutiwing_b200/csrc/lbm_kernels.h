@@ -37,22 +37,32 @@ void launch_fused_import(const DevState& d, const double* f, float* g, cudaStrea
 // ty) covers the interior nodes [PASS_TX tx, PASS_TX tx + PASS_TX - 1] x
 // [1 + PASS_TY ty, PASS_TY (ty + 1)]; its first step needs the tile and one
 // ring of neighbours (R1), its pulls a second ring.
+// Tiles of PASS_TX columns and, per handle, PASS_TY rows or PASS_TY_TALL
+// rows: the taller tile recomputes a smaller share of its nodes (R1 against
+// the tile) and runs three blocks per SM instead of four; it pays where the
+// far tiles bound the pass (large lattices), the shorter one where the
+// immersed-boundary chains do (PASS_TALL_NODES: the lattice size from which
+// a handle takes the tall tiles).
 #ifndef LBM_PASS_TX
 #define LBM_PASS_TX 64
 #endif
 #ifndef LBM_PASS_TY
 #define LBM_PASS_TY 8
 #endif
-constexpr int PASS_TX = LBM_PASS_TX, PASS_TY = LBM_PASS_TY;
+#ifndef LBM_PASS_TY_TALL
+#define LBM_PASS_TY_TALL 12
+#endif
+constexpr int PASS_TX = LBM_PASS_TX, PASS_TY = LBM_PASS_TY, PASS_TY_TALL = LBM_PASS_TY_TALL;
+constexpr long long PASS_TALL_NODES = 32LL << 20;
 // flagged tiles a support box can touch: its 6 nodes and the ring either
 // side span 8 nodes in each direction
-constexpr int PASS_TILES_PER_SEGMENT = ((8 + PASS_TX - 1) / PASS_TX + 1) * ((8 + PASS_TY - 1) / PASS_TY + 1);
+constexpr int pass_tiles_per_segment(int rows) { return ((8 + PASS_TX - 1) / PASS_TX + 1) * ((8 + rows - 1) / rows + 1); }
 inline int pass_tiles_x(int nx) { return (nx + PASS_TX - 1) / PASS_TX; }
-inline int pass_tiles_y(int ny) { return (ny - 2 + PASS_TY - 1) / PASS_TY; }
-// whether R1 of tile (tx, ty) holds a node of the lattice border
-inline __host__ __device__ bool pass_border_tile(int tx, int ty, int nx, int ny) {
-    const int x0 = tx * PASS_TX, y0 = 1 + ty * PASS_TY;
-    return x0 - 1 <= 0 || x0 + PASS_TX >= nx - 1 || y0 - 1 <= 0 || y0 + PASS_TY >= ny - 1;
+inline int pass_tiles_y(int ny, int rows) { return (ny - 2 + rows - 1) / rows; }
+// whether R1 of tile (tx, ty) of `rows` rows holds a node of the lattice border
+inline __host__ __device__ bool pass_border_tile(int tx, int ty, int nx, int ny, int rows) {
+    const int x0 = tx * PASS_TX, y0 = 1 + ty * rows;
+    return x0 - 1 <= 0 || x0 + PASS_TX >= nx - 1 || y0 - 1 <= 0 || y0 + rows >= ny - 1;
 }
 // The collision's constants as pairs (both lanes equal), for the paired
 // FP32 instructions of the far tiles: in the kernel's parameters they are
@@ -73,14 +83,16 @@ struct PassArgs {
     const int* band_n;           // their count
     int nborder, band_cap;       // border tiles; capacity of the flagged-tile list
     int nx, ny, pitch, ntx, nty;
+    int rows;                    // tile rows: PASS_TY or PASS_TY_TALL
     long long plane;
     FusedConsts c;
     PassPairs k;
     int* status;
     int* far_tiles;              // counts the far tiles processed (null: not counted)
 };
-// Tensor map of the nine planes at base for the pass kernel's boxes.
-int pass_tensor_map(const DevState& d, const float* base, void* out);
+// Tensor map of the nine planes at base for the boxes of the pass kernels
+// with tiles of `rows` rows (PASS_TY or PASS_TY_TALL).
+int pass_tensor_map(const DevState& d, const float* base, int rows, void* out);
 // far tiles (every tile not flagged and off the border), from P alone
 void launch_pass_far(const PassArgs& a, const void* tmap, cudaStream_t st);
 // the border tiles and the flagged tiles, after the band and the far field

@@ -10,7 +10,8 @@ a time (LBM_FLAG_SINGLE_STEPS), and the no-slip residual of each call's last
 step (a call without field requests ends in a pass, which computes it), for
 odd and even step counts, calls that continue one another, eager launches
 and CUDA graph replay, wings close to tile edges, coupled wings and a
-lattice made only of border tiles.
+lattice made only of border tiles; with both tile shapes a handle may take
+(64 x 8, and 64 x 12 as on large lattices).
 """
 import numpy as np
 import pytest
@@ -92,3 +93,33 @@ def test_passes_small_lattice_all_border_tiles(gpu_lib):
                                heave=0.02)
     assert (ep.nx, ep.ny) == (27, 19)
     _compare(_run(ep, [12]), _run(ep, [12], flags=api.FLAG_SINGLE_STEPS))
+
+
+TALL = api.FLAG_PASS_TALL_TILES
+
+
+@pytest.mark.parametrize("calls", [[2], [5], [26], [7, 8, 1, 12]])
+def test_tall_tiles_equal_single_steps(gpu_lib, calls):
+    ep = small("pt", 2, (5.0, 2.5))
+    _compare(_run(ep, calls, flags=TALL), _run(ep, calls, flags=api.FLAG_SINGLE_STEPS))
+
+
+def test_tall_tiles_fields_and_eager(gpu_lib):
+    ep = small("qt", 3, (7.0, 2.5))
+    _compare(_run(ep, [11, 10], flags=TALL | api.FLAG_NO_GRAPHS, step_flags=api.STEP_FIELDS),
+             _run(ep, [11, 10], flags=api.FLAG_SINGLE_STEPS, step_flags=api.STEP_FIELDS))
+
+
+def test_tall_tiles_wings_across_tile_edges(gpu_lib):
+    ep = wl.tandem_pitch_heave("edges_t", 6.0, 3.0, 1.0 / 64.0, 100.0, -1.5, 0.0, 120, 40, n_wings=2,
+                               x_spacing=1.28, spacing="uniform", pitch_deg=20.0, heave=0.3, freq=2.0)
+    _compare(_run(ep, [40], flags=TALL), _run(ep, [40], flags=api.FLAG_SINGLE_STEPS))
+
+
+def test_tall_tiles_coupled_wings_and_small_lattice(gpu_lib):
+    ep = wl.tandem_pitch_heave("coupled_t", 5.0, 2.5, 0.02, 100.0, -1.0, 0.0, 100, 20, n_wings=2,
+                               x_spacing=1.03, lag=0.0, pitch_deg=3.0, heave=0.1, freq=1.0)
+    _compare(_run(ep, [20], flags=TALL), _run(ep, [20], flags=api.FLAG_SINGLE_STEPS))
+    ep = wl.tandem_pitch_heave("tiny_t", 2.6, 1.8, 0.1, 100.0, -0.4, 0.0, 30, 12, n_wings=1, pitch_deg=2.0,
+                               heave=0.02)
+    _compare(_run(ep, [12], flags=TALL), _run(ep, [12], flags=api.FLAG_SINGLE_STEPS))

@@ -9,9 +9,10 @@ on the lattices they run:
   interior and its pulls inside the lattice, and every tile's staged box
   starts on a 16-byte boundary;
 * the ring kernel covers every interior node the far field reads;
-* a support box touches at most ``PASS_TILES_PER_SEGMENT`` tiles (the near
+* a support box touches at most ``pass_tiles_per_segment`` tiles (the near
   kernel's capacity per segment).
-The tile shape is read from the header that sets it.
+Both tile shapes a handle may take (``PASS_TY`` and ``PASS_TY_TALL`` rows)
+are read from the header that sets them.
 """
 import itertools
 import os
@@ -24,14 +25,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HDR = os.path.join(HERE, "..", "lbm_mutiwing_b200", "csrc", "lbm_kernels.h")
 
 
-def _shape():
+def _shapes():
     s = open(HDR).read()
     tx = int(re.search(r"#define LBM_PASS_TX (\d+)", s).group(1))
     ty = int(re.search(r"#define LBM_PASS_TY (\d+)", s).group(1))
-    return tx, ty
+    tall = int(re.search(r"#define LBM_PASS_TY_TALL (\d+)", s).group(1))
+    return [(tx, ty), (tx, tall)]
 
 
-TX, TY = _shape()
+SHAPES = _shapes()
+TX, TY = SHAPES[0]
 
 
 def ntx(nx):
@@ -61,8 +64,19 @@ def in_r1(tx, ty, i, j):
 LATTICES = [(27, 19), (201, 101), (385, 193), (130, 66)]
 
 
+@pytest.fixture(params=SHAPES, ids=lambda s: "%dx%d" % s)
+def shape(request):
+    """The tile shape the formulas above use (module globals, as in the
+    kernels' compile-time constants)."""
+    g = globals()
+    old = g["TX"], g["TY"]
+    g["TX"], g["TY"] = request.param
+    yield request.param
+    g["TX"], g["TY"] = old
+
+
 @pytest.mark.parametrize("nx,ny", LATTICES)
-def test_flags_and_partition(nx, ny):
+def test_flags_and_partition(shape, nx, ny):
     rng = random.Random(nx * 7 + ny)
     for _ in range(400):   # band nodes keep 3 nodes off the border
         i, j = rng.randrange(3, nx - 3), rng.randrange(3, ny - 3)
@@ -84,7 +98,7 @@ def test_flags_and_partition(nx, ny):
 
 
 @pytest.mark.parametrize("nx,ny", LATTICES)
-def test_ring_covers_far_field_reads(nx, ny):
+def test_ring_covers_far_field_reads(shape, nx, ny):
     ring = set()
     for u in range(6 * (ny - 2)):
         col = u // (ny - 2)
@@ -103,7 +117,7 @@ def test_ring_covers_far_field_reads(nx, ny):
     assert need <= ring
 
 
-def test_tiles_per_segment_bound():
+def test_tiles_per_segment_bound(shape):
     per = ((8 + TX - 1) // TX + 1) * ((8 + TY - 1) // TY + 1)
     worst = 0
     for i1, j1 in itertools.product(range(3, 3 + 2 * TX), range(3, 3 + 2 * TY)):
