@@ -22,8 +22,9 @@ roofline: the dominant kernel's algorithmic traffic over its mean CUDA-event
          time, against the measured HBM copy bandwidth.  FP32 path: the
          two-step pass's far-tile kernel, 9 reads of step n + 9 writes of
          step n + 2, 4 bytes each, per node of the far tiles it processed
-         (64 x 8 nodes a tile); whole_step_frac counts 36 bytes per node and
-         step (a pass moves each node's distributions once for two steps),
+         (64 x 8 nodes a tile, 64 x 12 from 32 Mi lattice nodes on);
+         whole_step_frac counts 36 bytes per node and step (a pass moves
+         each node's distributions once for two steps),
          one_step_equivalent_frac 72 (the bytes a one-step scheme moves at
          the same step rate).
 The distribution planes (2 x 288 MB) exceed the 126 MB L2, so no separate L2
@@ -83,6 +84,9 @@ def parse(argv=None):
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     p.add_argument("--workload", default="4000x2000", choices=["800x400", "4000x2000", "16000x8000"])
+    p.add_argument("--pass-tiles", default="auto", choices=["auto", "short", "tall"],
+                   help="tile shape of the two-step passes: by lattice size (64 x 12 from 32 Mi nodes, else "
+                        "64 x 8), or forced either way")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the batched and served measurements")
     p.add_argument("--packed", action="store_true",
@@ -432,7 +436,8 @@ def run_ours(args):
     KP = min(K, 100)
     ep = workload(args.workload, Wm + max_reps * K + KP + 8)
     nodes = ep.nx * ep.ny
-    sim = api.Simulation(ep, prec, device=local)
+    tiles = {"auto": 0, "short": api.FLAG_PASS_SHORT_TILES, "tall": api.FLAG_PASS_TALL_TILES}[args.pass_tiles]
+    sim = api.Simulation(ep, prec, device=local, flags=tiles)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
     # warm-up (builds the step graphs)
     sim.step(Wm, first_cycle=1, rows=False)
@@ -491,7 +496,7 @@ def run_ours(args):
     # e2e: online STEP segments (driver.f90:174-195) through the C ABI with
     # host buffers -- per segment the start and target motion rows go to the
     # device, and every step's force row comes back.
-    sim_e = api.Simulation(ep, prec, motion_source=api.MOTION_STREAM, device=local)
+    sim_e = api.Simulation(ep, prec, motion_source=api.MOTION_STREAM, device=local, flags=tiles)
     ncol = 1 + 9 * ep.wing_count
     # online rows carry displacements relative to the wing bases (mode.f90:207-214)
     motion_rows = ep.motion.copy()
@@ -527,7 +532,7 @@ def run_ours(args):
         kernel = "pass_far_kernel"
         launches = phases["passes"]
         kernel_ms = phases["pass_far_ms"] / launches
-        alg_bytes = 72 * 512 * phases["far_tiles"] / launches
+        alg_bytes = 72 * phases["far_tile_nodes"] / launches
         step_bytes = 36 * interior
     else:
         kernel = "fused_bulk_tma_kernel" if prec == api.PRECISION_FP32 else "plain stream+moments+collide"
@@ -557,6 +562,9 @@ def run_ours(args):
                     "segment_steps": SEG},
             "clocks": clk.summary(),
             "gpu_launches": len(reps) * kernels_in_call(K, args.precision)}
+    if prec == api.PRECISION_FP32:
+        tall = args.pass_tiles == "tall" or (args.pass_tiles == "auto" and nodes >= 32 << 20)
+        line["config"]["pass_tiles"] = "64x12" if tall else "64x8"
     if plain:
         line["plain_fp64"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -205,8 +205,8 @@ int lbm_status(LbmHandle* h, int32_t* bits);
  * re-collision and the cycle advance), [5] assembly and factorisation of
  * the immersed-boundary system, [6] the number of steps timed, and for the
  * FP32 path's two-step passes [7] their far-tile kernel (also in [1]), [8]
- * the passes timed and [9] the far tiles they processed (64 x 8 nodes
- * each).  On the FP32 path phases 0, 3, 4 and 5 overlap phase 1; in a pass
+ * the passes timed and [9] the nodes of the far tiles they processed
+ * (64 x 8 or 64 x 12 nodes a tile).  On the FP32 path phases 0, 3, 4 and 5 overlap phase 1; in a pass
  * [2] holds the step n + 1 ring and the near tiles.  Enabling (or disabling)
  * clears the totals.  n is the length of out (at most 10 values are
  * written). */

@@ -333,7 +333,7 @@ class Simulation:
         self._check(self.L.lbm_get_phase_times(self.h, _dp(out), 10))
         return {"move_boundary_ms": out[0], "collide_stream_ms": out[1], "band_ms": out[2],
                 "bc_ms": out[3], "ibm_solve_ms": out[4], "ibm_factor_ms": out[5], "steps": int(out[6]),
-                "pass_far_ms": out[7], "passes": int(out[8]), "far_tiles": int(out[9])}
+                "pass_far_ms": out[7], "passes": int(out[8]), "far_tile_nodes": int(out[9])}
 
     def stream(self) -> int:
         return int(self.L.lbm_stream(self.h) or 0)

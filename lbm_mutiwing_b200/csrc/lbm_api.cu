@@ -184,9 +184,9 @@ struct LbmHandle {
     // near: the near tiles of a pass
     cudaStream_t s_main = nullptr, s_ibm = nullptr, s_bc = nullptr, s_aux[2] = {}, s_aux2[2] = {}, s_near = nullptr;
     cudaEvent_t ev_ibm = nullptr, ev_main = nullptr, ev_bc = nullptr, ev_geom[GEO_SETS] = {};
-    // a pass: first step's chain and far field done, step n + 1 ring
+    // a pass: first step's rhs, chain and far field done, step n + 1 ring
     // values written, near tiles done
-    cudaEvent_t ev_chain1 = nullptr, ev_bc1 = nullptr, ev_ring = nullptr, ev_near = nullptr;
+    cudaEvent_t ev_rhs1 = nullptr, ev_chain1 = nullptr, ev_bc1 = nullptr, ev_ring = nullptr, ev_near = nullptr;
     cudaEvent_t ev_list[GEO_SETS] = {}, ev_fact[GEO_SETS] = {};   // a set's band list / factor done
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
@@ -664,7 +664,7 @@ void enqueue_step(LbmHandle* h, bool fields, bool diag, bool prefetch, bool drai
 //           columns and rows the far field reads), then, after the first
 //           chain (a band node may sit in column 3), the far field of
 //           step n + 1 (O -> Q border)
-//   s_main  far tiles (P -> Q), from the start
+//   s_main  far tiles (P -> Q), once the first chain's rhs is done
 //   s_near  near tiles (P and O -> Q), after the first chain and far field
 //   aux     the geometry of steps n + 2 and n + 3
 // The pass ends when all are done (the next pass reads all of them).
@@ -726,6 +726,12 @@ void enqueue_pass(LbmHandle* h, bool diag_last = false) {
     {
         PhaseMark pm(h, 4, h->s_ibm);
         launch_ibm_rhs(dA, true, h->s_ibm);
+        // the far tiles start once the first rhs is done: the substitution
+        // block then finds an SM before the far tiles fill them all (its
+        // shared memory can exceed what one far-tile block frees, and
+        // lower-priority blocks that fit are placed first)
+        cudaEventRecord(h->ev_rhs1, h->s_ibm);
+        cudaStreamWaitEvent(h->s_main, h->ev_rhs1, 0);
         launch_ibm_solve(dA, true, false, h->s_ibm);
     }
     cudaEventRecord(h->ev_chain1, h->s_ibm);
@@ -1215,7 +1221,8 @@ int lbm_create(const LbmConfig* cfg, const double* markers_xy, const int32_t* po
     for (int s = 0; s < GEO_SETS; ++s) CK(cudaEventCreateWithFlags(&h->ev_geom[s], cudaEventDisableTiming));
     CK(cudaStreamCreateWithPriority(&h->s_bc, cudaStreamNonBlocking, h->prio_mid));
     CK(cudaStreamCreateWithPriority(&h->s_near, cudaStreamNonBlocking, h->prio_mid));
-    for (cudaEvent_t* e : {&h->ev_ibm, &h->ev_main, &h->ev_bc, &h->ev_chain1, &h->ev_bc1, &h->ev_ring, &h->ev_near})
+    for (cudaEvent_t* e :
+         {&h->ev_ibm, &h->ev_main, &h->ev_bc, &h->ev_rhs1, &h->ev_chain1, &h->ev_bc1, &h->ev_ring, &h->ev_near})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     for (int s = 0; s < GEO_SETS; ++s) {
         CK(cudaEventCreateWithFlags(&h->ev_list[s], cudaEventDisableTiming));
@@ -2073,7 +2080,7 @@ int lbm_get_phase_times(LbmHandle* h, double* out, int32_t n) {
         int ft = 0;
         CK(cudaSetDevice(h->cfg.device));
         CK(cudaMemcpy(&ft, h->d_far_tiles, sizeof(int), cudaMemcpyDeviceToHost));
-        v[9] = (double)ft;
+        v[9] = (double)ft * PASS_TX * h->d.pass_rows;   // nodes of the far tiles
     }
     for (int k = 0; k < n && k < 10; ++k) out[k] = v[k];
     return 0;
@@ -2109,7 +2116,7 @@ void lbm_destroy(LbmHandle* h) {
     for (cudaStream_t s :
          {h->s_main, h->s_ibm, h->s_aux[0], h->s_aux[1], h->s_aux2[0], h->s_aux2[1], h->s_bc, h->s_near})
         if (s) cudaStreamDestroy(s);
-    for (cudaEvent_t e : {h->ev_bc, h->ev_ibm, h->ev_main, h->ev_chain1, h->ev_bc1, h->ev_ring, h->ev_near})
+    for (cudaEvent_t e : {h->ev_bc, h->ev_ibm, h->ev_main, h->ev_rhs1, h->ev_chain1, h->ev_bc1, h->ev_ring, h->ev_near})
         if (e) cudaEventDestroy(e);
     for (int s = 0; s < GEO_SETS; ++s) {
         if (h->ev_list[s]) cudaEventDestroy(h->ev_list[s]);
