@@ -152,12 +152,11 @@ int lbm_err(LbmHandle* h, double* err);
  * is written by the same call.  The array is shared by every call on a
  * device, so calls that overlap in time on one device race and must be
  * serialised by the caller.  The first call on each device looks the array
- * up (cudaGetSymbolAddress); make it before any stream capture begins.
- * Kernels run on `stream` (a cudaStream_t, NULL for the default stream) of
- * `device`; every call then synchronises `stream` and copies err to the
- * host before it returns.  Returns 0,
- * or -1 (bad argument), -2 (too many rows), -3 (CUDA error) with the text in
- * msg (msg_cap bytes, may be NULL).  The caller's current device is kept. */
+ * up (cudaGetSymbolAddress).  Kernels run on `stream` (a cudaStream_t, NULL
+ * for the default stream) of `device`; every call then synchronises `stream`
+ * and copies err to the host before it returns.  Returns 0, or -1 (bad
+ * argument), -2 (too many rows), -3 (CUDA error) with the text in msg
+ * (msg_cap bytes, may be NULL).  The caller's current device is kept. */
 #define LBM_NOALLOC_MAX_ROWS 16384
 int lbm_err_fields_noalloc(const double* u, const double* v, const double* u0, const double* v0,
                            int32_t nx, int32_t ny, int64_t pitch, int32_t device, void* stream,

@@ -19,9 +19,8 @@
 // ordered by events) race on it, so the caller must serialise them.
 //
 // The address of the array is looked up once per device, on the first call
-// for that device; make that first call before any stream capture begins.
-// Every call synchronises the caller's stream and copies the result to the
-// host before it returns.
+// for that device.  Every call synchronises the caller's stream and copies
+// the result to the host before it returns.
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
