@@ -563,7 +563,12 @@ __device__ __forceinline__ void ibm_rhs_fused_body(const DevState& d, const int 
     const int stride = rhs_grid(d) * 4;   // warps of the grid
     for (int s = (bid_ * 128 + threadIdx.x) >> 5; s < d.nseg; s += stride) ibm_rhs_fused_seg(d, s, threadIdx.x & 31);
 }
-__global__ void ibm_rhs_fused_kernel(DevState d) { ibm_rhs_fused_body(d, blockIdx.x); }
+// the substitution after it may be scheduled at once (its block holds much
+// shared memory and so finds an SM while this kernel runs)
+__global__ void ibm_rhs_fused_kernel(DevState d) {
+    pdl_release();
+    ibm_rhs_fused_body(d, blockIdx.x);
+}
 __global__ void ibm_rhs_fused_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     ibm_rhs_fused_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
@@ -631,7 +636,10 @@ __device__ __forceinline__ void ibm_spread_kernel_body(const DevState& d, const 
                   (unsigned long long)__double2ll_rn(ldexp(wv * d.ry[s], e)));
     }
 }
-__global__ void ibm_spread_kernel(DevState d) { ibm_spread_kernel_body(d, blockIdx.x); }
+__global__ void ibm_spread_kernel(DevState d) {
+    pdl_wait();
+    ibm_spread_kernel_body(d, blockIdx.x);
+}
 __global__ void ibm_spread_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     ibm_spread_kernel_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
@@ -963,7 +971,10 @@ __device__ __forceinline__ void ibm_close_body(const DevState& d, const int bid_
     }
 }
 template <bool FIELDS>
-__global__ void __launch_bounds__(FINISH_THREADS) ibm_close_kernel(DevState d) { ibm_close_body<FIELDS>(d, blockIdx.x); }
+__global__ void __launch_bounds__(FINISH_THREADS) ibm_close_kernel(DevState d) {
+    pdl_wait();
+    ibm_close_body<FIELDS>(d, blockIdx.x);
+}
 __global__ void __launch_bounds__(FINISH_THREADS) ibm_close_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     const DevState& d = *m.ds[e];
@@ -1020,15 +1031,15 @@ void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st) {
     ibm_rhs_kernel<<<blocks(32LL * d.nseg, 128), 128, 0, st>>>(d);
 }
 
-void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st) {
-    launch_ibm_substitution(d, (size_t)d.solve_smem, st);
-    ibm_spread_kernel<<<slot_grid(d), 256, 0, st>>>(d);
+void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st, bool chained) {
+    launch_ibm_substitution(d, (size_t)d.solve_smem, st, chained);
+    launch_chained(chained, ibm_spread_kernel, slot_grid(d), 256, 0, st, d);
     const int nbk = ibm_finish_blocks(d);
     if (fused) {
         if (fields)
-            ibm_close_kernel<true><<<close_grid(d), FINISH_THREADS, 0, st>>>(d);
+            launch_chained(chained, ibm_close_kernel<true>, close_grid(d), FINISH_THREADS, 0, st, d);
         else
-            ibm_close_kernel<false><<<close_grid(d), FINISH_THREADS, 0, st>>>(d);
+            launch_chained(chained, ibm_close_kernel<false>, close_grid(d), FINISH_THREADS, 0, st, d);
         return;
     }
     ibm_finish_kernel<<<nbk, FINISH_THREADS, 0, st>>>(d);

@@ -779,6 +779,7 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
     }
     for (int o = 16; o > 0; o >>= 1) ym = fmax(ym, __shfl_xor_sync(0xffffffffu, ym, o));
     if (lane == 0) d.ymax[2 * w + comp] = ym;
+    pdl_release();   // the spread may be scheduled (it waits for this grid to complete)
     // Supports of different wings share nodes: the last wing block to finish
     // (a per-episode counter after a fence; no block waits) solves the joint
     // system from the per-wing solutions, before the spread reads them.
@@ -795,7 +796,10 @@ __device__ __forceinline__ void ibm_solve_kernel_body(const DevState& d, const i
     }
 }
 template <bool SMEM>
-__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) { ibm_solve_kernel_body<SMEM>(d, blockIdx.x); }
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel(DevState d) {
+    pdl_wait();
+    ibm_solve_kernel_body<SMEM>(d, blockIdx.x);
+}
 template <bool SMEM>
 __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
@@ -914,7 +918,10 @@ __device__ __forceinline__ void ibm_solve32_body(const DevState& d, const int bi
         cg_joint_solve(d, z, comp, lane);
     }
 }
-__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve32_kernel(DevState d) { ibm_solve32_body(d, blockIdx.x); }
+__global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve32_kernel(DevState d) {
+    pdl_wait();
+    ibm_solve32_body(d, blockIdx.x);
+}
 __global__ void __launch_bounds__(SOLVE_THREADS) ibm_solve32_kernel_multi(MultiArgs m) {
     const int e = multi_episode(m, blockIdx.x);
     ibm_solve32_body(*m.ds[e], blockIdx.x - __ldg(m.boff + e));
@@ -993,14 +1000,14 @@ void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_
         ibm_factor_kernel<false><<<d.wing_count, FACTOR_THREADS, factor_smem, st>>>(d);
 }
 
-void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st) {
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st, bool chained) {
     if (d.wing_count <= 0) return;
     if (d.solve32)
-        ibm_solve32_kernel<<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+        launch_chained(chained, ibm_solve32_kernel, d.wing_count, SOLVE_THREADS, solve_smem, st, d);
     else if (d.solve_in_smem)
-        ibm_solve_kernel<true><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+        launch_chained(chained, ibm_solve_kernel<true>, d.wing_count, SOLVE_THREADS, solve_smem, st, d);
     else
-        ibm_solve_kernel<false><<<d.wing_count, SOLVE_THREADS, solve_smem, st>>>(d);
+        launch_chained(chained, ibm_solve_kernel<false>, d.wing_count, SOLVE_THREADS, solve_smem, st, d);
 }
 
 // Packed launches: one block per wing of every episode; episodes whose

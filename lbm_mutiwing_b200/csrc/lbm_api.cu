@@ -732,14 +732,14 @@ void enqueue_pass(LbmHandle* h, bool diag_last = false) {
         // lower-priority blocks that fit are placed first)
         cudaEventRecord(h->ev_rhs1, h->s_ibm);
         cudaStreamWaitEvent(h->s_main, h->ev_rhs1, 0);
-        launch_ibm_solve(dA, true, false, h->s_ibm);
+        launch_ibm_solve(dA, true, false, h->s_ibm, true);
     }
     cudaEventRecord(h->ev_chain1, h->s_ibm);
     cudaStreamWaitEvent(h->s_ibm, h->ev_ring, 0);
     {
         PhaseMark pm(h, 4, h->s_ibm);
         launch_ibm_rhs(dB, true, h->s_ibm);
-        launch_ibm_solve(dB, true, false, h->s_ibm);
+        launch_ibm_solve(dB, true, false, h->s_ibm, true);
     }
     cudaEventRecord(h->ev_ibm, h->s_ibm);
     cudaStreamWaitEvent(h->s_bc, h->ev_chain1, 0);

@@ -195,4 +195,32 @@ __host__ __device__ inline long long pidx(const DevState& d, int i, int j) {
     return (long long)j * d.pitch + i;   // 0-based (i, j)
 }
 
+// Programmatic dependent launch (the chain of the immersed boundary): a
+// kernel launched with programmatic stream serialization (launch_chained)
+// may be scheduled while its predecessor in the stream still runs, once
+// every block of the predecessor has called pdl_release(); pdl_wait() then
+// holds it until the predecessor grid has completed and its writes are
+// visible.  Both are no-ops for kernels launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launches kernel k; chained: with programmatic stream serialization (the
+// kernel must begin with pdl_wait() before it touches what its predecessor
+// writes or reads).
+template <class... P, class... A>
+inline cudaError_t launch_chained(bool chained, void (*k)(P...), int grid, int block, size_t smem,
+                                  cudaStream_t st, const A&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = chained ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 }  // namespace lbm

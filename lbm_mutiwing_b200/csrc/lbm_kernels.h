@@ -119,8 +119,10 @@ void launch_ibm_factor(const DevState& d, size_t factor_smem, cudaStream_t st);
 void launch_ibm_rhs(const DevState& d, bool fused, cudaStream_t st);
 // substitution, spread, velocity correction, forces (needs rhs and factor);
 // on the fused path also the band nodes' re-collision (fields: write rho,
-// u, v there) and the cycle advance
-void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st);
+// u, v there) and the cycle advance.  chained: the substitution, spread and
+// closing kernel go out with programmatic stream serialization, each
+// scheduled while its predecessor (the rhs first) still runs
+void launch_ibm_solve(const DevState& d, bool fused, bool fields, cudaStream_t st, bool chained = false);
 int ibm_finish_blocks(const DevState& d);
 // kernels of a step's geometry (motion through factorisation)
 bool is_geometry_kernel(const void* func);
@@ -137,7 +139,7 @@ bool ibm_solve_ring_fits(int bw);
 // (a multiple of 16 bytes)
 size_t ibm_factor_staging_bytes(int bw_max);
 void launch_ibm_factor_blocks(const DevState& d, size_t factor_smem, cudaStream_t st);
-void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st);
+void launch_ibm_substitution(const DevState& d, size_t solve_smem, cudaStream_t st, bool chained = false);
 // 32-row panel substitution: doubles of a wing's panel data, and the
 // kernel's dynamic shared memory for the largest wing's panel data
 long long ibm_panel32_storage(int nw, int bw);
