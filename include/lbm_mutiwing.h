@@ -53,7 +53,8 @@ extern "C" {
 #define LBM_FLAG_PASS_TALL_TILES 16   /* fused path: two-step passes over 64 x 12 tiles whatever the lattice
                                          size (by default from 32 Mi nodes on; the same results) */
 #define LBM_FLAG_PASS_SHORT_TILES 32  /* fused path: two-step passes over 64 x 8 tiles whatever the lattice
-                                         size (by default below 32 Mi nodes; the same results) */
+                                         size (by default below 32 Mi nodes; the same results);
+                                         LBM_FLAG_PASS_TALL_TILES wins when both are given */
 
 /* lbm_step flags */
 #define LBM_STEP_FIELDS 1      /* last step leaves rho, u, v, pre readable by lbm_get_fields */
