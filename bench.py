@@ -562,9 +562,9 @@ def run_ours(args):
                     "segment_steps": SEG},
             "clocks": clk.summary(),
             "gpu_launches": len(reps) * kernels_in_call(K, args.precision)}
-    if prec == api.PRECISION_FP32:
+    if prec == api.PRECISION_FP32 and roof["kernel"] == "pass_far_kernel":
         tall = args.pass_tiles == "tall" or (args.pass_tiles == "auto" and nodes >= 32 << 20)
-        line["config"]["pass_tiles"] = "64x12" if tall else "64x8"
+        roof["tile"] = "64x12" if tall else "64x8"   # the far-tile kernel's tile (nodes)
     if plain:
         line["plain_fp64"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
