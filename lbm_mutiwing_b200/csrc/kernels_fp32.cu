@@ -322,17 +322,18 @@ int fused_tensor_map(const DevState& d, const float* base, void* out) {
 // ------------------------------------------------------------ two-step passes
 // One pass advances the interior n -> n + 2 with one read of step n's planes
 // P and one write of step n + 2's planes Q (temporal blocking: half the HBM
-// traffic of two steps).  A block takes a tile of PASS_TX x PASS_TY nodes:
-// one thread issues nine tiled tensor loads of the tile and two rings of
+// traffic of two steps).  A block takes a tile of PASS_TX x R nodes (R =
+// PASS_TY or PASS_TY_TALL rows, a template parameter of the kernels): one
+// thread issues nine tiled tensor loads of the tile and two rings of
 // neighbours (box of PASS_TX + 8 columns from x0 - 4, 16-byte aligned, and
-// PASS_TY + 4 rows from y0 - 2; out-of-range parts read as zero), the block
+// R + 4 rows from y0 - 2; out-of-range parts read as zero), the block
 // computes step n + 1 on the tile and one ring (R1) into shared memory, then
 // step n + 2 on the tile from there.  Step n + 1 values that are not plain
 // collisions -- band nodes of step n (immersed boundary) and the border (far
 // field) -- come from O, where the band re-collision and the far field of
 // step n put them; tiles whose R1 holds such nodes are the near tiles, run
-// after those writers, every other tile (the far tiles) from the start of
-// the pass.  Band nodes of step n + 1 and the border are left out of Q: the
+// after those writers, every other tile (the far tiles) without waiting for
+// them (it reads nothing but P).  Band nodes of step n + 1 and the border are left out of Q: the
 // second step's band re-collision and far field write them.  Every node is
 // computed by fused_collide, as in the one-step kernels, so a pass gives the
 // bits of two steps.
