@@ -44,3 +44,22 @@ def test_create_fails_loudly_without_gpu_or_bad_config():
         assert "6 x 6" in str(e) or "CUDA" in str(e)
     else:
         raise AssertionError("expected LbmError")
+
+
+def test_flag_constants_match_header_and_fortran_block():
+    """Every LBM_FLAG_* / LBM_STEP_* / LBM_PRECISION_* macro of the header has
+    the same value in the Python binding and in the Fortran interface block
+    a maintainer would add."""
+    hdr = open(os.path.join(ROOT, "include", "lbm_mutiwing.h")).read()
+    macros = dict((m, int(v)) for m, v in re.findall(r"#define (LBM_(?:FLAG|STEP|PRECISION)_[A-Z0-9_]+)\s+(\d+)", hdr))
+    assert {"LBM_FLAG_PASS_TALL_TILES", "LBM_FLAG_PASS_SHORT_TILES", "LBM_FLAG_SINGLE_STEPS"} <= set(macros)
+    for m, v in macros.items():
+        name = m[len("LBM_"):]
+        if hasattr(api, name):
+            assert getattr(api, name) == v, m
+    flags = {m: v for m, v in macros.items() if m.startswith("LBM_FLAG_")}
+    for m, v in flags.items():
+        assert hasattr(api, m[len("LBM_"):]), m
+    fortran = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    fvals = dict((m, int(v)) for m, v in re.findall(r"(LBM_FLAG_[A-Z0-9_]+) = (\d+)", fortran))
+    assert fvals == flags
