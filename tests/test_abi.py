@@ -48,8 +48,8 @@ def test_create_fails_loudly_without_gpu_or_bad_config():
 
 def test_flag_constants_match_header_and_fortran_block():
     """Every LBM_FLAG_* / LBM_STEP_* / LBM_PRECISION_* macro of the header has
-    the same value in the Python binding and in the Fortran interface block
-    a maintainer would add."""
+    the same value in the Python binding, and every flag the same value in
+    the Fortran interface block of the integration notes."""
     hdr = open(os.path.join(ROOT, "include", "lbm_mutiwing.h")).read()
     macros = dict((m, int(v)) for m, v in re.findall(r"#define (LBM_(?:FLAG|STEP|PRECISION)_[A-Z0-9_]+)\s+(\d+)", hdr))
     assert {"LBM_FLAG_PASS_TALL_TILES", "LBM_FLAG_PASS_SHORT_TILES", "LBM_FLAG_SINGLE_STEPS"} <= set(macros)
